@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Served calibration-flash stream on the B200 (one JSON line on rank 0).
+
+Workload: 4096 monochromatic 450 nm isotropic flashes of 1e10 photons, uniform
+in a cylinder (r 60 m, h 300 m) around the centroid of the 48-OM synthetic
+array (seed 11), served in uneven batches of 1-256 flashes (seed 12); orders
+0, 1 and >=2 from the multipole table, 65 RTE frequencies, 321-node readout,
+160 bins of 5 ns. A step is one pass over the whole stream.
+
+* ``value``: flashes/s of the served mixed-precision path (fused tcgen05
+  kernel, split-BF16 readout, fp32 accumulate), inputs resident in HBM,
+  CUDA-event timed, L2 flushed between steps.
+* ``plain_fp32``: the plain FP32 GPU path launched once per flash.
+* ``e2e``: the same stream through the public batch API from pinned host
+  buffers, every response field copied back to the host each step.
+* ``cpu_baseline``: the CPU oracle on a bounded sample on this host.
+
+``--impl reference`` times the reference algorithm on the host CPU (the oracle
+port, all cores) on the same workload and prints the same line.
+``--gpus N`` under torchrun runs N independent replicas (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "showers/s + p99 latency, served mixed-precision vs plain GPU at <=1e-3 rel pe error"
+TABLE = ROOT / "lighthit_b200" / "tables" / "flash_450nm_2-250m.npz"
+N_FLASH = 4096
+
+
+def workload():
+    from lighthit_b200.model import KernelConfig, synthetic_detector
+    from lighthit_b200.workloads import flash_batch_sizes, flash_positions
+    det = synthetic_detector()
+    cfg = KernelConfig(omega_per_ns=np.linspace(0, 1.2, 65),
+                       readout_omega_per_ns=np.linspace(0, 1.2, 321),
+                       relative_time_edges_ns=np.arange(-60.0, 745.0, 5.0),
+                       radial_range_m=(2.0, 250.0), threshold_pe=0.01)
+    pos = flash_positions(N_FLASH, det.positions_m.mean(axis=0), seed=11,
+                          om_positions=det.positions_m)
+    sizes = flash_batch_sizes(N_FLASH, seed=12)
+    return det, cfg, pos, sizes
+
+
+def config_json(sizes):
+    return {"workload": "config 1: 4096 isotropic 450 nm flashes (1e10 photons, seed 11) on "
+                        "the 48-OM synthetic array, served in uneven batches of 1-256",
+            "flashes_per_step": N_FLASH, "batches_per_step": len(sizes),
+            "n_om": 48, "omega_nodes": 65, "readout_nodes": 321, "bins": 160,
+            "table": "2-250 m, 48 radial nodes, degree 8", "l2": "flushed between steps",
+            "parallelism": "replicas"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def time_cpu_oracle(pos, det, cfg, sample, processes):
+    """Oracle (float64 NumPy restatement of the reference) on ``sample`` flashes."""
+    from lighthit_b200.model import acceptance_coefficients
+    table = dict(np.load(TABLE))
+    alpha = acceptance_coefficients(det.angular_acceptance, int(table["degree"]))
+    job = dict(table=table, det=dict(positions_m=det.positions_m, orientations=det.orientations,
+                                     area_m2=np.full(len(det), np.pi * 0.2 ** 2), alpha=alpha,
+                                     spectral_weight=float(det.spectral_weight(450.0))),
+               cfg=dict(omega_per_ns=cfg.omega_per_ns, readout_omega_per_ns=cfg.readout_omega_per_ns,
+                        edges_ns=cfg.relative_time_edges_ns, threshold_pe=cfg.threshold_pe,
+                        radial_range_m=cfg.radial_range_m))
+    flashes = [pos[i] for i in range(sample)]
+    t0 = time.perf_counter()
+    if processes <= 1:
+        for p in flashes:
+            _oracle_one((job, p))
+    else:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(processes) as pool:
+            pool.map(_oracle_one, [(job, p) for p in flashes], chunksize=max(1, sample // (4 * processes)))
+    return time.perf_counter() - t0
+
+
+def _oracle_one(arg):
+    job, p = arg
+    from oracle.flash import transport_flash
+    det = dict(job["det"], acceptance=lambda x: .45 + .45 * np.asarray(x) + .10 * np.asarray(x) ** 2)
+    return transport_flash(job["table"], det, dict(position_m=p, photons=1e10, time_ns=0.0),
+                           job["cfg"])["charge_components_pe"].sum()
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    det, cfg, pos, sizes = workload()
+    cores = os.cpu_count() or 1
+    sample = max(cores * 16, 64)
+    for _ in range(args.warmup):
+        time_cpu_oracle(pos, det, cfg, min(sample, cores), cores)
+    times = [time_cpu_oracle(pos, det, cfg, sample, cores) for _ in range(args.steps)]
+    per_flash = float(np.median(times)) / sample
+    value = 1.0 / per_flash
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "flashes/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": per_flash * N_FLASH * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_json(sizes),
+            "cpu_baseline": {"value": value, "unit": "flashes/s", "cores": cores, "kind": "port",
+                             "sample": f"{sample} flashes of the 4096-flash stream per step, "
+                                       f"float64 oracle restatement of the reference route"},
+            "e2e": {"value": value, "unit": "flashes/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ours(args, rank, world, local_rank):
+    import torch
+    from lighthit_b200.flash import FlashTable, FlashTransport
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    det, cfg, pos_np, sizes = workload()
+    table = FlashTable.load(TABLE)
+    served = FlashTransport(det, cfg, table, device=dev, mode="split-bf16")
+    plain = FlashTransport(det, cfg, table, device=dev, mode="fp32")
+    F = N_FLASH
+    pos = torch.tensor(pos_np, dtype=torch.float64, device=dev)
+    ph = torch.full((F,), 1e10, dtype=torch.float64, device=dev)
+    tt = torch.zeros(F, dtype=torch.float64, device=dev)
+    out = served.allocate(F)
+    bounds = np.concatenate([[0], np.cumsum(sizes)])
+    slices = [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:])]
+    # per-batch output views (first-dim slices stay contiguous); one status block per batch
+    views = []
+    for a, b in slices:
+        v = {k: t[a:b] for k, t in out.items() if k != "status"}
+        v["status"] = torch.zeros(4, dtype=torch.int32, device=dev)
+        views.append(v)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step(record=None):
+        for i, (a, b) in enumerate(slices):
+            if record is not None:
+                record[i][0].record(stream)
+            served.launch(pos[a:b], ph[a:b], tt[a:b], views[i], stream=stream)
+            if record is not None:
+                record[i][1].record(stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize(dev)
+    for v in views:
+        served.raise_for_status(v)
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in slices] for _ in range(args.steps)]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local_rank) as clocks:
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)  # write > L2 between timed steps (outside the events)
+            starts[k].record(stream)
+            step(ev[k])
+            ends[k].record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    batch_ms = np.array([[s.elapsed_time(e) for s, e in row] for row in ev])
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * F * args.steps / (total_ms / 1e3)
+
+    # roofline of the fused kernel: algorithmic bytes = outputs written per (flash, OM)
+    per_pair = 65 * 3 * 8 + 3 * 160 * 4 + 3 * 8 + 8 + 1
+    kernel_s = batch_ms.sum() / 1e3
+    achieved = per_pair * 48 * F * args.steps / kernel_s / 1e9
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (
+        ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+
+    # plain FP32 path, one launch per flash
+    n_plain = min(512, F)
+    pout = plain.allocate(1)
+    for i in range(8):
+        plain.launch(pos[i:i + 1], ph[i:i + 1], tt[i:i + 1], pout, stream=stream)
+    torch.cuda.synchronize(dev)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for i in range(n_plain):
+        plain.launch(pos[i:i + 1], ph[i:i + 1], tt[i:i + 1], pout, stream=stream)
+    p1.record(stream)
+    torch.cuda.synchronize(dev)
+    plain_value = n_plain / (p0.elapsed_time(p1) / 1e3)
+
+    # end to end through the public batch API from pinned host buffers
+    h_pos = torch.tensor(pos_np, dtype=torch.float64).pin_memory()
+    h_ph = torch.full((F,), 1e10, dtype=torch.float64).pin_memory()
+    h_t = torch.zeros(F, dtype=torch.float64).pin_memory()
+    h_out = {k: torch.empty(t.shape, dtype=t.dtype).pin_memory() for k, t in out.items()
+             if k != "status"}
+    d_pos, d_ph, d_t = torch.empty_like(pos), torch.empty_like(ph), torch.empty_like(tt)
+
+    def e2e_step():
+        for i, (a, b) in enumerate(slices):
+            d_pos[a:b].copy_(h_pos[a:b], non_blocking=True)
+            d_ph[a:b].copy_(h_ph[a:b], non_blocking=True)
+            d_t[a:b].copy_(h_t[a:b], non_blocking=True)
+            served.launch(d_pos[a:b], d_ph[a:b], d_t[a:b], views[i], stream=stream)
+            for key, host in h_out.items():
+                host[a:b].copy_(views[i][key], non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * F * args.steps / (e2e_ms / 1e3)
+    h2d = F * (3 * 8 + 8 + 8)
+    d2h = sum(t.numel() * t.element_size() for t in h_out.values())
+    # every response field equals the device result (the copy is complete)
+    assert np.array_equal(h_out["origin"].numpy(), out["origin"].cpu().numpy())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sample = 128
+        secs = time_cpu_oracle(pos_np, det, cfg, sample, 1)
+        cpu = {"value": sample / secs, "unit": "flashes/s", "cores": 1, "kind": "port",
+               "sample": f"first {sample} flashes of the stream, float64 oracle restatement "
+                         "of the reference route, one process"}
+    if rank == 0:
+        lat = batch_ms.ravel()
+        line = {
+            "metric": METRIC, "value": value, "unit": "flashes/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 spectrum, split-bf16 readout (f32 accumulate), f64 clocks",
+            "data": "synthetic", "config": config_json(sizes),
+            "latency": {"batch_device_ms_p50": float(np.percentile(lat, 50)),
+                        "batch_device_ms_p99": float(np.percentile(lat, 99)),
+                        "definition": "device time of one served batch (1-256 flashes)"},
+            "plain_fp32": {"value": plain_value, "unit": "flashes/s",
+                           "launch": "one flash per launch (2 kernels), fp32 CUDA-core readout",
+                           "sample": n_plain},
+            "served_over_plain": value / world / plain_value,
+            "roofline": {"kernel": "flash_tc_kernel", "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+                         "algorithmic_bytes_per_pair": per_pair, "traffic": None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "flashes/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": len(slices) * args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

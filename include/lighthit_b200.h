@@ -1,0 +1,131 @@
+/*
+ * lighthit_b200.h -- C ABI of the B200 (sm_100a) LightHit per-event transport path.
+ *
+ * The reference (NeutrinoHit/LightHit) is a Python package; its hot path is a set
+ * of NumPy/Numba routines behind TransportKernel / ShowerTransport /
+ * EventTransport. Each entry point below replaces one of those routines for a
+ * batch of events. The Python host layer (lighthit_b200/) keeps the reference's
+ * call surface and binds these symbols through ctypes.
+ *
+ * Conventions
+ *  - Every pointer in a *_problem / *_batch struct is a DEVICE pointer owned by
+ *    the caller (tables uploaded once, read-only; outputs caller-allocated),
+ *    except where a field says "host".
+ *  - Functions return LH_OK or an LH_E* code and never throw across the ABI.
+ *  - Data-dependent conditions found on the device (an OM outside the table's
+ *    radial range whose bound is above threshold, a source on an OM centre) are
+ *    reported in the batch's device `status` block; the host reads it with the
+ *    results and raises the reference's ValueError.
+ *  - Work is enqueued on `stream` (a cudaStream_t); nothing synchronises.
+ */
+#ifndef LIGHTHIT_B200_H
+#define LIGHTHIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LH_OK 0
+#define LH_EINVAL 1     /* bad sizes / null pointers (reference: ValueError)   */
+#define LH_ECUDA 2      /* a CUDA launch failed                                */
+#define LH_ENOMEM 3     /* workspace smaller than required (reference: MemoryError) */
+#define LH_ETIMEDOUT 4  /* a bounded device wait gave up                      */
+#define LH_EUNSUPPORTED 5
+
+/* status[0] flag bits written by the device */
+#define LH_STATUS_COINCIDENT 1u  /* a source sits on an OM centre (transport.py:1072-1073) */
+#define LH_STATUS_UNSAFE 2u      /* OM outside range above bound (transport.py:1115-1123)  */
+#define LH_STATUS_TIMEOUT 4u     /* a tensor-core pipeline wait timed out                  */
+
+/* Precision / launch modes. */
+#define LH_MODE_PLAIN_FP32 0   /* CUDA-core fp32 readout: the plain GPU path          */
+#define LH_MODE_SPLIT_BF16 1   /* tcgen05 BF16 hi+lo (3 products), fp32 accumulate    */
+#define LH_MODE_BF16 2         /* tcgen05 single BF16 product, fp32 accumulate        */
+
+/* ------------------------------------------------------------------ readout
+ * Readout operator: bins[b] = sum_k A[k] * B[b][k] with A the relative spectrum
+ * packed as (Re omega_0..n-1, Im omega_0..n-1, zero padding to k_pad).
+ * Built on the host from readout.py:9-40 (inverse_bins) composed with the
+ * not-a-knot cubic refinement of readout.py:55-62.
+ */
+typedef struct {
+  int32_t n_bins;          /* N: output bins                                   */
+  int32_t k_pad;           /* K padded to a multiple of 16 (>= 2*n_omega)      */
+  int32_t n_tile;          /* N columns per tensor-core tile (<= 256, %16 == 0) */
+  int32_t n_tiles;         /* ceil(n_bins / n_tile)                            */
+  const float* b_fp32;     /* [n_bins][k_pad] row-major                        */
+  const uint16_t* b_hi;    /* bf16 bits, [n_tiles][k_pad/8][n_tile][8]         */
+  const uint16_t* b_lo;    /* bf16 bits, same layout (residual x - hi)         */
+} lh_readout_operator;
+
+/* Replaces readout.inverse_bins + CubicSpline refinement (readout.py:43-72) for
+ * `rows` spectra already packed in the workspace layout of `mode`.
+ * out[row][bin] (row stride `out_row_stride` floats). */
+int lh_readout_rows(const lh_readout_operator* op, int mode, const void* a_packed, int64_t rows,
+                    float* out, int64_t out_row_stride, int32_t* status, void* stream);
+
+/* Pack `rows` complex spectra (float2, [row][n_omega]) into the A layout of `mode`. */
+int lh_readout_pack(const lh_readout_operator* op, int mode, const float* spectra_c64,
+                    int32_t n_omega, int64_t rows, void* a_packed, void* stream);
+
+/* Bytes of packed A storage for `rows` rows in `mode`. */
+size_t lh_readout_packed_bytes(const lh_readout_operator* op, int mode, int64_t rows);
+
+/* ------------------------------------------------------------------ flashes
+ * Replaces TransportKernel._transport_isotropic (transport.py:1061-1164) with
+ * ResponseCache.acceptance_spectrum / moments_at (cache.py:294-436) for a batch
+ * of monochromatic isotropic flashes sharing one wavelength table.
+ */
+typedef struct {
+  int32_t n_om;
+  const double* om_pos;        /* [n_om][3]                                        */
+  const double* om_look;       /* [n_om][3] OM orientation (head-on axis)          */
+  const double* om_area;       /* [n_om] effective area m^2                        */
+  int32_t acc_top;             /* highest significant acceptance degree            */
+  const double* alpha;         /* [acc_top+1] Legendre coefficients of acceptance  */
+  double efficiency;           /* spectral weight at the flash wavelength          */
+  int32_t n_omega;
+  const double* omega;         /* [n_omega] rad/ns                                 */
+  int32_t n_radii;
+  const double* log_r;         /* [n_radii] log of table radii                     */
+  const float* coef;           /* float2 [n_radii-1][n_omega][acc_top+1][2][4]    */
+  double mu_a, mu_t;           /* absorption, extinction 1/m                       */
+  double speed;                /* m/ns of the table's band                        */
+  double origin_speed;         /* c / min group index (clock)                      */
+  double r_low, r_high;        /* table radial range m                             */
+  double threshold;            /* pe                                               */
+  int32_t n_edges;
+  const double* edges;         /* [n_edges] relative bin edges ns                  */
+} lh_flash_problem;
+
+typedef struct {
+  int32_t n_flash;
+  const double* pos;           /* [n_flash][3]                                     */
+  const double* photons;       /* [n_flash]                                        */
+  const double* time_ns;       /* [n_flash]                                        */
+  float* spectrum;             /* float2 [n_flash][n_om][n_omega][3] absolute      */
+  float* components;           /* [n_flash][n_om][3][n_bins]                       */
+  double* charge;              /* [n_flash][n_om][3]                               */
+  double* origin;              /* [n_flash][n_om]                                  */
+  uint8_t* active;             /* [n_flash][n_om] bit0 active, bit1 unsafe, bit2 coincident */
+  int32_t* status;             /* [4]: flags, unsafe count, max unsafe radius (double bits) */
+} lh_flash_batch;
+
+size_t lh_flash_workspace_bytes(const lh_flash_problem* p, const lh_readout_operator* op,
+                                int mode, int32_t n_flash);
+
+int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op, int mode,
+                       const lh_flash_batch* b, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
+/* Library version string (host). */
+const char* lh_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIGHTHIT_B200_H */

@@ -1,0 +1,94 @@
+"""ctypes binding of ``liblh_b200.so`` (declarations in ``include/lighthit_b200.h``).
+
+The library is the only compute path: there is no CPU fallback. Loading fails
+loudly when it is missing; ``lighthit_b200.build`` compiles it in-tree.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "liblh_b200.so"
+
+LH_OK, LH_EINVAL, LH_ECUDA, LH_ENOMEM, LH_ETIMEDOUT, LH_EUNSUPPORTED = 0, 1, 2, 3, 4, 5
+LH_STATUS_COINCIDENT, LH_STATUS_UNSAFE, LH_STATUS_TIMEOUT = 1, 2, 4
+LH_MODE_PLAIN_FP32, LH_MODE_SPLIT_BF16, LH_MODE_BF16 = 0, 1, 2
+MODES = {"fp32": LH_MODE_PLAIN_FP32, "split-bf16": LH_MODE_SPLIT_BF16, "bf16": LH_MODE_BF16}
+
+_ERRORS = {LH_EINVAL: "invalid argument", LH_ECUDA: "CUDA launch failed",
+           LH_ENOMEM: "workspace too small", LH_ETIMEDOUT: "device wait timed out",
+           LH_EUNSUPPORTED: "unsupported shape"}
+
+P = C.c_void_p
+
+
+class ReadoutOperator(C.Structure):
+    _fields_ = [("n_bins", C.c_int32), ("k_pad", C.c_int32), ("n_tile", C.c_int32),
+                ("n_tiles", C.c_int32), ("b_fp32", P), ("b_hi", P), ("b_lo", P)]
+
+
+class FlashProblem(C.Structure):
+    _fields_ = [("n_om", C.c_int32), ("om_pos", P), ("om_look", P), ("om_area", P),
+                ("acc_top", C.c_int32), ("alpha", P), ("efficiency", C.c_double),
+                ("n_omega", C.c_int32), ("omega", P), ("n_radii", C.c_int32), ("log_r", P),
+                ("coef", P), ("mu_a", C.c_double), ("mu_t", C.c_double), ("speed", C.c_double),
+                ("origin_speed", C.c_double), ("r_low", C.c_double), ("r_high", C.c_double),
+                ("threshold", C.c_double), ("n_edges", C.c_int32), ("edges", P)]
+
+
+class FlashBatch(C.Structure):
+    _fields_ = [("n_flash", C.c_int32), ("pos", P), ("photons", P), ("time_ns", P),
+                ("spectrum", P), ("components", P), ("charge", P), ("origin", P),
+                ("active", P), ("status", P)]
+
+
+# name -> (restype, argtypes); every symbol the header declares
+SIGNATURES = {
+    "lh_version": (C.c_char_p, []),
+    "lh_readout_packed_bytes": (C.c_size_t, [C.POINTER(ReadoutOperator), C.c_int, C.c_int64]),
+    "lh_readout_pack": (C.c_int, [C.POINTER(ReadoutOperator), C.c_int, P, C.c_int32, C.c_int64,
+                                  P, P]),
+    "lh_readout_rows": (C.c_int, [C.POINTER(ReadoutOperator), C.c_int, P, C.c_int64, P,
+                                  C.c_int64, P, P]),
+    "lh_flash_workspace_bytes": (C.c_size_t, [C.POINTER(FlashProblem),
+                                              C.POINTER(ReadoutOperator), C.c_int, C.c_int32]),
+    "lh_flash_transport": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(ReadoutOperator), C.c_int,
+                                     C.POINTER(FlashBatch), P, C.c_size_t, P]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the library once and bind every declared symbol."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with "
+                               "`python -m lighthit_b200.build` (nvcc, sm_100a)")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (restype, argtypes) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib
+
+
+def check(rc, what):
+    if rc != LH_OK:
+        raise RuntimeError(f"{what}: {_ERRORS.get(rc, 'error')} (code {rc})")
+
+
+def ptr(tensor):
+    """Device address of a contiguous torch tensor (None -> NULL)."""
+    if tensor is None:
+        return None
+    if not tensor.is_contiguous():
+        raise ValueError("tensor must be contiguous")
+    return C.c_void_p(tensor.data_ptr())
+
+
+def stream_ptr(stream):
+    return C.c_void_p(stream.cuda_stream) if stream is not None else None

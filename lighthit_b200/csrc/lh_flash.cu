@@ -1,0 +1,398 @@
+// Isotropic calibration flashes, all scattering orders, on the device.
+//
+// Reference: TransportKernel._transport_isotropic (transport.py:1061-1164) with
+// ResponseCache.acceptance_spectrum / moments_at (cache.py:294-436) and
+// readout_bins (readout.py:43-72), for a monochromatic flash and the
+// centre-ray receiver.
+//
+// Work decomposition: a tile is 64 (flash, OM) pairs = 128 readout rows
+// (orders 1 and 2 of each pair).
+//  1. pair setup (float64, one thread per pair): distance, head-on cosine,
+//     acceptance, the OM clock time_origin_ns, the order-0 bin, the radial
+//     interval of the log-r spline and the safety bound of transport.py:1115;
+//  2. spectrum (float32, one thread per (pair, omega)): cubic in log r of the
+//     detrended multipole moments, contracted with alpha_l P_l(cos)/(4 pi),
+//     times attenuation and the flight phase; writes the absolute spectrum and
+//     the demodulated (relative) spectrum of orders 1 and 2 as readout rows;
+//  3. readout of the rows (see lh_readout.cu) and the order-0 bin rows,
+//     charge (spectrum at the first frequency) and the active mask.
+// flash_tc_kernel fuses 1-3 in one persistent kernel: the readout rows are
+// written straight into shared memory as the tensor-core A tile.
+#include "lh_common.cuh"
+#include "lh_readout.cuh"
+
+namespace lh {
+
+constexpr int kFlashPairs = 64;  // pairs per tile -> 128 readout rows
+constexpr int kMaxAcc = 8;       // highest acceptance degree handled
+constexpr int kFlashThreads = 256;
+
+struct FlashPair {
+  double origin;  // time_origin_ns of the OM for this flash
+  double t12;     // r / speed: flight time of the spectrum phase (orders 1, 2)
+  double t0;      // absolute order-0 phase time (r / speed inside, t + r / speed outside)
+  double q0;      // order-0 bin weight
+  float tt;       // offset in the log-r interval
+  float amp12;    // photons * area * efficiency * exp(-mu_a r) / (4 pi r^2)
+  float amp0;     // order-0 amplitude
+  int j;          // log-r interval, -1 outside the table's radial range
+  int bin0;       // order-0 bin, -1 outside the window
+  int valid;      // pair exists
+  int inside;
+  int flags;      // bit 1: unsafe (outside range, bound above threshold); bit 2: coincident
+  float w[kMaxAcc + 1];  // alpha_l P_l(cos) / (4 pi)
+  float charge[3];
+};
+
+// Step 1 for one pair.
+LH_DEVICE void flash_pair_setup(const lh_flash_problem& p, const lh_flash_batch& b, int64_t pair,
+                                FlashPair& s) {
+  const int n_om = p.n_om;
+  const int64_t f = pair / n_om;
+  const int d = (int)(pair % n_om);
+  const double sx = b.pos[3 * f], sy = b.pos[3 * f + 1], sz = b.pos[3 * f + 2];
+  const double px = p.om_pos[3 * d], py = p.om_pos[3 * d + 1], pz = p.om_pos[3 * d + 2];
+  // displacement = positions - source; radii = |displacement| (transport.py:1069-1070)
+  const double dx = __dsub_rn(px, sx), dy = __dsub_rn(py, sy), dz = __dsub_rn(pz, sz);
+  const double r = sqrt(dot3_rn(dx, dy, dz, dx, dy, dz));
+  s.flags = 0;
+  if (r == 0.0) {
+    atomicOr(reinterpret_cast<unsigned*>(b.status), LH_STATUS_COINCIDENT);
+    s.flags |= 4;
+  }
+  // head_on_cosine (model.py:158-162): toward = (source - position) / |.|
+  const double tx = __dsub_rn(sx, px), ty = __dsub_rn(sy, py), tz = __dsub_rn(sz, pz);
+  const double tn = sqrt(dot3_rn(tx, ty, tz, tx, ty, tz));
+  const double cosine = dot3_rn(p.om_look[3 * d], p.om_look[3 * d + 1], p.om_look[3 * d + 2],
+                                tx / tn, ty / tn, tz / tn);
+  // Legendre P_l(cos): acceptance A = sum alpha_l (2l+1) P_l / (4 pi) (cache.py:509-521)
+  // and contraction weights alpha_l P_l / (4 pi) (cache.py:416-418)
+  double pl_prev = 1.0, pl = cosine, acc = 0.0;
+  for (int l = 0; l <= p.acc_top; ++l) {
+    double P;
+    if (l == 0) P = 1.0;
+    else if (l == 1) P = cosine;
+    else {
+      P = ((2 * l - 1) * cosine * pl - (l - 1) * pl_prev) / l;
+      pl_prev = pl;
+      pl = P;
+    }
+    acc += p.alpha[l] * (2 * l + 1) * P / (4 * kPi);
+    s.w[l] = (float)(P * p.alpha[l] / (4 * kPi));
+  }
+  const double area = p.om_area[d];
+  const double photons = b.photons[f];
+  const double t_src = b.time_ns[f];
+  const double scale = photons * area * p.efficiency;
+  const double four_pi_r2 = 4 * kPi * r * r;
+  s.q0 = scale * acc * exp(-p.mu_t * r) / four_pi_r2;
+  s.inside = (r >= p.r_low) && (r <= p.r_high);
+  const double upper = photons * area * p.efficiency * acc * exp(-p.mu_a * r) / four_pi_r2;
+  if (!s.inside && 10 * upper >= p.threshold) {
+    s.flags |= 2;
+    atomicOr(reinterpret_cast<unsigned*>(b.status), LH_STATUS_UNSAFE);
+    atomicAdd(b.status + 1, 1);
+    atomicMax(reinterpret_cast<unsigned long long*>(b.status + 2),
+              (unsigned long long)__double_as_longlong(r));
+  }
+  const double arrival = t_src + r / p.speed;
+  s.origin = t_src + r / p.origin_speed;
+  const int bin = bin_right(p.edges, p.n_edges, arrival - s.origin);
+  s.bin0 = (bin >= 0 && bin < p.n_edges - 1) ? bin : -1;
+  if (s.inside) {
+    const double logr = log(r);
+    int j = bin_right(p.log_r, p.n_radii, logr);
+    j = j < 0 ? 0 : (j > p.n_radii - 2 ? p.n_radii - 2 : j);
+    s.j = j;
+    s.tt = (float)(logr - p.log_r[j]);
+    s.amp12 = (float)(scale * (exp(-p.mu_a * r) / four_pi_r2));
+    s.amp0 = (float)(scale * acc * (exp(-p.mu_t * r) / four_pi_r2));
+    s.t12 = r / p.speed;
+    s.t0 = r / p.speed;
+  } else {
+    s.j = -1;
+    s.tt = 0.f;
+    s.amp12 = 0.f;
+    s.amp0 = (float)s.q0;
+    s.t12 = 0.0;
+    s.t0 = arrival;
+  }
+  s.valid = 1;
+}
+
+// exp(i * omega * t) with the argument reduced in float64 (turns), then float32.
+LH_DEVICE float2 phase(double omega, double t) {
+  const double turns = omega * t * (1.0 / (2 * kPi));
+  const float frac = (float)(turns - rint(turns));
+  float sv, cv;
+  sincospif(2.f * frac, &sv, &cv);
+  return make_float2(cv, sv);
+}
+
+LH_DEVICE float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Step 2 for one (pair, omega). Returns the relative spectra of orders 1, 2
+// through rel1/rel2 and writes the absolute spectrum of all orders.
+LH_DEVICE void flash_item(const lh_flash_problem& p, const lh_flash_batch& b, int64_t pair,
+                          int w, FlashPair& s, float2& rel1, float2& rel2) {
+  const double om = p.omega[w];
+  float2 s1 = make_float2(0.f, 0.f), s2 = make_float2(0.f, 0.f);
+  if (s.j >= 0) {
+    const int L = p.acc_top + 1;
+    const float4* c = reinterpret_cast<const float4*>(p.coef) +
+                      ((int64_t)s.j * p.n_omega + w) * L * 4;  // 8 float2 = 4 float4 per l
+    const float t = s.tt;
+    for (int l = 0; l < L; ++l) {
+      const float4 a0 = __ldg(c + 4 * l + 0), a1 = __ldg(c + 4 * l + 1);  // order 1: c0..c3
+      const float4 b0 = __ldg(c + 4 * l + 2), b1 = __ldg(c + 4 * l + 3);  // order 2
+      float vr = fmaf(fmaf(fmaf(a0.x, t, a0.z), t, a1.x), t, a1.z);
+      float vi = fmaf(fmaf(fmaf(a0.y, t, a0.w), t, a1.y), t, a1.w);
+      const float wl = s.w[l];
+      s1.x = fmaf(wl, vr, s1.x);
+      s1.y = fmaf(wl, vi, s1.y);
+      vr = fmaf(fmaf(fmaf(b0.x, t, b0.z), t, b1.x), t, b1.z);
+      vi = fmaf(fmaf(fmaf(b0.y, t, b0.w), t, b1.y), t, b1.w);
+      s2.x = fmaf(wl, vr, s2.x);
+      s2.y = fmaf(wl, vi, s2.y);
+    }
+    s1.x *= s.amp12; s1.y *= s.amp12;
+    s2.x *= s.amp12; s2.y *= s.amp12;
+  }
+  const float2 e12 = phase(om, s.t12);
+  const float2 e0 = phase(om, s.t0);
+  const float2 r12 = phase(om, s.t12 - s.origin);
+  const float2 o0 = make_float2(s.amp0 * e0.x, s.amp0 * e0.y);
+  const float2 o1 = cmul(s1, e12), o2 = cmul(s2, e12);
+  if (s.valid) {
+    float2* out = reinterpret_cast<float2*>(b.spectrum) + (pair * p.n_omega + w) * 3;
+    out[0] = o0;
+    out[1] = o1;
+    out[2] = o2;
+    if (w == 0) {
+      s.charge[0] = o0.x;
+      s.charge[1] = o1.x;
+      s.charge[2] = o2.x;
+    }
+  }
+  rel1 = cmul(s1, r12);
+  rel2 = cmul(s2, r12);
+}
+
+// Step 3 (order 0 and the mask) for the tile's pairs.
+LH_DEVICE void flash_tile_order0(const lh_flash_problem& p, const lh_flash_batch& b,
+                                 const FlashPair* sp, int64_t base, int n_bins) {
+  for (int i = threadIdx.x; i < kFlashPairs * n_bins; i += blockDim.x) {
+    const int lp = i / n_bins, bin = i % n_bins;
+    const FlashPair& s = sp[lp];
+    if (!s.valid) continue;
+    b.components[((base + lp) * 3) * n_bins + bin] = (bin == s.bin0) ? (float)s.q0 : 0.f;
+  }
+  if (threadIdx.x < kFlashPairs) {
+    const FlashPair& s = sp[threadIdx.x];
+    if (s.valid) {
+      const int64_t pair = base + threadIdx.x;
+      const double q = ((double)s.charge[0] + (double)s.charge[1]) + (double)s.charge[2];
+      for (int o = 0; o < 3; ++o) b.charge[pair * 3 + o] = (double)s.charge[o];
+      b.origin[pair] = s.origin;
+      const bool active = p.threshold == 0.0 ? s.inside : (s.inside && q >= p.threshold);
+      b.active[pair] = (uint8_t)((active ? 1 : 0) | s.flags);
+    }
+  }
+}
+
+LH_DEVICE void flash_tile_setup(const lh_flash_problem& p, const lh_flash_batch& b, FlashPair* sp,
+                                int64_t base, int64_t n_pairs) {
+  if (threadIdx.x < kFlashPairs) {
+    FlashPair& s = sp[threadIdx.x];
+    const int64_t pair = base + threadIdx.x;
+    if (pair < n_pairs) {
+      flash_pair_setup(p, b, pair, s);
+    } else {
+      s.valid = 0;
+      s.j = -1;
+      s.amp12 = s.amp0 = 0.f;
+      s.t12 = s.t0 = s.origin = 0.0;
+      s.inside = 0;
+      s.flags = 0;
+    }
+    s.charge[0] = s.charge[1] = s.charge[2] = 0.f;
+  }
+}
+
+// ---------------------------------------------------------------- plain path
+// One block per tile; readout rows go to a row-major fp32 workspace that
+// readout_fp32_kernel consumes.
+__global__ void __launch_bounds__(kFlashThreads)
+flash_plain_kernel(lh_flash_problem p, lh_flash_batch b, int kpad, int n_bins, float* a_rows) {
+  __shared__ FlashPair sp[kFlashPairs];
+  const int64_t n_pairs = (int64_t)b.n_flash * p.n_om;
+  const int64_t base = (int64_t)blockIdx.x * kFlashPairs;
+  flash_tile_setup(p, b, sp, base, n_pairs);
+  __syncthreads();
+  const int nw = p.n_omega;
+  for (int i = threadIdx.x; i < kFlashPairs * nw; i += blockDim.x) {
+    const int lp = i / nw, w = i % nw;
+    float2 r1, r2;
+    flash_item(p, b, base + lp, w, sp[lp], r1, r2);
+    if (sp[lp].valid) {
+      float* row1 = a_rows + (2 * (base + lp)) * (int64_t)kpad;
+      float* row2 = row1 + kpad;
+      row1[w] = r1.x;
+      row1[nw + w] = r1.y;
+      row2[w] = r2.x;
+      row2[nw + w] = r2.y;
+      if (w < kpad - 2 * nw) {
+        row1[2 * nw + w] = 0.f;
+        row2[2 * nw + w] = 0.f;
+      }
+    }
+  }
+  __syncthreads();
+  flash_tile_order0(p, b, sp, base, n_bins);
+}
+
+// ---------------------------------------------------------------- fused tcgen05 path
+// 256 threads, one CTA per SM, persistent over tiles. B (the readout operator,
+// hi and lo parts) is loaded once per CTA. Per tile: setup -> spectrum items
+// writing A (bf16 hi/lo) into shared memory -> one thread issues the MMAs ->
+// order-0 rows and mask while the tensor core runs -> TMEM drain.
+__global__ void __launch_bounds__(kFlashThreads, 1)
+flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __restrict__ g_bhi,
+                const __nv_bfloat16* __restrict__ g_blo, int kpad, int n_bins, int n_tile,
+                int passes) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t a_bytes = 128u * kpad * 2u;
+  const uint32_t b_bytes = (uint32_t)n_tile * kpad * 2u;
+  __nv_bfloat16* s_ahi = reinterpret_cast<__nv_bfloat16*>(smem);
+  __nv_bfloat16* s_alo = reinterpret_cast<__nv_bfloat16*>(smem + a_bytes);
+  __nv_bfloat16* s_bhi = reinterpret_cast<__nv_bfloat16*>(smem + 2 * a_bytes);
+  __nv_bfloat16* s_blo = reinterpret_cast<__nv_bfloat16*>(smem + 2 * a_bytes + b_bytes);
+  FlashPair* sp = reinterpret_cast<FlashPair*>(smem + 2 * a_bytes + 2 * b_bytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sp + kFlashPairs);
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 2);
+  uint64_t* bar_b = bars;
+  uint64_t* bar_mma = bars + 1;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool need_lo_b = passes >= 2;
+  if (tid == 0) {
+    mbar_init(bar_b, 1);
+    mbar_init(bar_mma, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(s_tmem, 256);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  if (tid == 0) {
+    mbar_expect_tx(bar_b, b_bytes * (need_lo_b ? 2u : 1u));
+    bulk_g2s(s_bhi, g_bhi, b_bytes, bar_b);
+    if (need_lo_b) bulk_g2s(s_blo, g_blo, b_bytes, bar_b);
+  }
+  const uint32_t idesc = instr_desc_bf16_f32(128, n_tile);
+  const int64_t n_pairs = (int64_t)b.n_flash * p.n_om;
+  const int64_t n_tiles = (n_pairs + kFlashPairs - 1) / kFlashPairs;
+  const int nw = p.n_omega;
+  const int padw = kpad - 2 * nw;
+  uint32_t ph_mma = 0;
+  bool b_ready = false, failed = false, mma_pending = false;
+
+  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t base = tile * kFlashPairs;
+    flash_tile_setup(p, b, sp, base, n_pairs);
+    for (int i = tid; i < 128 * padw; i += blockDim.x) {
+      const int off = tile_offset(i / padw, 2 * nw + i % padw);
+      s_ahi[off] = __float2bfloat16_rn(0.f);
+      s_alo[off] = __float2bfloat16_rn(0.f);
+    }
+    __syncthreads();
+    for (int i = tid; i < kFlashPairs * nw; i += blockDim.x) {
+      const int lp = i / nw, w = i % nw;
+      float2 r1, r2;
+      flash_item(p, b, base + lp, w, sp[lp], r1, r2);
+      __nv_bfloat16 hi, lo;
+      split_bf16(r1.x, hi, lo);
+      s_ahi[tile_offset(2 * lp, w)] = hi;       s_alo[tile_offset(2 * lp, w)] = lo;
+      split_bf16(r1.y, hi, lo);
+      s_ahi[tile_offset(2 * lp, nw + w)] = hi;  s_alo[tile_offset(2 * lp, nw + w)] = lo;
+      split_bf16(r2.x, hi, lo);
+      s_ahi[tile_offset(2 * lp + 1, w)] = hi;   s_alo[tile_offset(2 * lp + 1, w)] = lo;
+      split_bf16(r2.y, hi, lo);
+      s_ahi[tile_offset(2 * lp + 1, nw + w)] = hi; s_alo[tile_offset(2 * lp + 1, nw + w)] = lo;
+    }
+    fence_proxy_async();  // generic-proxy smem writes -> visible to the tensor core
+    __syncthreads();
+    if (tid == 0) {
+      bool ok = true;
+      if (!b_ready) {
+        ok = mbar_wait(bar_b, 0);
+        b_ready = true;
+      }
+      if (ok) {
+        tc_fence_after();
+        const int ksteps = kpad / 16;
+        const uint32_t lbo_a = 128u * 16u, lbo_b = (uint32_t)n_tile * 16u;
+        int first = 1;
+        for (int pass = 0; pass < passes; ++pass) {
+          const __nv_bfloat16* pa = (pass == 2) ? s_alo : s_ahi;
+          const __nv_bfloat16* pb = (pass == 1) ? s_blo : s_bhi;
+          for (int kk = 0; kk < ksteps; ++kk) {
+            uint64_t da = smem_desc_kmajor(reinterpret_cast<const uint8_t*>(pa) + kk * 2 * lbo_a,
+                                           lbo_a, 128);
+            uint64_t db = smem_desc_kmajor(reinterpret_cast<const uint8_t*>(pb) + kk * 2 * lbo_b,
+                                           lbo_b, 128);
+            tc_mma_bf16(tmem, da, db, idesc, first ? 0u : 1u);
+            first = 0;
+          }
+        }
+        tc_commit(bar_mma);
+      } else {
+        failed = true;
+      }
+    }
+    flash_tile_order0(p, b, sp, base, n_bins);
+    if (__syncthreads_or(failed)) { failed = true; break; }
+    const bool ok = mbar_wait(bar_mma, ph_mma);
+    ph_mma ^= 1u;
+    if (__syncthreads_or(!ok)) { failed = true; mma_pending = true; break; }
+    tc_fence_after();
+    // drain: warp w reads TMEM lanes 32*(w%4).. (rows), half (w/4) of the columns
+    const int q = warp & 3, h = warp >> 2;
+    const int row = q * 32 + lane;
+    const int lp = row >> 1, order = 1 + (row & 1);
+    const bool valid = sp[lp].valid;
+    const int chunks = n_tile / 16;
+    const int c_begin = h * ((chunks + 1) / 2), c_end = min(chunks, (h + 1) * ((chunks + 1) / 2));
+    const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
+    float* dst = b.components + ((base + lp) * 3 + order) * (int64_t)n_bins;
+    for (int c = c_begin; c < c_end; ++c) {
+      float v[16];
+      tmem_ld16(lane_addr + (uint32_t)(c * 16), v);
+      if (valid) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (c * 16 + i < n_bins) dst[c * 16 + i] = v[i];
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  if (failed && tid == 0) atomicOr(reinterpret_cast<unsigned*>(b.status), LH_STATUS_TIMEOUT);
+  if (mma_pending) mbar_wait(bar_mma, ph_mma ^ 1u);
+  if (tid == 0 && !b_ready) mbar_wait(bar_b, 0);  // never leave a bulk copy in flight
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+size_t flash_tc_smem_bytes(int kpad, int n_tile) {
+  return 2ull * 128 * kpad * 2 + 2ull * n_tile * kpad * 2 + sizeof(FlashPair) * kFlashPairs + 64;
+}
+
+}  // namespace lh

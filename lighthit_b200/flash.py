@@ -1,0 +1,243 @@
+"""Isotropic calibration flashes on the B200: the ``TransportKernel.transport`` path.
+
+Reference: ``TransportKernel._transport_isotropic`` (``transport.py:1061-1164``)
+for the centre-ray receiver (``KernelConfig.scattered_receiver == 'centre'``),
+with ``ResponseCache.moments_at`` / ``acceptance_spectrum``
+(``cache.py:294-436``) and ``readout_bins`` (``readout.py:43-72``).
+
+The multipole table is built once by the reference (``TransportKernel.build``)
+and uploaded read-only: the host detrends it exactly as ``moments_at`` does
+(attenuation ``exp(-mu_a r)/(4 pi r^2)`` and, for ``radial_phase='flight'``,
+the flight phase), forms the not-a-knot cubic coefficients in log r in
+float64 and stores them as complex64 in the layout
+``[interval][omega][degree][order][power]``. Everything per flash runs in
+``liblh_b200.so``; there is no host fallback.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .model import C_VACUUM_M_PER_NS, Medium, TransportResponse, acceptance_coefficients
+from .readout import DeviceReadout
+from .spline import spline_coefficients
+
+__all__ = ["FlashTable", "FlashTransport"]
+
+
+@dataclass
+class FlashTable:
+    """Multipole moments of one wavelength (``ResponseCache``): (omega, r, degree, order)."""
+    omega_per_ns: np.ndarray
+    radii_m: np.ndarray
+    moments: np.ndarray
+    medium: Medium
+    radial_phase: str
+    degree: int
+
+    @classmethod
+    def load(cls, path):
+        """Table exported from the reference (``tests/golden/make_flash_golden.py``)."""
+        z = np.load(path)
+        medium = Medium(float(z["absorption_per_m"]), float(z["scattering_per_m"]),
+                        float(z["g"]), float(z["group_index"]), float(z["wavelength_nm"]))
+        return cls(np.asarray(z["omega_per_ns"], float), np.asarray(z["radii_m"], float),
+                   np.asarray(z["moments"]), medium, str(z["radial_phase"]), int(z["degree"]))
+
+    @classmethod
+    def from_cache(cls, cache):
+        """From a reference ``ResponseCache`` object (attributes read by name)."""
+        m = cache.medium
+        return cls(np.asarray(cache.grid.omega_per_ns, float), np.asarray(cache.grid.radii_m, float),
+                   np.asarray(cache.moments), Medium(m.absorption_per_m, m.scattering_per_m, m.g,
+                                                     m.group_index, m.wavelength_nm),
+                   str(cache.radial_phase), int(cache.degree))
+
+    def spline_table(self, top):
+        """Complex (interval, omega, degree, order, power) cubic coefficients in log r."""
+        r = self.radii_m
+        omega = self.omega_per_ns
+        scale = np.exp(-self.medium.absorption_per_m * r) / (4 * np.pi * r ** 2)
+        if np.any(scale == 0):
+            raise FloatingPointError("Reference amplitude underflow: reduce radius range")
+        detrended = self.moments[:, :, :top + 1] / scale[None, :, None, None]
+        if self.radial_phase == "flight":
+            detrended = detrended * np.exp(
+                -1j * omega[:, None] * r[None, :] / self.medium.speed_m_per_ns)[:, :, None, None]
+        coef = spline_coefficients(np.log(r), detrended, axis=1)  # (w, j, 4, l, o)
+        return np.ascontiguousarray(coef.transpose(1, 0, 3, 4, 2))  # (j, w, l, o, p)
+
+
+class FlashTransport:
+    """Batched device transport of monochromatic isotropic flashes.
+
+    ``detector`` and ``config`` follow the reference's ``DetectorArray`` and
+    ``KernelConfig``; ``table`` is a :class:`FlashTable` for the flash
+    wavelength. ``mode`` selects the readout precision: ``'split-bf16'``
+    (tensor cores, hi+lo BF16, fp32 accumulate), ``'bf16'`` or ``'fp32'``
+    (the plain CUDA-core path).
+    """
+
+    def __init__(self, detector, config, table, *, device="cuda", mode="split-bf16"):
+        import torch
+        if getattr(config, "scattered_receiver", "centre") != "centre":
+            raise NotImplementedError("only the centre-ray receiver is on the device path")
+        self.detector, self.config, self.table = detector, config, table
+        self.device = torch.device(device)
+        self.mode = mode
+        dev = self.device
+        alpha = acceptance_coefficients(detector.angular_acceptance, table.degree)
+        peak = np.max(np.abs(alpha))
+        significant = np.flatnonzero(np.abs(alpha) > 1e-12 * peak) if peak > 0 else []
+        top = int(significant[-1]) if len(significant) else 0
+        if top > 8:
+            raise NotImplementedError("acceptance degree above 8 is not on the device path")
+        probe = np.asarray(detector.angular_acceptance(np.linspace(-1.0, 1.0, 65)), float)
+        if np.allclose(probe, probe[0], rtol=1e-11, atol=1e-14):
+            # transport.py:1084-1089: a constant acceptance switches order 1 to
+            # the exact full-HG physical-time integral, not implemented here.
+            raise NotImplementedError("constant acceptance (exact order 1) is not on the device path")
+        self.alpha, self.top = alpha, top
+        self.wavelength_nm = float(table.medium.wavelength_nm)
+        self.efficiency = float(detector.spectral_weight(self.wavelength_nm))
+        n = len(detector.positions_m)
+        area = np.broadcast_to(np.asarray(detector.effective_area_m2, float), (n,))
+        omega = np.asarray(config.omega_per_ns, float)
+        if (len(omega) != len(table.omega_per_ns)
+                or not np.allclose(omega, table.omega_per_ns, rtol=0, atol=1e-12)):
+            raise ValueError("table and kernel frequency grids differ")
+        low, high = map(float, config.radial_range_m)
+        if low < table.radii_m[0] - 1e-9 or high > table.radii_m[-1] + 1e-9:
+            raise ValueError("radial_range_m lies outside the table's radii")
+
+        def f64(x):
+            return torch.tensor(np.ascontiguousarray(x, float), dtype=torch.float64, device=dev)
+
+        self._om_pos = f64(detector.positions_m)
+        self._om_look = f64(detector.orientations)
+        self._om_area = f64(area)
+        self._alpha = f64(alpha[:top + 1])
+        self._omega = f64(omega)
+        self._log_r = f64(np.log(table.radii_m))
+        coef = table.spline_table(top).astype(np.complex64)
+        self._coef = torch.view_as_real(torch.from_numpy(coef)).contiguous().to(dev)
+        self._edges = f64(config.relative_time_edges_ns)
+        self.readout = DeviceReadout(omega, config.relative_time_edges_ns,
+                                     config.readout_omega_per_ns, device=dev)
+        medium = table.medium
+        self.problem = _lib.FlashProblem(
+            n, self._om_pos.data_ptr(), self._om_look.data_ptr(), self._om_area.data_ptr(), top,
+            self._alpha.data_ptr(), self.efficiency, len(omega), self._omega.data_ptr(),
+            len(table.radii_m), self._log_r.data_ptr(), self._coef.data_ptr(),
+            medium.absorption_per_m, medium.extinction_per_m, medium.speed_m_per_ns,
+            C_VACUUM_M_PER_NS / medium.group_index, low, high, float(config.threshold_pe),
+            len(config.relative_time_edges_ns), self._edges.data_ptr())
+        self.n_om, self.n_omega = n, len(omega)
+        self.n_bins = len(config.relative_time_edges_ns) - 1
+        self._workspace = None
+
+    # ------------------------------------------------------------------ batch API
+    def allocate(self, n_flash):
+        """Device output buffers for ``n_flash`` flashes (reusable across calls)."""
+        import torch
+        dev, F, D = self.device, int(n_flash), self.n_om
+        return dict(
+            spectrum=torch.empty((F, D, self.n_omega, 3), dtype=torch.complex64, device=dev),
+            components=torch.empty((F, D, 3, self.n_bins), dtype=torch.float32, device=dev),
+            charge=torch.empty((F, D, 3), dtype=torch.float64, device=dev),
+            origin=torch.empty((F, D), dtype=torch.float64, device=dev),
+            active=torch.empty((F, D), dtype=torch.uint8, device=dev),
+            status=torch.zeros(4, dtype=torch.int32, device=dev))
+
+    def workspace_bytes(self, n_flash, mode=None):
+        lib = _lib.load()
+        m = _lib.MODES[mode or self.mode]
+        return int(lib.lh_flash_workspace_bytes(self.problem, self.readout.struct, m, int(n_flash)))
+
+    def launch(self, pos, photons, time_ns, out, *, mode=None, stream=None, workspace=None):
+        """Enqueue one batch. ``pos`` (F,3), ``photons`` (F,), ``time_ns`` (F,) are
+        float64 device tensors; ``out`` comes from :meth:`allocate`. Nothing syncs."""
+        import torch
+        lib = _lib.load()
+        m = _lib.MODES[mode or self.mode]
+        F = int(pos.shape[0])
+        need = self.workspace_bytes(F, mode)
+        if workspace is None and need:
+            if self._workspace is None or self._workspace.numel() < need:
+                self._workspace = torch.empty(need, dtype=torch.uint8, device=self.device)
+            workspace = self._workspace
+        batch = _lib.FlashBatch(
+            F, pos.data_ptr(), photons.data_ptr(), time_ns.data_ptr(),
+            out["spectrum"].data_ptr(), out["components"].data_ptr(), out["charge"].data_ptr(),
+            out["origin"].data_ptr(), out["active"].data_ptr(), out["status"].data_ptr())
+        s = _lib.stream_ptr(stream or torch.cuda.current_stream(self.device))
+        ws_ptr = workspace.data_ptr() if workspace is not None else None
+        ws_bytes = workspace.numel() if workspace is not None else 0
+        _lib.check(lib.lh_flash_transport(self.problem, self.readout.struct, m, batch, ws_ptr,
+                                          ws_bytes, s), "lh_flash_transport")
+        return out
+
+    def run(self, positions, photons, time_ns=None, *, mode=None, stream=None):
+        """Synchronous batch from host arrays; returns device outputs and checks errors."""
+        import torch
+        F = len(positions)
+        pos = torch.tensor(np.asarray(positions, float).reshape(F, 3), dtype=torch.float64,
+                           device=self.device)
+        ph = torch.tensor(np.broadcast_to(np.asarray(photons, float), (F,)).copy(),
+                          dtype=torch.float64, device=self.device)
+        t = torch.tensor(np.zeros(F) if time_ns is None else
+                         np.broadcast_to(np.asarray(time_ns, float), (F,)).copy(),
+                         dtype=torch.float64, device=self.device)
+        out = self.allocate(F)
+        self.launch(pos, ph, t, out, mode=mode, stream=stream)
+        torch.cuda.synchronize(self.device)
+        self.raise_for_status(out)
+        return out
+
+    def raise_for_status(self, out, flash=None):
+        """Raise the reference's ``ValueError`` for the device status of a batch."""
+        status = out["status"].cpu().numpy()
+        flags = int(status[0])
+        if flags & _lib.LH_STATUS_TIMEOUT:
+            raise RuntimeError("a tensor-core pipeline wait timed out on the device")
+        if flags & _lib.LH_STATUS_COINCIDENT:
+            raise ValueError("isotropic point source cannot coincide with an OM centre")
+        if flags & _lib.LH_STATUS_UNSAFE:
+            radius = float(status[2:4].view(np.float64)[0])
+            raise ValueError(
+                f"{int(status[1])} OMs outside radial_range_m have an absorption-only "
+                "estimate above threshold; prepare a cache covering the source-to-OM "
+                f"distances (up to {radius:g} m). "
+                "point_source_radial_range(detector, source.position_m) gives "
+                "the geometric range; validate its numerical resolution separately")
+
+    # ------------------------------------------------------------------ drop-in
+    def transport(self, source, *, method="isotropic"):
+        """``TransportKernel.transport(IsotropicFlash)``: one flash -> ``TransportResponse``."""
+        if getattr(source, "wavelength_nm", None) is None:
+            raise NotImplementedError("broadband flashes need one table per wavelength node")
+        if not np.isclose(float(source.wavelength_nm), self.wavelength_nm, rtol=0, atol=1e-9):
+            raise ValueError("flash wavelength differs from the table's wavelength")
+        out = self.run(np.asarray(source.position_m, float)[None, :], [float(source.photons)],
+                       [float(source.time_ns)])
+        return self.response(out, 0, method=method)
+
+    def response(self, out, index, *, method="isotropic"):
+        """Host ``TransportResponse`` of flash ``index`` of a finished batch."""
+        spectrum = out["spectrum"][index].cpu().numpy().astype(np.complex128)  # (D, w, 3)
+        components = out["components"][index].cpu().numpy().astype(np.float64)  # (D, 3, b)
+        active = out["active"][index].cpu().numpy()
+        return TransportResponse(
+            self.detector, np.asarray(self.config.omega_per_ns, float).copy(),
+            np.asarray(self.config.relative_time_edges_ns, float).copy(),
+            spectrum.transpose(1, 0, 2), components.transpose(0, 2, 1),
+            out["charge"][index].cpu().numpy(), out["origin"][index].cpu().numpy(),
+            (active & 1).astype(bool), method,
+            {"wavelength_nm": [self.wavelength_nm], "detector_angular_model":
+             "exact multipole contraction", "first_order":
+             "finite-L directional-acceptance spectrum and Fourier bins",
+             "fourier_inverted_orders": [1, 2],
+             "radial_range_m": list(map(float, self.config.radial_range_m)),
+             "readout_precision": self.mode, "route": "lighthit_b200.flash"})

@@ -1,0 +1,60 @@
+"""Host-side operator construction (float64, no GPU)."""
+import numpy as np
+import pytest
+from scipy.interpolate import CubicSpline
+
+from conftest import GOLDEN, TABLES
+from lighthit_b200.readout import readout_matrix
+from lighthit_b200.spline import resample_matrix, spline_coefficients
+
+
+@pytest.mark.parametrize("n", [4, 7, 48, 65])
+def test_spline_coefficients_match_scipy(n):
+    rng = np.random.default_rng(n)
+    x = np.sort(rng.uniform(0, 3, n)) + np.arange(n) * 0.05
+    y = rng.normal(size=(n, 3)) + 1j * rng.normal(size=(n, 3))
+    c = spline_coefficients(x, y, axis=0)  # (n-1, 4, 3)
+    ref = CubicSpline(x, y.real, axis=0).c + 1j * CubicSpline(x, y.imag, axis=0).c
+    scale = np.abs(ref).max()
+    assert np.max(np.abs(np.moveaxis(c, 1, 0) - ref)) < 1e-11 * scale
+
+
+def test_resample_matrix_matches_scipy():
+    o = np.linspace(0, 1.2, 65)
+    o2 = np.linspace(0, 1.2, 321)
+    y = np.random.default_rng(1).normal(size=(65, 4))
+    assert np.max(np.abs(resample_matrix(o, o2) @ y - CubicSpline(o, y, axis=0)(o2))) < 1e-13
+
+
+def test_readout_matrix_matches_reference_fixture():
+    g = np.load(GOLDEN / "readout_c0.npz")
+    W = readout_matrix(g["omega_per_ns"], g["edges_ns"], g["readout_omega_per_ns"])
+    assert np.max(np.abs((W @ g["relative"]).real.T - g["bins"])) < 1e-13
+
+
+def test_flash_spline_table_reproduces_oracle_moments(flash_table):
+    from oracle.flash import moments_at
+    t = flash_table
+    table = dict(np.load(TABLES / "flash_450nm_2-250m.npz"))
+    coef = t.spline_table(2)  # (j, w, l, o, p)
+    r = np.array([2.0, 3.3, 17.0, 99.9, 200.0, 250.0])
+    log_r = np.log(t.radii_m)
+    j = np.clip(np.searchsorted(log_r, np.log(r), side="right") - 1, 0, len(log_r) - 2)
+    tt = np.log(r) - log_r[j]
+    c = coef[j]  # (n, w, l, o, p)
+    val = ((c[..., 0] * tt[:, None, None, None] + c[..., 1]) * tt[:, None, None, None]
+           + c[..., 2]) * tt[:, None, None, None] + c[..., 3]
+    scale = np.exp(-t.medium.absorption_per_m * r) / (4 * np.pi * r ** 2)
+    flight = np.exp(1j * t.omega_per_ns[None, :] * r[:, None] / t.medium.speed_m_per_ns)
+    got = val * scale[:, None, None, None] * flight[:, :, None, None]  # (n, w, l, o)
+    ref = moments_at(table, r, 3)  # (w, n, l, o)
+    ref = np.moveaxis(ref, 1, 0)
+    assert np.max(np.abs(got - ref)) < 1e-9 * np.abs(ref).max()
+
+
+def test_acceptance_coefficients_match_fixture(flash_golden):
+    from lighthit_b200.model import acceptance_coefficients, synthetic_detector
+    det = synthetic_detector()
+    alpha = acceptance_coefficients(det.angular_acceptance, 8)
+    assert np.max(np.abs(alpha - flash_golden["alpha"])) < 1e-11
+    np.testing.assert_array_equal(det.positions_m, flash_golden["om_positions_m"])
