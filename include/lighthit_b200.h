@@ -121,6 +121,22 @@ int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op,
                        const lh_flash_batch* b, void* workspace, size_t workspace_bytes,
                        void* stream);
 
+/* Flash transport that allocates nothing (no counterpart in the reference).
+ * For callers that cannot allocate device memory: processes whose device memory
+ * is reserved up front by their own framework's allocator (trigger/DAQ farms),
+ * and latency-critical loops where cudaMalloc/cudaFree would synchronise the
+ * device. Runs the plain FP32 path (as lh_flash_transport with
+ * LH_MODE_PLAIN_FP32) with its scratch in a static 4 MiB __device__ array of the
+ * library: at most 2 * n_flash * n_om * k_pad * 4 bytes, e.g. 75 flashes of a
+ * 48-OM array at k_pad = 144; larger batches return LH_ESCRATCH and launch
+ * nothing. The caller still passes inputs and outputs. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current, so make it before any stream capture. All calls on a device
+ * share the array: calls that overlap on the GPU race and must be serialised. */
+#define LH_ESCRATCH 6   /* request larger than the static scratch of the entry point below */
+int lh_flash_transport_noalloc(const lh_flash_problem* p, const lh_readout_operator* op,
+                               const lh_flash_batch* b, void* stream);
+
 /* Library version string (host). */
 const char* lh_version(void);
 

@@ -55,7 +55,10 @@ SIGNATURES = {
                                               C.POINTER(ReadoutOperator), C.c_int, C.c_int32]),
     "lh_flash_transport": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(ReadoutOperator), C.c_int,
                                      C.POINTER(FlashBatch), P, C.c_size_t, P]),
+    "lh_flash_transport_noalloc": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(ReadoutOperator),
+                                             C.POINTER(FlashBatch), P]),
 }
+LH_ESCRATCH = 6
 
 _lib = None
 
