@@ -37,12 +37,16 @@ def moments_at(table, radii, top):
     def scale(r):
         return np.exp(-mu_a * r) / (4 * np.pi * r ** 2)
 
-    block = np.asarray(table["moments"])[:, :, :top]
-    detrended = block / scale(grid_r)[None, :, None, None]
     flight = str(table["radial_phase"]) == "flight"
-    if flight:
-        detrended = detrended * np.exp(-1j * omega[:, None] * grid_r[None, :] / speed)[:, :, None, None]
-    spline = CubicSpline(np.log(grid_r), detrended, axis=1)
+    key = ("_spline", top)
+    spline = table.get(key)
+    if spline is None:  # the reference caches the spline per degree count too (cache.py:321-334)
+        block = np.asarray(table["moments"])[:, :, :top]
+        detrended = block / scale(grid_r)[None, :, None, None]
+        if flight:
+            detrended = detrended * np.exp(
+                -1j * omega[:, None] * grid_r[None, :] / speed)[:, :, None, None]
+        spline = table[key] = CubicSpline(np.log(grid_r), detrended, axis=1)
     out = spline(np.log(radii)) * scale(radii)[None, :, None, None]
     if flight:
         out = out * np.exp(1j * omega[:, None] * radii[None, :] / speed)[:, :, None, None]
