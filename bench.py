@@ -187,9 +187,14 @@ def reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def _events(torch, n):
+    return [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+
+
 def ours(args, rank, world, local_rank):
     import torch
     from lighthit_b200.flash import FlashTable, FlashTransport
+    from lighthit_b200.serve import FlashServer, ServeConfig, autotune, flash_bytes
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     det, cfg, pos_np, sizes = workload()
@@ -197,54 +202,43 @@ def ours(args, rank, world, local_rank):
     served = FlashTransport(det, cfg, table, device=dev, mode="split-bf16")
     plain = FlashTransport(det, cfg, table, device=dev, mode="fp32")
     F = N_FLASH
+    threads = autotune(served, F, cache=str(ROOT / "_work" / "autotune.json")
+                       if (ROOT / "_work").exists() else None)
     pos = torch.tensor(pos_np, dtype=torch.float64, device=dev)
     ph = torch.full((F,), 1e10, dtype=torch.float64, device=dev)
     tt = torch.zeros(F, dtype=torch.float64, device=dev)
     out = served.allocate(F)
-    bounds = np.concatenate([[0], np.cumsum(sizes)])
-    slices = [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:])]
-    # per-batch output views (first-dim slices stay contiguous); one status block per batch
-    views = []
-    for a, b in slices:
-        v = {k: t[a:b] for k, t in out.items() if k != "status"}
-        v["status"] = torch.zeros(4, dtype=torch.int32, device=dev)
-        views.append(v)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    bounds = np.concatenate([[0], np.cumsum(sizes)])
+    requests = [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:])]
 
-    def step(record=None):
-        for i, (a, b) in enumerate(slices):
-            if record is not None:
-                record[i][0].record(stream)
-            served.launch(pos[a:b], ph[a:b], tt[a:b], views[i], stream=stream)
-            if record is not None:
-                record[i][1].record(stream)
+    # Served launches: the loop coalesces every queued request into one launch
+    # per free slot, so with the whole stream queued a step is one fused launch.
+    def coalesced(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        served.launch(pos, ph, tt, out, stream=stream, block_threads=threads)
+        if ev is not None:
+            ev[1].record(stream)
 
     for _ in range(max(args.warmup, 3)):
-        step()
+        coalesced()
     torch.cuda.synchronize(dev)
-    for v in views:
-        served.raise_for_status(v)
-
+    served.raise_for_status(out)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
-    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in slices] for _ in range(args.steps)]
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev = [_events(torch, 2) for _ in range(args.steps)]
     with ClockSampler(local_rank) as clocks:
         for k in range(args.steps):
             flush.fill_(k & 0xFF)  # write > L2 between timed steps (outside the events)
-            starts[k].record(stream)
-            step(ev[k])
-            ends[k].record(stream)
+            coalesced(ev[k])
         torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = float(sum(step_ms))
-    batch_ms = np.array([[s.elapsed_time(e) for s, e in row] for row in ev])
+    step_ms = np.array([a.elapsed_time(b) for a, b in ev])
+    total_ms = float(step_ms.sum())
     if world > 1:
         t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -253,11 +247,26 @@ def ours(args, rank, world, local_rank):
 
     # roofline of the fused kernel: algorithmic bytes = outputs written per (flash, OM)
     per_pair = 65 * 3 * 8 + 3 * 160 * 4 + 3 * 8 + 8 + 1
-    kernel_s = batch_ms.sum() / 1e3
-    achieved = per_pair * 48 * F * args.steps / kernel_s / 1e9
+    achieved = per_pair * 48 * F * args.steps / (step_ms.sum() / 1e3) / 1e9
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (
         ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
+
+    # one launch per request (no coalescing), same kernel
+    views = []
+    for a, b in requests:
+        v = {k: t[a:b] for k, t in out.items() if k != "status"}
+        v["status"] = torch.zeros(4, dtype=torch.int32, device=dev)
+        views.append(v)
+    pr_steps = min(args.steps, 20)
+    r0, r1 = _events(torch, 2)
+    r0.record(stream)
+    for _ in range(pr_steps):
+        for i, (a, b) in enumerate(requests):
+            served.launch(pos[a:b], ph[a:b], tt[a:b], views[i], stream=stream, block_threads=threads)
+    r1.record(stream)
+    torch.cuda.synchronize(dev)
+    per_request_value = F * pr_steps / (r0.elapsed_time(r1) / 1e3)
 
     # plain FP32 path, one launch per flash
     n_plain = min(512, F)
@@ -265,7 +274,7 @@ def ours(args, rank, world, local_rank):
     for i in range(8):
         plain.launch(pos[i:i + 1], ph[i:i + 1], tt[i:i + 1], pout, stream=stream)
     torch.cuda.synchronize(dev)
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0, p1 = _events(torch, 2)
     p0.record(stream)
     for i in range(n_plain):
         plain.launch(pos[i:i + 1], ph[i:i + 1], tt[i:i + 1], pout, stream=stream)
@@ -273,32 +282,31 @@ def ours(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     plain_value = n_plain / (p0.elapsed_time(p1) / 1e3)
 
-    # end to end through the public batch API from pinned host buffers
-    h_pos = torch.tensor(pos_np, dtype=torch.float64).pin_memory()
-    h_ph = torch.full((F,), 1e10, dtype=torch.float64).pin_memory()
-    h_t = torch.zeros(F, dtype=torch.float64).pin_memory()
-    h_out = {k: torch.empty(t.shape, dtype=t.dtype).pin_memory() for k, t in out.items()
-             if k != "status"}
-    d_pos, d_ph, d_t = torch.empty_like(pos), torch.empty_like(ph), torch.empty_like(tt)
+    # end to end: the serving loop (public API) from host arrays to host results,
+    # every response field copied back; all requests queued at once
+    cap = 2048
+    srv = FlashServer(served, ServeConfig(hbm_budget_bytes=2 * cap * flash_bytes(48, 65, 160),
+                                          slots=2, max_flashes_per_launch=cap,
+                                          block_threads=threads))
 
-    def e2e_step():
-        for i, (a, b) in enumerate(slices):
-            d_pos[a:b].copy_(h_pos[a:b], non_blocking=True)
-            d_ph[a:b].copy_(h_ph[a:b], non_blocking=True)
-            d_t[a:b].copy_(h_t[a:b], non_blocking=True)
-            served.launch(d_pos[a:b], d_ph[a:b], d_t[a:b], views[i], stream=stream)
-            for key, host in h_out.items():
-                host[a:b].copy_(views[i][key], non_blocking=True)
+    def serve_all():
+        for a, b in requests:
+            srv.submit(pos_np[a:b], 1e10)
+        srv.poll()
+        return srv.drain()
 
-    e2e_step()
+    serve_all()
+    srv.completed.clear()
+    e2e_steps = min(args.steps, 10)
+    e0, e1 = _events(torch, 2)
     torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_steps = min(args.steps, 20)
+    w0 = time.perf_counter()
     e0.record(stream)
     for _ in range(e2e_steps):
-        e2e_step()
+        serve_all()
     e1.record(stream)
     torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - w0
     e2e_ms = e0.elapsed_time(e1)
     if world > 1:
         t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
@@ -306,9 +314,28 @@ def ours(args, rank, world, local_rank):
         e2e_ms = float(t.item())
     e2e_value = world * F * e2e_steps / (e2e_ms / 1e3)
     h2d = F * (3 * 8 + 8 + 8)
-    d2h = sum(t.numel() * t.element_size() for t in h_out.values())
-    # every response field equals the device result (the copy is complete)
-    assert np.array_equal(h_out["origin"].numpy(), out["origin"].cpu().numpy())
+    d2h = F * 48 * per_pair
+    done = srv.completed
+    first = done[0]
+    assert first.result["charge"].shape == (requests[0][1] - requests[0][0], 48, 3)
+
+    # latency under Poisson arrivals at half the end-to-end capacity
+    srv.completed.clear()
+    offered = 0.5 * F * e2e_steps / wall
+    rng = np.random.default_rng(13)
+    mean_req = F / len(requests)
+    arrivals = np.cumsum(rng.exponential(mean_req / offered, size=len(requests) * 3))
+    order = [requests[i % len(requests)] for i in range(len(arrivals))]
+    t_start = time.perf_counter()
+    nxt = 0
+    while nxt < len(arrivals) or srv.queue or srv.busy:
+        now = time.perf_counter() - t_start
+        while nxt < len(arrivals) and arrivals[nxt] <= now:
+            a, b = order[nxt]
+            srv.submit(pos_np[a:b], 1e10, arrival=t_start + arrivals[nxt])
+            nxt += 1
+        srv.poll()
+    lat_ms = np.array([r.latency for r in srv.completed]) * 1e3
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -318,16 +345,20 @@ def ours(args, rank, world, local_rank):
                "sample": f"first {sample} flashes of the stream, float64 oracle restatement "
                          "of the reference route, one process"}
     if rank == 0:
-        lat = batch_ms.ravel()
         line = {
             "metric": METRIC, "value": value, "unit": "flashes/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3),
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 spectrum, split-bf16 readout (f32 accumulate), f64 clocks",
+            "vs_baseline": None,
+            "dtype": "f32 spectrum, split-bf16 readout (f32 accumulate), f64 clocks",
             "data": "synthetic", "config": config_json(sizes),
-            "latency": {"batch_device_ms_p50": float(np.percentile(lat, 50)),
-                        "batch_device_ms_p99": float(np.percentile(lat, 99)),
-                        "definition": "device time of one served batch (1-256 flashes)"},
+            "latency": {"p50_ms": float(np.percentile(lat_ms, 50)),
+                        "p99_ms": float(np.percentile(lat_ms, 99)),
+                        "offered_flashes_per_s": offered, "requests": len(lat_ms),
+                        "definition": "request arrival (Poisson, uneven 1-256 flash requests) to "
+                                      "every response field on the host, serving loop, 2 slots"},
+            "served_per_request_launch": {"value": per_request_value, "unit": "flashes/s",
+                                          "launches_per_step": len(requests)},
             "plain_fp32": {"value": plain_value, "unit": "flashes/s",
                            "launch": "one flash per launch (2 kernels), fp32 CUDA-core readout",
                            "sample": n_plain},
@@ -335,11 +366,14 @@ def ours(args, rank, world, local_rank):
             "roofline": {"kernel": "flash_tc_kernel", "bound": "hbm", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
-                         "algorithmic_bytes_per_pair": per_pair, "traffic": None},
+                         "algorithmic_bytes_per_pair": per_pair, "pairs_per_launch": 48 * F,
+                         "block_threads": threads, "traffic": None},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "flashes/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
-            "gpu_launches": len(slices) * args.steps,
+                    "d2h_bytes_per_step": d2h, "wall_s": wall, "steps": e2e_steps,
+                    "path": "FlashServer (serving loop): pinned staging, graph replay, D2H of "
+                            "every response field"},
+            "gpu_launches": args.steps,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

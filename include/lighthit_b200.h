@@ -112,6 +112,9 @@ typedef struct {
   double* origin;              /* [n_flash][n_om]                                  */
   uint8_t* active;             /* [n_flash][n_om] bit0 active, bit1 unsafe, bit2 coincident */
   int32_t* status;             /* [4]: flags, unsafe count, max unsafe radius (double bits) */
+  const int32_t* n_flash_device; /* optional: device count (<= n_flash) read by the kernel, so
+                                    one captured CUDA graph sized for n_flash serves any batch */
+  int32_t block_threads;       /* fused kernel CTA size: 0 (default 512), 256 or 512 */
 } lh_flash_batch;
 
 size_t lh_flash_workspace_bytes(const lh_flash_problem* p, const lh_readout_operator* op,

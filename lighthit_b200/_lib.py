@@ -40,7 +40,8 @@ class FlashProblem(C.Structure):
 class FlashBatch(C.Structure):
     _fields_ = [("n_flash", C.c_int32), ("pos", P), ("photons", P), ("time_ns", P),
                 ("spectrum", P), ("components", P), ("charge", P), ("origin", P),
-                ("active", P), ("status", P)]
+                ("active", P), ("status", P), ("n_flash_device", P),
+                ("block_threads", C.c_int32)]
 
 
 # name -> (restype, argtypes); every symbol the header declares

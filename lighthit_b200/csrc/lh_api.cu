@@ -149,7 +149,9 @@ int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op,
   if (smem > 227 * 1024) return LH_EUNSUPPORTED;
   cudaFuncSetAttribute(flash_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int grid = (int)(tiles < sm_count() ? tiles : sm_count());
-  flash_tc_kernel<<<grid, 256, smem, s>>>(*p, *b, reinterpret_cast<const __nv_bfloat16*>(op->b_hi),
+  const int threads = b->block_threads == 0 ? 512 : b->block_threads;
+  if (threads != 256 && threads != 512) return LH_EINVAL;
+  flash_tc_kernel<<<grid, threads, smem, s>>>(*p, *b, reinterpret_cast<const __nv_bfloat16*>(op->b_hi),
                                           reinterpret_cast<const __nv_bfloat16*>(op->b_lo),
                                           op->k_pad, op->n_bins, op->n_tile, passes_of(mode));
   return check_launch();

@@ -25,7 +25,8 @@ namespace lh {
 
 constexpr int kFlashPairs = 64;  // pairs per tile -> 128 readout rows
 constexpr int kMaxAcc = 8;       // highest acceptance degree handled
-constexpr int kFlashThreads = 256;
+constexpr int kFlashThreads = 256;    // plain path
+constexpr int kFlashTcThreads = 512;  // fused path: 16 warps hide the table-load latency
 
 struct FlashPair {
   double origin;  // time_origin_ns of the OM for this flash
@@ -43,6 +44,15 @@ struct FlashPair {
   float w[kMaxAcc + 1];  // alpha_l P_l(cos) / (4 pi)
   float charge[3];
 };
+
+// Flashes in this launch: the device count when given (graph replay), else n_flash.
+LH_DEVICE int flash_count(const lh_flash_batch& b) {
+  if (b.n_flash_device) {
+    const int n = *b.n_flash_device;
+    return n < 0 ? 0 : (n > b.n_flash ? b.n_flash : n);
+  }
+  return b.n_flash;
+}
 
 // Step 1 for one pair.
 LH_DEVICE void flash_pair_setup(const lh_flash_problem& p, const lh_flash_batch& b, int64_t pair,
@@ -161,8 +171,8 @@ LH_DEVICE void flash_item(const lh_flash_problem& p, const lh_flash_batch& b, in
     s2.x *= s.amp12; s2.y *= s.amp12;
   }
   const float2 e12 = phase(om, s.t12);
-  const float2 e0 = phase(om, s.t0);
-  const float2 r12 = phase(om, s.t12 - s.origin);
+  const float2 e0 = (s.t0 == s.t12) ? e12 : phase(om, s.t0);
+  const float2 r12 = s.j >= 0 ? phase(om, s.t12 - s.origin) : make_float2(1.f, 0.f);
   const float2 o0 = make_float2(s.amp0 * e0.x, s.amp0 * e0.y);
   const float2 o1 = cmul(s1, e12), o2 = cmul(s2, e12);
   if (s.valid) {
@@ -183,11 +193,24 @@ LH_DEVICE void flash_item(const lh_flash_problem& p, const lh_flash_batch& b, in
 // Step 3 (order 0 and the mask) for the tile's pairs.
 LH_DEVICE void flash_tile_order0(const lh_flash_problem& p, const lh_flash_batch& b,
                                  const FlashPair* sp, int64_t base, int n_bins) {
-  for (int i = threadIdx.x; i < kFlashPairs * n_bins; i += blockDim.x) {
-    const int lp = i / n_bins, bin = i % n_bins;
-    const FlashPair& s = sp[lp];
-    if (!s.valid) continue;
-    b.components[((base + lp) * 3) * n_bins + bin] = (bin == s.bin0) ? (float)s.q0 : 0.f;
+  if ((n_bins & 3) == 0) {  // rows are 16-byte aligned: four bins per store
+    const int quads = n_bins >> 2;
+    for (int i = threadIdx.x; i < kFlashPairs * quads; i += blockDim.x) {
+      const int lp = i / quads, bin = (i % quads) * 4;
+      const FlashPair& s = sp[lp];
+      if (!s.valid) continue;
+      const float q = (float)s.q0;
+      const float4 v = make_float4(bin == s.bin0 ? q : 0.f, bin + 1 == s.bin0 ? q : 0.f,
+                                   bin + 2 == s.bin0 ? q : 0.f, bin + 3 == s.bin0 ? q : 0.f);
+      *reinterpret_cast<float4*>(b.components + ((base + lp) * 3) * n_bins + bin) = v;
+    }
+  } else {
+    for (int i = threadIdx.x; i < kFlashPairs * n_bins; i += blockDim.x) {
+      const int lp = i / n_bins, bin = i % n_bins;
+      const FlashPair& s = sp[lp];
+      if (!s.valid) continue;
+      b.components[((base + lp) * 3) * n_bins + bin] = (bin == s.bin0) ? (float)s.q0 : 0.f;
+    }
   }
   if (threadIdx.x < kFlashPairs) {
     const FlashPair& s = sp[threadIdx.x];
@@ -227,7 +250,7 @@ LH_DEVICE void flash_tile_setup(const lh_flash_problem& p, const lh_flash_batch&
 __global__ void __launch_bounds__(kFlashThreads)
 flash_plain_kernel(lh_flash_problem p, lh_flash_batch b, int kpad, int n_bins, float* a_rows) {
   __shared__ FlashPair sp[kFlashPairs];
-  const int64_t n_pairs = (int64_t)b.n_flash * p.n_om;
+  const int64_t n_pairs = (int64_t)flash_count(b) * p.n_om;
   const int64_t base = (int64_t)blockIdx.x * kFlashPairs;
   flash_tile_setup(p, b, sp, base, n_pairs);
   __syncthreads();
@@ -258,7 +281,7 @@ flash_plain_kernel(lh_flash_problem p, lh_flash_batch b, int kpad, int n_bins, f
 // hi and lo parts) is loaded once per CTA. Per tile: setup -> spectrum items
 // writing A (bf16 hi/lo) into shared memory -> one thread issues the MMAs ->
 // order-0 rows and mask while the tensor core runs -> TMEM drain.
-__global__ void __launch_bounds__(kFlashThreads, 1)
+__global__ void __launch_bounds__(kFlashTcThreads, 1)
 flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __restrict__ g_bhi,
                 const __nv_bfloat16* __restrict__ g_blo, int kpad, int n_bins, int n_tile,
                 int passes) {
@@ -296,7 +319,7 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
     if (need_lo_b) bulk_g2s(s_blo, g_blo, b_bytes, bar_b);
   }
   const uint32_t idesc = instr_desc_bf16_f32(128, n_tile);
-  const int64_t n_pairs = (int64_t)b.n_flash * p.n_om;
+  const int64_t n_pairs = (int64_t)flash_count(b) * p.n_om;
   const int64_t n_tiles = (n_pairs + kFlashPairs - 1) / kFlashPairs;
   const int nw = p.n_omega;
   const int padw = kpad - 2 * nw;
@@ -362,22 +385,31 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
     ph_mma ^= 1u;
     if (__syncthreads_or(!ok)) { failed = true; mma_pending = true; break; }
     tc_fence_after();
-    // drain: warp w reads TMEM lanes 32*(w%4).. (rows), half (w/4) of the columns
-    const int q = warp & 3, h = warp >> 2;
+    // drain: warp w reads TMEM lanes 32*(w%4).. (rows); the warps with the same
+    // lane quarter split the 16-column chunks between them
+    const int q = warp & 3, h = warp >> 2, groups = (int)blockDim.x / 128;
     const int row = q * 32 + lane;
     const int lp = row >> 1, order = 1 + (row & 1);
     const bool valid = sp[lp].valid;
     const int chunks = n_tile / 16;
-    const int c_begin = h * ((chunks + 1) / 2), c_end = min(chunks, (h + 1) * ((chunks + 1) / 2));
+    const int per = (chunks + groups - 1) / groups;
+    const int c_begin = h * per, c_end = min(chunks, (h + 1) * per);
     const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
     float* dst = b.components + ((base + lp) * 3 + order) * (int64_t)n_bins;
+    const bool vec = (n_bins & 3) == 0;
     for (int c = c_begin; c < c_end; ++c) {
       float v[16];
       tmem_ld16(lane_addr + (uint32_t)(c * 16), v);
       if (valid) {
+        if (vec && c * 16 + 16 <= n_bins) {
+          float4* d4 = reinterpret_cast<float4*>(dst + c * 16);
 #pragma unroll
-        for (int i = 0; i < 16; ++i)
-          if (c * 16 + i < n_bins) dst[c * 16 + i] = v[i];
+          for (int i = 0; i < 4; ++i) d4[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            if (c * 16 + i < n_bins) dst[c * 16 + i] = v[i];
+        }
       }
     }
     tc_fence_before();

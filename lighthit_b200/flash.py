@@ -156,9 +156,12 @@ class FlashTransport:
         m = _lib.MODES[mode or self.mode]
         return int(lib.lh_flash_workspace_bytes(self.problem, self.readout.struct, m, int(n_flash)))
 
-    def launch(self, pos, photons, time_ns, out, *, mode=None, stream=None, workspace=None):
+    def launch(self, pos, photons, time_ns, out, *, mode=None, stream=None, workspace=None,
+               n_device=None, block_threads=0):
         """Enqueue one batch. ``pos`` (F,3), ``photons`` (F,), ``time_ns`` (F,) are
-        float64 device tensors; ``out`` comes from :meth:`allocate`. Nothing syncs."""
+        float64 device tensors; ``out`` comes from :meth:`allocate`. ``n_device``
+        (int32 device scalar) makes the kernel read the flash count on the device,
+        as a captured graph replayed for varying batch sizes needs. Nothing syncs."""
         import torch
         lib = _lib.load()
         m = _lib.MODES[mode or self.mode]
@@ -171,7 +174,8 @@ class FlashTransport:
         batch = _lib.FlashBatch(
             F, pos.data_ptr(), photons.data_ptr(), time_ns.data_ptr(),
             out["spectrum"].data_ptr(), out["components"].data_ptr(), out["charge"].data_ptr(),
-            out["origin"].data_ptr(), out["active"].data_ptr(), out["status"].data_ptr())
+            out["origin"].data_ptr(), out["active"].data_ptr(), out["status"].data_ptr(),
+            n_device.data_ptr() if n_device is not None else None, int(block_threads))
         s = _lib.stream_ptr(stream or torch.cuda.current_stream(self.device))
         ws_ptr = workspace.data_ptr() if workspace is not None else None
         ws_bytes = workspace.numel() if workspace is not None else 0
