@@ -125,20 +125,20 @@ class FlashServer:
                 used += count
             self.backend.stage(slot, [(r.positions[s:s + c], r.photons[s:s + c],
                                        r.time_ns[s:s + c], off) for r, s, c, off in items], used)
-            self.backend.launch(slot, used)
+            self.backend.launch(slot, used, [(off, c) for _, _, c, off in items])
             self.busy[slot] = items
             self.launches += 1
         return finished
 
     def _finish(self, slot):
         items = self.busy.pop(slot)
-        out = self.backend.collect(slot)
+        outs = self.backend.collect(slot)  # one dict of host arrays per admitted chunk
         self.free.append(slot)
         now = time.perf_counter()
         done = []
-        for req, start, count, off in items:
-            req._parts.append((start, {k: out[k][off:off + count] for k in RESULT_KEYS}))
-            flags = out["active"][off:off + count] >> 1
+        for (req, start, count, off), part in zip(items, outs):
+            req._parts.append((start, part))
+            flags = part["active"] >> 1
             if np.any(flags) and req.error is None:
                 bad = int(np.flatnonzero(np.any(flags, axis=1))[0]) + start
                 req.error = ("isotropic point source cannot coincide with an OM centre"
@@ -148,7 +148,8 @@ class FlashServer:
             req._pending -= 1
             if req._pending == 0:
                 parts = sorted(req._parts, key=lambda p: p[0])
-                req.result = {k: np.concatenate([p[1][k] for p in parts]) for k in RESULT_KEYS}
+                req.result = (dict(parts[0][1]) if len(parts) == 1 else
+                              {k: np.concatenate([p[1][k] for p in parts]) for k in RESULT_KEYS})
                 req.result["active"] = (req.result["active"] & 1).astype(bool)
                 req._parts = []
                 req.done = now
@@ -195,9 +196,8 @@ class CudaFlashBackend:
             s["d_t"] = torch.zeros(cap, dtype=torch.float64, device=dev)
             s["d_n"] = torch.zeros(1, dtype=torch.int32, device=dev)
             s["out"] = transport.allocate(cap)
-            s["h_out"] = {k: torch.empty(s["out"][k].shape, dtype=s["out"][k].dtype).pin_memory()
-                          for k in RESULT_KEYS}
             s["graph"] = None
+            s["parts"] = None
             s["count"] = 0
             self.slots.append(s)
         for i in range(self.n_slots):
@@ -235,7 +235,10 @@ class CudaFlashBackend:
         s["h_n"][0] = used
         s["count"] = used
 
-    def launch(self, slot, used):
+    def launch(self, slot, used, chunks):
+        """Replay the slot's graph, then copy each chunk's results straight into
+        its own pinned host buffers (torch's caching host allocator), so results
+        outlive the slot without any host-side copy."""
         torch = self.torch
         s = self.slots[slot]
         with torch.cuda.stream(s["stream"]):
@@ -243,8 +246,17 @@ class CudaFlashBackend:
                 s["graph"].replay()
             else:
                 self._body(s)
-            for k in RESULT_KEYS:
-                s["h_out"][k][:used].copy_(s["out"][k][:used], non_blocking=True)
+            parts = []
+            for off, count in chunks:
+                part = {}
+                for k in RESULT_KEYS:
+                    src = s["out"][k][off:off + count]
+                    part[k] = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+                    part[k].copy_(src, non_blocking=True)
+                parts.append(part)
+            s["status_host"] = torch.empty(4, dtype=torch.int32, pin_memory=True)
+            s["status_host"].copy_(s["out"]["status"], non_blocking=True)
+            s["parts"] = parts
             s["event"].record(s["stream"])
 
     def ready(self, slot):
@@ -253,11 +265,10 @@ class CudaFlashBackend:
     def collect(self, slot):
         s = self.slots[slot]
         s["event"].synchronize()
-        status = s["out"]["status"].cpu().numpy()
-        if int(status[0]) & _lib.LH_STATUS_TIMEOUT:
+        if int(s["status_host"][0]) & _lib.LH_STATUS_TIMEOUT:
             raise RuntimeError("a tensor-core pipeline wait timed out on the device")
-        n = s["count"]
-        return {k: s["h_out"][k][:n].numpy().copy() for k in RESULT_KEYS}
+        parts, s["parts"] = s["parts"], None
+        return [{k: t.numpy() for k, t in part.items()} for part in parts]
 
 
 def autotune(transport, n_flash, *, cache=None, candidates=(256, 512), repeats=5):

@@ -23,9 +23,11 @@ class FakeBackend:
             buf[off:off + len(pos), 4] = tt
         self.staged[slot] = buf
 
-    def launch(self, slot, used):
+    def launch(self, slot, used, chunks):
         self.launch_sizes.append(used)
         self.clock[slot] = self.delay
+        self.chunks = getattr(self, "chunks", {})
+        self.chunks[slot] = chunks
 
     def ready(self, slot):
         self.clock[slot] -= 1
@@ -37,8 +39,9 @@ class FakeBackend:
         charge = buf[:, 3:4, None] * np.arange(1, self.n_om + 1)[None, :, None] * np.ones(3)
         active = np.ones((n, self.n_om), np.uint8)
         active[buf[:, 3] < 0] |= 2  # a negative photon count plays an unsafe flash
-        return dict(spectrum=np.repeat(buf[:, None, :3], self.n_om, 1), components=buf[:, None, :],
-                    charge=charge, origin=buf[:, 4:5] + np.zeros(self.n_om), active=active)
+        out = dict(spectrum=np.repeat(buf[:, None, :3], self.n_om, 1), components=buf[:, None, :],
+                   charge=charge, origin=buf[:, 4:5] + np.zeros(self.n_om), active=active)
+        return [{k: v[off:off + count] for k, v in out.items()} for off, count in self.chunks[slot]]
 
 
 def test_requests_split_batched_and_reassembled_in_order():
