@@ -124,6 +124,55 @@ int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op,
                        const lh_flash_batch* b, void* workspace, size_t workspace_bytes,
                        void* stream);
 
+/* ------------------------------------------------------------------ order >= 2
+ * Replaces apply_folded -> apply_multi_spectral -> _apply_multi_spectral
+ * (shower/ge2.py:99-119, _shower_basis.py:894-1198): node-band axial sources
+ * sharing one point set, contracted with the band-folded RTE kernels. Points,
+ * receivers and looks are in the source's axis frame (as apply_multi_spectral
+ * rotates them); channels are already aligned to the earliest band reference.
+ */
+typedef struct {
+  int32_t n_bands;             /* folded node bands                                   */
+  int32_t n_intervals;         /* radial intervals (log-r knots - 1)                  */
+  int32_t degree;              /* kernel degree L (<= 16)                             */
+  int32_t acc_degree;          /* detector (acceptance) degree A (<= 4)               */
+  int32_t max_m;               /* azimuthal degree min(source M, L) (<= 4)            */
+  int32_t n_pairs;             /* detector pairs (<= 8)                               */
+  int32_t nch;                 /* kept source channels sum_l (2 min(l, M) + 1)         */
+  int32_t n_omega;             /* frequencies of the table (stride of coef)          */
+  const float* coef;           /* complex64 [band][interval][l][pair][4][n_omega]     */
+  const double* log_r;         /* [n_intervals + 1]                                   */
+  const double* absorption;    /* [band] 1/m                                          */
+  const double* speed;         /* [band] m/ns                                         */
+  const double* omega;         /* [n_omega] rad/ns                                    */
+  const int32_t* pair_lambda;  /* [n_pairs]                                           */
+  const int32_t* pair_mu;      /* [n_pairs]                                           */
+  const double* alpha;         /* [acc_degree + 1] acceptance Legendre coefficients   */
+  const int32_t* starts;       /* [degree + 2] first kept channel of each source l    */
+  const double* start_norm;    /* [(jmax + 1) (2 jmax + 1)] sqrt(binom(2j, j - nu))    */
+  int32_t jmax;                /* max(max_m, acc_degree)                              */
+  int32_t flight;              /* table phase is the flight phase                     */
+} lh_ge2_table;
+
+typedef struct {
+  int32_t n_points;
+  const double* points;        /* [n_points][3] axis frame                            */
+  const float* channels;       /* complex64 [band][n_points][nch][n_omega_channels]   */
+  int32_t n_omega_channels;    /* frequencies stored per channel (1 at zero frequency) */
+  int32_t n_omega;             /* frequencies computed: the first n_omega of the table */
+  int32_t n_om;
+  const double* receivers;     /* [n_om][3] axis frame                                */
+  const double* looks;         /* [n_om][3] axis frame                                */
+  const double* out_scale;     /* [band][n_om] detector scale (effective area)        */
+  double radial_low, radial_high; /* radial window m                                  */
+  double reference_ns;         /* emission-time reference of the aligned channels     */
+  double* result;              /* complex128 [n_om][n_omega]                          */
+} lh_ge2_problem;
+
+size_t lh_ge2_workspace_bytes(const lh_ge2_table* t, const lh_ge2_problem* p);
+int lh_ge2_apply(const lh_ge2_table* t, const lh_ge2_problem* p, void* workspace,
+                 size_t workspace_bytes, void* stream);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

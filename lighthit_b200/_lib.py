@@ -44,6 +44,22 @@ class FlashBatch(C.Structure):
                 ("block_threads", C.c_int32)]
 
 
+class Ge2Table(C.Structure):
+    _fields_ = [("n_bands", C.c_int32), ("n_intervals", C.c_int32), ("degree", C.c_int32),
+                ("acc_degree", C.c_int32), ("max_m", C.c_int32), ("n_pairs", C.c_int32),
+                ("nch", C.c_int32), ("n_omega", C.c_int32), ("coef", P), ("log_r", P),
+                ("absorption", P), ("speed", P), ("omega", P), ("pair_lambda", P),
+                ("pair_mu", P), ("alpha", P), ("starts", P), ("start_norm", P),
+                ("jmax", C.c_int32), ("flight", C.c_int32)]
+
+
+class Ge2Problem(C.Structure):
+    _fields_ = [("n_points", C.c_int32), ("points", P), ("channels", P),
+                ("n_omega_channels", C.c_int32), ("n_omega", C.c_int32), ("n_om", C.c_int32),
+                ("receivers", P), ("looks", P), ("out_scale", P), ("radial_low", C.c_double),
+                ("radial_high", C.c_double), ("reference_ns", C.c_double), ("result", P)]
+
+
 # name -> (restype, argtypes); every symbol the header declares
 SIGNATURES = {
     "lh_version": (C.c_char_p, []),
@@ -58,6 +74,8 @@ SIGNATURES = {
                                      C.POINTER(FlashBatch), P, C.c_size_t, P]),
     "lh_flash_transport_noalloc": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(ReadoutOperator),
                                              C.POINTER(FlashBatch), P]),
+    "lh_ge2_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem)]),
+    "lh_ge2_apply": (C.c_int, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem), P, C.c_size_t, P]),
 }
 LH_ESCRATCH = 6
 

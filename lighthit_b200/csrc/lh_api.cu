@@ -158,3 +158,47 @@ int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op,
 }
 
 }  // extern "C"
+
+namespace lh {
+size_t ge2_workspace(const lh_ge2_table& T, const lh_ge2_problem& P);
+int ge2_launch(const lh_ge2_table& T, const lh_ge2_problem& P, void* ws, cudaStream_t s);
+}  // namespace lh
+
+namespace {
+bool ge2_valid(const lh_ge2_table* t, const lh_ge2_problem* p) {
+  if (!t || !p) return false;
+  if (t->n_bands < 1 || t->n_intervals < 1 || t->degree < 0 || t->degree > 16 ||
+      t->acc_degree < 0 || t->acc_degree > 4 || t->max_m < 0 || t->max_m > 4 ||
+      t->max_m > t->degree || t->n_pairs < 1 || t->n_pairs > 8 || t->nch < 1 ||
+      t->n_omega < 1 || t->jmax < t->max_m || t->jmax < t->acc_degree)
+    return false;
+  if (!t->coef || !t->log_r || !t->absorption || !t->speed || !t->omega || !t->pair_lambda ||
+      !t->pair_mu || !t->alpha || !t->starts || !t->start_norm)
+    return false;
+  if (p->n_points < 0 || p->n_om < 0 || p->n_omega < 1 || p->n_omega > t->n_omega ||
+      p->n_omega_channels < p->n_omega || !p->result)
+    return false;
+  if (p->n_points && (!p->points || !p->channels)) return false;
+  if (p->n_om && (!p->receivers || !p->looks || !p->out_scale)) return false;
+  if ((size_t)t->nch * t->n_pairs * 32 * sizeof(float) > 200 * 1024) return false;
+  return true;
+}
+}  // namespace
+
+extern "C" size_t lh_ge2_workspace_bytes(const lh_ge2_table* t, const lh_ge2_problem* p) {
+  if (!ge2_valid(t, p)) return 0;
+  return lh::ge2_workspace(*t, *p);
+}
+
+extern "C" int lh_ge2_apply(const lh_ge2_table* t, const lh_ge2_problem* p, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+  if (!ge2_valid(t, p)) return LH_EINVAL;
+  if (p->n_om == 0) return LH_OK;
+  if (!workspace || workspace_bytes < lh::ge2_workspace(*t, *p)) return LH_ENOMEM;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->n_points == 0) {
+    cudaMemsetAsync(p->result, 0, (size_t)p->n_om * p->n_omega * 2 * sizeof(double), s);
+    return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+  }
+  return lh::ge2_launch(*t, *p, workspace, s);
+}

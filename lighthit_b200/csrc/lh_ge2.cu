@@ -1,0 +1,335 @@
+// Order >=2: contraction of axial-basis source moments with band-folded RTE
+// kernels (reference _shower_basis.py:894-1050, apply_multi_spectral
+// :1126-1198, shower/ge2.py:99-119).
+//
+// For an OM d and a basis point c at distance r (interval j of the log-r
+// grid, offset t) the reference sums, per band lambda and frequency w,
+//
+//   N_d(w) += s_lambda(r) e^{i w r / v_lambda}
+//             sum_l sum_a rot_l[a](w) * sum_p D_p[a] cubic_{lambda j l p}(t, w),
+//   rot_l[a](w) = sum_b erow_l[a][b] ch_lambda[c][l, b](w).
+//
+// Exchanging the sums over a and b gives
+//
+//   N_d(w) += s e^{i w r/v} sum_l sum_b ch[c][l,b](w) sum_p F_l[b][p] cubic_{j l p}(t, w),
+//   F_l[b][p] = sum_a erow_l[a][b] D_p[a],
+//
+// where F (nch x pairs real numbers per (d, c)) carries all the geometry:
+// Wigner small-d rotation, azimuthal rotation, detector harmonics and the
+// acceptance coefficients. ge2_geometry_kernel forms F in float64 once per
+// (d, c); ge2_apply_kernel runs the float32 contraction with one thread per
+// (band, frequency); ge2_reduce_kernel sums the point chunks in a fixed order
+// (identical results alone or in a batch) and applies the emission-time phase.
+#include "lh_common.cuh"
+
+namespace lh {
+
+constexpr int kGe2Degree = 16;   // source/kernel degree bound
+constexpr int kGe2Out = 4;       // acceptance (detector) degree bound
+constexpr int kGe2M = 4;         // azimuthal degree bound
+constexpr int kGe2Chunk = 32;    // points per partial sum
+
+LH_DEVICE double par(int n) { return (n & 1) ? -1.0 : 1.0; }
+
+// d^j_(mu nu) at j = max(|mu|, |nu|)  (_directional_numba.py:37-48)
+LH_DEVICE double wigner_start(int j, int mu, int nu, double hc, double hs, const double* norm,
+                              int jmax) {
+  double sign = 1.0;
+  if (abs(nu) == j && abs(mu) != j) {
+    int t = mu; mu = nu; nu = t;
+    sign *= par(mu - nu);
+  }
+  if (mu == -j) {
+    mu = j;
+    nu = -nu;
+    sign *= par(j + nu);
+  }
+  double v = sign * norm[j * (2 * jmax + 1) + nu + jmax];
+  for (int k = 0; k < j + nu; ++k) v *= hc;
+  for (int k = 0; k < j - nu; ++k) v *= -hs;
+  return v;
+}
+
+// Real orthonormal harmonics up to degree A of (x, y, z), flat l*l+l+m (:90-128)
+LH_DEVICE void real_harmonics(double x, double y, double z, int A, double* out) {
+  const double radius = sqrt(x * x + y * y + z * z);
+  const double mu = z / radius;
+  const double tr = sqrt(x * x + y * y);
+  const double sine = tr / radius;
+  const double cp = tr == 0.0 ? 1.0 : x / tr;
+  const double sp = tr == 0.0 ? 0.0 : y / tr;
+  double cm = 1.0, sm = 0.0, diag = 1.0 / sqrt(4 * kPi), v0 = 0.0, v1 = 0.0;
+  for (int m = 0; m <= A; ++m) {
+    if (m) {
+      diag *= sqrt((2.0 * m + 1) / (2.0 * m)) * sine;
+      const double c2 = cm * cp - sm * sp, s2 = sm * cp + cm * sp;
+      cm = c2;
+      sm = s2;
+    }
+    v0 = diag;
+    for (int l = m; l <= A; ++l) {
+      double value;
+      if (l == m) value = v0;
+      else if (l == m + 1) {
+        value = sqrt(2.0 * m + 3) * mu * v0;
+        v1 = value;
+      } else {
+        const double aa = sqrt((4.0 * l * l - 1) / (double)(l * l - m * m));
+        const double bb = sqrt(((2.0 * l + 1) * ((l - 1) * (l - 1) - m * m)) /
+                               ((2.0 * l - 3) * (double)(l * l - m * m)));
+        value = aa * mu * v1 - bb * v0;
+        v0 = v1;
+        v1 = value;
+      }
+      const int c = l * l + l;
+      if (m == 0) out[c] = value;
+      else {
+        out[c - m] = sqrt(2.0) * value * sm;
+        out[c + m] = sqrt(2.0) * value * cm;
+      }
+    }
+  }
+}
+
+// One thread per (OM, point): radius, interval, band scales and F.
+__global__ void ge2_geometry_kernel(lh_ge2_table T, lh_ge2_problem P, int* g_j, float* g_t,
+                                    double* g_r, float* g_scale, float* g_F) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t total = (int64_t)P.n_om * P.n_points;
+  if (idx >= total) return;
+  const int d = (int)(idx / P.n_points), c = (int)(idx % P.n_points);
+  const double dx = P.receivers[3 * d] - P.points[3 * c];
+  const double dy = P.receivers[3 * d + 1] - P.points[3 * c + 1];
+  const double dz = P.receivers[3 * d + 2] - P.points[3 * c + 2];
+  const double radius = sqrt(dx * dx + dy * dy + dz * dz);
+  g_r[idx] = radius;
+  if (!(radius >= P.radial_low && radius <= P.radial_high)) {
+    g_j[idx] = -1;
+    return;
+  }
+  const int L = T.degree, A = T.acc_degree, M = T.max_m, W = 2 * A + 1, NP = T.n_pairs;
+  double cosine = dz / radius;
+  cosine = cosine > 1.0 ? 1.0 : (cosine < -1.0 ? -1.0 : cosine);
+  const double phi = atan2(dy, dx);
+  const double tr = sqrt(dx * dx + dy * dy);
+  const double sine = tr / radius;
+  const double cp = tr == 0.0 ? 1.0 : dx / tr;
+  const double sp = tr == 0.0 ? 0.0 : dy / tr;
+  double cosn[kGe2M + 1], sinn[kGe2M + 1];
+  for (int n = 0; n <= M; ++n) {
+    cosn[n] = cos(n * phi);
+    sinn[n] = sin(n * phi);
+  }
+  const double lx = P.looks[3 * d], ly = P.looks[3 * d + 1], lz = P.looks[3 * d + 2];
+  const double a1 = cosine * cp * lx + cosine * sp * ly - sine * lz;
+  const double a2 = -sp * lx + cp * ly;
+  const double a3 = sine * cp * lx + sine * sp * ly + cosine * lz;
+  double det[(kGe2Out + 1) * (kGe2Out + 1)];
+  real_harmonics(a1, a2, a3, A, det);
+  // pair weights D_p[a]: alpha_lam Y[lam, +mu] at a = A + mu, alpha Y[lam, -mu] at A - mu
+  // Wigner d^l_(mu nu): wig[l][nu + A][mu], mu = 0..M, by recurrence in l (:51-87)
+  double wig[kGe2Degree + 1][2 * kGe2Out + 1][kGe2M + 1];
+  for (int l = 0; l <= L; ++l)
+    for (int a = 0; a < W; ++a)
+      for (int m = 0; m <= M; ++m) wig[l][a][m] = 0.0;
+  const double hc = sqrt((1.0 + cosine) / 2.0), hs = sqrt((1.0 - cosine) / 2.0);
+  for (int nu = -A; nu <= A; ++nu) {
+    for (int mu = 0; mu <= M; ++mu) {
+      const int start = abs(nu) > mu ? abs(nu) : mu;
+      if (start > L) continue;
+      double prev = 0.0, cur = wigner_start(start, mu, nu, hc, hs, T.start_norm, T.jmax);
+      wig[start][nu + A][mu] = cur;
+      for (int l = start; l < L; ++l) {
+        double value;
+        if (l == 0) value = cosine * cur;
+        else {
+          double lower = (double)(l * l - mu * mu) * (double)(l * l - nu * nu);
+          lower = lower > 0.0 ? sqrt(lower) : 0.0;
+          const double upper = sqrt((double)((l + 1) * (l + 1) - mu * mu) *
+                                    (double)((l + 1) * (l + 1) - nu * nu));
+          value = ((2 * l + 1) * (l * (l + 1) * cosine - mu * nu) * cur - (l + 1) * lower * prev) /
+                  (l * upper);
+        }
+        prev = cur;
+        cur = value;
+        wig[l + 1][nu + A][mu] = cur;
+      }
+    }
+  }
+  // F_l[b][p] for every kept source channel (row = starts[l] + (b - M + keep))
+  float* F = g_F + idx * (int64_t)T.nch * NP;
+  const double root2 = sqrt(2.0);
+  for (int l = 0; l <= L; ++l) {
+    double erow[2 * kGe2Out + 1][2 * kGe2M + 1];
+    for (int a = 0; a < W; ++a)
+      for (int b = 0; b <= 2 * M; ++b) erow[a][b] = 0.0;
+    erow[A][M] = wig[l][A][0];
+    const int top_n = l < M ? l : M, top_p = l < A ? l : A;
+    for (int n = 1; n <= top_n; ++n) {
+      const double base = root2 * par(n) * wig[l][A][n];
+      erow[A][M + n] = base * cosn[n];
+      erow[A][M - n] = base * sinn[n];
+    }
+    for (int pp = 1; pp <= top_p; ++pp) {
+      erow[A + pp][M] = root2 * par(pp) * wig[l][A + pp][0];
+      for (int n = 1; n <= top_n; ++n) {
+        const double cross = par(pp) * wig[l][A + pp][n];
+        const double straight = wig[l][A - pp][n];
+        const double cc = par(n) * (cross + straight), ss = par(n) * (cross - straight);
+        erow[A + pp][M + n] = cc * cosn[n];
+        erow[A + pp][M - n] = cc * sinn[n];
+        erow[A - pp][M + n] = -ss * sinn[n];
+        erow[A - pp][M - n] = ss * cosn[n];
+      }
+    }
+    const int keep = top_n;
+    for (int b = M - keep; b <= M + keep; ++b) {
+      const int row = T.starts[l] + keep + (b - M);
+      for (int p = 0; p < NP; ++p) {
+        const int lam = T.pair_lambda[p], mup = T.pair_mu[p];
+        double f = 0.0;
+        if (mup <= top_p) {
+          const int cidx = lam * lam + lam;
+          const double pos = T.alpha[lam] * det[cidx + mup];
+          const double neg = mup ? T.alpha[lam] * det[cidx - mup] : 0.0;
+          if (neg != 0.0) f += erow[A - mup][b] * neg;
+          if (pos != 0.0) f += erow[A + mup][b] * pos;
+        }
+        F[row * NP + p] = (float)f;
+      }
+    }
+  }
+  const double logr = log(radius);
+  int j = bin_right(T.log_r, T.n_intervals + 1, logr);
+  j = j < 0 ? 0 : (j > T.n_intervals - 1 ? T.n_intervals - 1 : j);
+  g_j[idx] = j;
+  g_t[idx] = (float)(logr - T.log_r[j]);
+  for (int lam = 0; lam < T.n_bands; ++lam)
+    g_scale[(int64_t)lam * total + idx] =
+        (float)(P.out_scale[(int64_t)lam * P.n_om + d] * exp(-T.absorption[lam] * radius) /
+                (4 * kPi * radius * radius));
+}
+
+// Grid (OM, point chunk); thread = (band, frequency). Partial sums per chunk.
+__global__ void ge2_apply_kernel(lh_ge2_table T, lh_ge2_problem P, const int* g_j,
+                                 const float* g_t, const double* g_r, const float* g_scale,
+                                 const float* g_F, double2* partial) {
+  extern __shared__ float s_F[];  // [kGe2Chunk][nch*NP] for the chunk's points
+  const int d = blockIdx.x, chunk = blockIdx.y;
+  const int c0 = chunk * kGe2Chunk;
+  const int c1 = min(P.n_points, c0 + kGe2Chunk);
+  const int NP = T.n_pairs, nch = T.nch, Wn = P.n_omega;
+  const int64_t total = (int64_t)P.n_om * P.n_points;
+  const int64_t base = (int64_t)d * P.n_points;
+  const int fsz = nch * NP;
+  for (int i = threadIdx.x; i < (c1 - c0) * fsz; i += blockDim.x)
+    s_F[i] = g_F[(base + c0) * fsz + i];
+  __syncthreads();
+  const int items = T.n_bands * Wn;
+  for (int item = threadIdx.x; item < items; item += blockDim.x) {
+    const int lam = item / Wn, w = item % Wn;
+    const double om = T.omega[w];
+    float acc_re = 0.f, acc_im = 0.f;
+    for (int c = c0; c < c1; ++c) {
+      const int64_t idx = base + c;
+      const int j = g_j[idx];
+      if (j < 0) continue;
+      const float t = g_t[idx];
+      const float* F = s_F + (c - c0) * fsz;
+      const float2* ch = reinterpret_cast<const float2*>(P.channels) +
+                         (((int64_t)lam * P.n_points + c) * nch) * P.n_omega_channels;
+      float pr = 0.f, pi = 0.f;
+      for (int l = 0; l <= T.degree; ++l) {
+        // radial cubic of every pair at (lam, j, l, w)
+        float rr[8], ri[8];
+        const float2* cf = reinterpret_cast<const float2*>(T.coef) +
+                           ((((int64_t)lam * T.n_intervals + j) * (T.degree + 1) + l) * NP * 4) *
+                               T.n_omega + w;
+        for (int p = 0; p < NP; ++p) {
+          const float2 k0 = cf[(p * 4 + 0) * T.n_omega], k1 = cf[(p * 4 + 1) * T.n_omega];
+          const float2 k2 = cf[(p * 4 + 2) * T.n_omega], k3 = cf[(p * 4 + 3) * T.n_omega];
+          rr[p] = fmaf(fmaf(fmaf(k0.x, t, k1.x), t, k2.x), t, k3.x);
+          ri[p] = fmaf(fmaf(fmaf(k0.y, t, k1.y), t, k2.y), t, k3.y);
+        }
+        const int keep = l < T.max_m ? l : T.max_m;
+        for (int row = T.starts[l]; row < T.starts[l] + 2 * keep + 1; ++row) {
+          float gr = 0.f, gi = 0.f;
+          for (int p = 0; p < NP; ++p) {
+            const float f = F[row * NP + p];
+            gr = fmaf(f, rr[p], gr);
+            gi = fmaf(f, ri[p], gi);
+          }
+          const float2 x = ch[row * P.n_omega_channels + w];
+          pr += x.x * gr - x.y * gi;
+          pi += x.x * gi + x.y * gr;
+        }
+      }
+      // band scale and flight phase e^{i w r / v}
+      const float s = g_scale[(int64_t)lam * total + idx];
+      float sv = 0.f, cv = 1.f;
+      if (T.flight) {
+        const double turns = om * g_r[idx] / T.speed[lam] * (1.0 / (2 * kPi));
+        sincospif(2.f * (float)(turns - rint(turns)), &sv, &cv);
+      }
+      acc_re += s * (pr * cv - pi * sv);
+      acc_im += s * (pr * sv + pi * cv);
+    }
+    partial[(((int64_t)d * gridDim.y + chunk) * T.n_bands + lam) * Wn + w] =
+        make_double2(acc_re, acc_im);
+  }
+}
+
+// result[d][w] = e^{i w ref} * sum over chunks and bands, fixed order.
+__global__ void ge2_reduce_kernel(lh_ge2_table T, lh_ge2_problem P, int chunks,
+                                  const double2* partial) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int Wn = P.n_omega;
+  if (idx >= (int64_t)P.n_om * Wn) return;
+  const int d = (int)(idx / Wn), w = (int)(idx % Wn);
+  double re = 0.0, im = 0.0;
+  for (int ch = 0; ch < chunks; ++ch)
+    for (int lam = 0; lam < T.n_bands; ++lam) {
+      const double2 v = partial[(((int64_t)d * chunks + ch) * T.n_bands + lam) * Wn + w];
+      re += v.x;
+      im += v.y;
+    }
+  const double ang = T.omega[w] * P.reference_ns;
+  const double c = cos(ang), s = sin(ang);
+  P.result[2 * idx] = re * c - im * s;
+  P.result[2 * idx + 1] = re * s + im * c;
+}
+
+int ge2_chunks(const lh_ge2_problem& P) { return (P.n_points + kGe2Chunk - 1) / kGe2Chunk; }
+
+size_t ge2_workspace(const lh_ge2_table& T, const lh_ge2_problem& P) {
+  const size_t pairs = (size_t)P.n_om * P.n_points;
+  const size_t chunks = (size_t)ge2_chunks(P);
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  return up(pairs * 4) + up(pairs * 4) + up(pairs * 8) + up(pairs * T.n_bands * 4) +
+         up(pairs * T.nch * T.n_pairs * 4) +
+         up((size_t)P.n_om * chunks * T.n_bands * P.n_omega * sizeof(double2));
+}
+
+int ge2_launch(const lh_ge2_table& T, const lh_ge2_problem& P, void* ws, cudaStream_t s) {
+  const size_t pairs = (size_t)P.n_om * P.n_points;
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  uint8_t* p = static_cast<uint8_t*>(ws);
+  int* g_j = reinterpret_cast<int*>(p); p += up(pairs * 4);
+  float* g_t = reinterpret_cast<float*>(p); p += up(pairs * 4);
+  double* g_r = reinterpret_cast<double*>(p); p += up(pairs * 8);
+  float* g_scale = reinterpret_cast<float*>(p); p += up(pairs * T.n_bands * 4);
+  float* g_F = reinterpret_cast<float*>(p); p += up(pairs * T.nch * T.n_pairs * 4);
+  double2* partial = reinterpret_cast<double2*>(p);
+  ge2_geometry_kernel<<<(unsigned)((pairs + 127) / 128), 128, 0, s>>>(T, P, g_j, g_t, g_r, g_scale, g_F);
+  const int chunks = ge2_chunks(P);
+  const size_t smem = (size_t)kGe2Chunk * T.nch * T.n_pairs * sizeof(float);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(ge2_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  ge2_apply_kernel<<<dim3(P.n_om, chunks), 256, smem, s>>>(T, P, g_j, g_t, g_r, g_scale, g_F,
+                                                            partial);
+  const int64_t outs = (int64_t)P.n_om * P.n_omega;
+  ge2_reduce_kernel<<<(unsigned)((outs + 255) / 256), 256, 0, s>>>(T, P, chunks, partial);
+  return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+}
+
+}  // namespace lh

@@ -1,0 +1,213 @@
+"""Order >=2 on the B200: ``apply_folded`` for node-band axial sources.
+
+Reference: ``apply_folded`` (``shower/ge2.py:99-119``) ->
+``apply_multi_spectral`` (``_shower_basis.py:1126-1198``) ->
+``_apply_multi_spectral`` (``_shower_basis.py:894-1050``).
+
+The band-folded kernels (``ShowerTransport.tables()['folded']``,
+``band_fold.py:155-208``) are built once by the reference and uploaded
+read-only as complex64 ``[band][interval][l][pair][power][omega]``. Per call
+the host only rotates the points and OMs into the source's axis frame
+(float64, O(points + OMs)); the phase alignment of the band sources, the
+geometry (float64) and the contraction (float32) run in ``liblh_b200.so``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from math import exp, lgamma
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["Ge2Table", "AxialSources", "apply_folded"]
+
+
+def _start_norm(jmax):
+    """``sqrt(binom(2j, j - nu))`` (``_directional_numba.py:389-397``)."""
+    table = np.zeros((jmax + 1, 2 * jmax + 1))
+    for j in range(jmax + 1):
+        for nu in range(-j, j + 1):
+            table[j, nu + jmax] = exp(0.5 * (lgamma(2 * j + 1) - lgamma(j + nu + 1)
+                                             - lgamma(j - nu + 1)))
+    return table
+
+
+@dataclass
+class AxialSources:
+    """Node-band sources on one point set (the reference's ``AxialSource`` list).
+
+    ``points_m`` (P, 3) detector coordinates; ``channels`` (band, P, nch, W)
+    complex; ``reference_ns`` per band; ``frame`` = (centre, first, second, axis).
+    """
+    points_m: np.ndarray
+    channels: object
+    reference_ns: np.ndarray
+    frame: tuple
+    degree: int
+    azimuthal_degree: int
+
+    @classmethod
+    def from_reference(cls, sources):
+        """From a list of reference ``AxialSource`` objects sharing their points."""
+        first = sources[0]
+        f = first.frame
+        return cls(np.asarray(first.points_m(), float),
+                   np.stack([np.asarray(s.channels, np.complex64) for s in sources]),
+                   np.array([float(s.reference_ns) for s in sources]),
+                   (np.asarray(f.centre_m, float), np.asarray(f.first, float),
+                    np.asarray(f.second, float), np.asarray(f.axis, float)),
+                   int(first.degree), int(first.azimuthal_degree))
+
+
+class Ge2Table:
+    """Band-folded order >=2 kernels resident on the device."""
+
+    def __init__(self, folded, alpha, *, device="cuda", source_degree=None,
+                 azimuthal_degree=None):
+        import torch
+        self.device = torch.device(device)
+        dev = self.device
+        coef = np.asarray(folded["coefficients"])
+        self.n_bands, self.n_intervals = coef.shape[0], coef.shape[1]
+        self.degree = int(folded["degree"])
+        self.acc_degree = int(folded["acceptance_degree"])
+        self.omega = np.asarray(folded["omega"], float)
+        self.pair_lambda = np.asarray(folded["pair_lambda"], np.int32)
+        self.pair_mu = np.asarray(folded["pair_mu"], np.int32)
+        self.log_r = np.asarray(folded["log_r"], float)
+        self.flight = str(folded["phase"]) == "flight"
+        self.absorption = np.asarray(folded["absorption"], float)
+        self.speed = np.asarray(folded["speed"], float)
+        self.alpha = np.ascontiguousarray(np.asarray(alpha, float)[:self.acc_degree + 1])
+        sd = self.degree if source_degree is None else int(source_degree)
+        az = sd if azimuthal_degree is None else int(azimuthal_degree)
+        if sd < self.degree:
+            raise ValueError("source degree is insufficient")
+        self.source_degree, self.azimuthal_degree = sd, az
+        self.max_m = min(az, self.degree)
+        starts = [0]
+        for ell in range(sd + 1):
+            starts.append(starts[-1] + 2 * min(ell, az) + 1)
+        self.starts = np.asarray(starts, np.int32)
+        self.nch = int(starts[-1])
+        self.jmax = max(self.max_m, self.acc_degree)
+        self._coef = torch.view_as_real(torch.from_numpy(coef.astype(np.complex64))).contiguous().to(dev)
+
+        def f64(x):
+            return torch.tensor(np.ascontiguousarray(x, float), dtype=torch.float64, device=dev)
+
+        def i32(x):
+            return torch.tensor(np.ascontiguousarray(x, np.int32), dtype=torch.int32, device=dev)
+
+        self._log_r, self._abs, self._speed = f64(self.log_r), f64(self.absorption), f64(self.speed)
+        self._omega, self._alpha = f64(self.omega), f64(self.alpha)
+        self._pl, self._pm, self._starts = i32(self.pair_lambda), i32(self.pair_mu), i32(self.starts)
+        self._norm = f64(_start_norm(self.jmax))
+        self.struct = _lib.Ge2Table(
+            self.n_bands, self.n_intervals, self.degree, self.acc_degree, self.max_m,
+            len(self.pair_lambda), self.nch, len(self.omega), self._coef.data_ptr(),
+            self._log_r.data_ptr(), self._abs.data_ptr(), self._speed.data_ptr(),
+            self._omega.data_ptr(), self._pl.data_ptr(), self._pm.data_ptr(),
+            self._alpha.data_ptr(), self._starts.data_ptr(), self._norm.data_ptr(), self.jmax,
+            int(self.flight))
+        self._workspace = None
+
+    @classmethod
+    def load(cls, path, alpha, **kw):
+        return cls(dict(np.load(path)), alpha, **kw)
+
+    def radial_limits(self):
+        return float(np.exp(self.log_r[0])), float(np.exp(self.log_r[-1]))
+
+    def apply(self, sources: AxialSources, positions, looks, out_scale, window=None, *,
+              zero_frequency=False, stream=None):
+        """``apply_folded``: (frequency, OM) complex128 spectrum on the host.
+
+        ``out_scale`` (OM,) or (band, OM): the detector scale of every band (the
+        route passes the effective area). ``zero_frequency`` evaluates only the
+        first frequency (``band_fold.zero_frequency``).
+        """
+        res = self.apply_device(sources, positions, looks, out_scale, window,
+                                zero_frequency=zero_frequency, stream=stream)
+        import torch
+        torch.cuda.synchronize(self.device)
+        return res.cpu().numpy().T
+
+    def apply_device(self, sources, positions, looks, out_scale, window=None, *,
+                     zero_frequency=False, stream=None):
+        import torch
+        lib = _lib.load()
+        dev = self.device
+        positions = np.atleast_2d(np.asarray(positions, float))
+        n_om = len(positions)
+        W = 1 if zero_frequency else len(self.omega)
+        if sources.degree < self.degree:
+            raise ValueError("source degree is insufficient")
+        if (sources.azimuthal_degree != self.azimuthal_degree
+                or sources.degree != self.source_degree):
+            raise ValueError("source angular layout differs from the table's")
+        low_c, high_c = self.radial_limits()
+        if window is None:
+            low, high = low_c, high_c
+        else:
+            low, high = map(float, window)
+            if (not np.isfinite(low) or not np.isfinite(high) or low < low_c - 1e-9
+                    or high > high_c + 1e-9 or low >= high):
+                raise ValueError("radial window must lie inside the kernel cache")
+        centre, e1, e2, e3 = (np.asarray(v, float) for v in sources.frame)
+        basis = np.stack([e1, e2, e3])
+        pts = (np.asarray(sources.points_m, float) - centre) @ basis.T
+        rec = (positions - centre) @ basis.T
+        lk = np.atleast_2d(np.asarray(looks, float)) @ basis.T
+        if window is None:
+            r = np.linalg.norm(pts[None, :, :] - rec[:, None, :], axis=2)
+            if np.any(r < low_c) or np.any(r > high_c):
+                raise ValueError("Source/receiver distances outside the cache")
+        ref = np.asarray(sources.reference_ns, float)
+        reference = float(ref.min())
+        ch = sources.channels
+        if not isinstance(ch, torch.Tensor):
+            ch = torch.from_numpy(np.ascontiguousarray(np.asarray(ch), dtype=np.complex64))
+        ch = ch.to(dev, torch.complex64)
+        if zero_frequency:
+            ch = ch[..., :1]
+        if ch.shape[0] != self.n_bands or ch.shape[2] != self.nch or ch.shape[3] < W:
+            raise ValueError("source channels do not match the folded kernels")
+        shift = ref - reference
+        if np.any(shift != 0):  # align every band to the earliest emission reference
+            ph = torch.exp(1j * torch.tensor(self.omega[:ch.shape[3]], device=dev)[None, :]
+                           * torch.tensor(shift, device=dev)[:, None]).to(torch.complex64)
+            ch = ch * ph[:, None, None, :]
+        ch = torch.view_as_real(ch.contiguous()).contiguous()
+        scale = np.asarray(out_scale, float)
+        if scale.ndim == 1:
+            scale = np.repeat(scale[None, :], self.n_bands, axis=0)
+
+        def f64(x):
+            return torch.tensor(np.ascontiguousarray(x, float), dtype=torch.float64, device=dev)
+
+        d_pts, d_rec, d_lk, d_scale = f64(pts), f64(rec), f64(lk), f64(scale)
+        result = torch.empty((n_om, W), dtype=torch.complex128, device=dev)
+        prob = _lib.Ge2Problem(len(pts), d_pts.data_ptr(), ch.data_ptr(), int(ch.shape[3]), W,
+                               n_om, d_rec.data_ptr(), d_lk.data_ptr(), d_scale.data_ptr(), low,
+                               high, reference, result.data_ptr())
+        need = int(lib.lh_ge2_workspace_bytes(self.struct, prob))
+        if need == 0 and n_om and len(pts):
+            raise ValueError("order >=2 problem rejected by the device library")
+        if self._workspace is None or self._workspace.numel() < need:
+            self._workspace = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+        s = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
+        _lib.check(lib.lh_ge2_apply(self.struct, prob, self._workspace.data_ptr(),
+                                    self._workspace.numel(), s), "lh_ge2_apply")
+        self._keep = (d_pts, d_rec, d_lk, d_scale, ch)  # alive until the stream runs
+        return result
+
+
+def apply_folded(table: Ge2Table, sources: AxialSources, positions, looks, area, window, *,
+                 zero_frequency=False):
+    """``shower/ge2.py:99-119``: folded >=2 spectrum (frequency, OM) of node-band sources."""
+    if not len(np.atleast_2d(positions)):
+        return np.zeros((1 if zero_frequency else len(table.omega), 0), complex)
+    return table.apply(sources, positions, looks, np.asarray(area, float), window,
+                       zero_frequency=zero_frequency)

@@ -1,0 +1,79 @@
+"""Order >=2 contraction: oracle pinned to the reference, device kernel vs oracle."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, TABLES
+from oracle.ge2 import apply_folded as oracle_apply
+
+# Device >=2 spectra: float32 contraction, float64 geometry. Error relative to
+# the largest |value| of the spectrum (>=2 charges can be slightly negative).
+GE2_TOL = 2e-5
+
+
+def fixture():
+    g = np.load(GOLDEN / "shower_c0.npz")
+    t = dict(np.load(TABLES / "ge2_fold_48om_2-150m.npz"))
+    frame = dict(centre=g["frame_centre_m"], first=g["frame_first"], second=g["frame_second"],
+                 axis=g["frame_axis"])
+    return g, t, frame
+
+
+def points(g, frame, tag):
+    z, tr = g[f"{tag}_z_m"], g[f"{tag}_transverse_m"]
+    return (frame["centre"][None] + z[:, None] * frame["axis"][None]
+            + tr[:, 0:1] * frame["first"][None] + tr[:, 1:2] * frame["second"][None])
+
+
+def oracle_sources(g, frame, tag, channels=None):
+    return dict(points_m=points(g, frame, tag),
+                channels=g[f"{tag}_channels"] if channels is None else channels,
+                reference_ns=g[f"{tag}_reference_ns"], frame=frame,
+                degree=int(g["source_degree"]), azimuthal_degree=int(g["azimuthal_degree"]))
+
+
+def test_oracle_matches_reference_full_frequency_subset():
+    g, t, frame = fixture()
+    out = oracle_apply(t, oracle_sources(g, frame, "sub"), g["om_positions_m"], g["om_looks"],
+                       g["alpha"], g["om_area_m2"], g["radial_window_m"])
+    assert np.abs(out - g["spec_sub"]).max() <= 1e-12 * np.abs(g["spec_sub"]).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", ["zero", "sub"])
+def test_device_apply_matches_reference(tag):
+    from lighthit_b200.ge2 import AxialSources, Ge2Table
+    g, t, frame = fixture()
+    table = Ge2Table(t, g["alpha"], source_degree=int(g["source_degree"]),
+                     azimuthal_degree=int(g["azimuthal_degree"]))
+    src = AxialSources(points(g, frame, tag), g[f"{tag}_channels"], g[f"{tag}_reference_ns"],
+                       (frame["centre"], frame["first"], frame["second"], frame["axis"]),
+                       int(g["source_degree"]), int(g["azimuthal_degree"]))
+    out = table.apply(src, g["om_positions_m"], g["om_looks"], g["om_area_m2"],
+                      g["radial_window_m"], zero_frequency=(tag == "zero"))
+    ref = g[f"spec_{tag}"]
+    assert out.shape == ref.shape
+    assert np.abs(out - ref).max() <= GE2_TOL * np.abs(ref).max()
+
+
+@pytest.mark.gpu
+def test_device_apply_all_points_random_channels_vs_oracle():
+    """Every basis point at all 65 frequencies (seeded channels), vs the oracle."""
+    from lighthit_b200.ge2 import AxialSources, Ge2Table
+    g, t, frame = fixture()
+    rng = np.random.default_rng(8)
+    P = int(g["n_points"])
+    zero_pts = points(g, frame, "zero")
+    ch = (rng.normal(size=(3, P, 39, 65)) + 1j * rng.normal(size=(3, P, 39, 65))).astype(np.complex64)
+    ch *= np.abs(g["zero_channels"][:, :, :, :1])  # keep the sources' magnitude profile
+    oms = np.arange(0, 48, 4)
+    src_o = dict(points_m=zero_pts, channels=ch, reference_ns=np.array([0.0, 0.3, -0.2]),
+                 frame=frame, degree=int(g["source_degree"]),
+                 azimuthal_degree=int(g["azimuthal_degree"]))
+    ref = oracle_apply(t, src_o, g["om_positions_m"][oms], g["om_looks"][oms], g["alpha"],
+                       g["om_area_m2"][oms], g["radial_window_m"])
+    table = Ge2Table(t, g["alpha"], source_degree=8, azimuthal_degree=2)
+    src = AxialSources(zero_pts, ch, src_o["reference_ns"],
+                       (frame["centre"], frame["first"], frame["second"], frame["axis"]), 8, 2)
+    out = table.apply(src, g["om_positions_m"][oms], g["om_looks"][oms], g["om_area_m2"][oms],
+                      g["radial_window_m"])
+    assert np.abs(out - ref).max() <= GE2_TOL * np.abs(ref).max()

@@ -107,11 +107,13 @@ def test_served_results_equal_alone_and_in_the_mix(flash_table, flash_config, tm
     sizes = flash_batch_sizes(700, seed=6, low=1, high=120)
     bounds = np.concatenate([[0], np.cumsum(sizes)])
     reqs = []
-    for a, b in zip(bounds[:-1], bounds[1:]):
+    burst = len(sizes) // 2
+    for i, (a, b) in enumerate(zip(bounds[:-1], bounds[1:])):
         reqs.append(srv.submit(pos[a:b], 1e10))
-        srv.poll()
+        if i >= burst:  # the first half arrives at once, the rest one by one
+            srv.poll()
     srv.drain()
-    assert srv.launches < len(reqs)  # requests were coalesced into launches
+    assert srv.launches < len(reqs)  # the burst was coalesced into launches
     for req, (a, b) in zip(reqs, zip(bounds[:-1], bounds[1:])):
         alone = ft.run(pos[a:b], 1e10)
         for k in RESULT_KEYS:
