@@ -37,6 +37,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = "showers/s + p99 latency, served mixed-precision vs plain GPU at <=1e-3 rel pe error"
 TABLE = ROOT / "lighthit_b200" / "tables" / "flash_450nm_2-250m.npz"
 N_FLASH = 4096
+# DRAM bytes (read + write) of one 4096-flash flash_tc_kernel launch, measured with
+# ncu on a B200 (profiles/flash_tc_kernel_4096flashes.txt).
+FLASH_TC_TRAFFIC = 637_070_336
 
 
 def workload():
@@ -290,14 +293,22 @@ def ours(args, rank, world, local_rank):
                                           block_threads=threads))
 
     def serve_all():
+        """One step: every request submitted, served and handed back; the client
+        then drops the results, so their pinned buffers return to the host pool."""
         for a, b in requests:
             srv.submit(pos_np[a:b], 1e10)
         srv.poll()
-        return srv.drain()
+        done = srv.drain()
+        served_flashes = sum(len(r.positions) for r in done)
+        assert served_flashes == F and all(r.error is None for r in done)
+        shape = done[0].result["charge"].shape
+        srv.completed.clear()
+        return shape
 
+    first_shape = serve_all()
+    assert first_shape == (requests[0][1] - requests[0][0], 48, 3)
     serve_all()
-    srv.completed.clear()
-    e2e_steps = min(args.steps, 10)
+    e2e_steps = min(args.steps, 20)
     e0, e1 = _events(torch, 2)
     torch.cuda.synchronize(dev)
     w0 = time.perf_counter()
@@ -315,9 +326,6 @@ def ours(args, rank, world, local_rank):
     e2e_value = world * F * e2e_steps / (e2e_ms / 1e3)
     h2d = F * (3 * 8 + 8 + 8)
     d2h = F * 48 * per_pair
-    done = srv.completed
-    first = done[0]
-    assert first.result["charge"].shape == (requests[0][1] - requests[0][0], 48, 3)
 
     # latency under Poisson arrivals at half the end-to-end capacity
     srv.completed.clear()
@@ -328,6 +336,7 @@ def ours(args, rank, world, local_rank):
     order = [requests[i % len(requests)] for i in range(len(arrivals))]
     t_start = time.perf_counter()
     nxt = 0
+    latencies = []
     while nxt < len(arrivals) or srv.queue or srv.busy:
         now = time.perf_counter() - t_start
         while nxt < len(arrivals) and arrivals[nxt] <= now:
@@ -335,7 +344,9 @@ def ours(args, rank, world, local_rank):
             srv.submit(pos_np[a:b], 1e10, arrival=t_start + arrivals[nxt])
             nxt += 1
         srv.poll()
-    lat_ms = np.array([r.latency for r in srv.completed]) * 1e3
+        latencies += [r.latency for r in srv.completed]
+        srv.completed.clear()  # the client takes each result as it completes
+    lat_ms = np.array(latencies) * 1e3
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -367,7 +378,9 @@ def ours(args, rank, world, local_rank):
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
                          "algorithmic_bytes_per_pair": per_pair, "pairs_per_launch": 48 * F,
-                         "block_threads": threads, "traffic": None},
+                         "block_threads": threads, "traffic": FLASH_TC_TRAFFIC,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one "
+                                           "4096-flash launch (profiles/flash_tc_kernel_4096flashes.txt)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "flashes/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "wall_s": wall, "steps": e2e_steps,

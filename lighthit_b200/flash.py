@@ -245,3 +245,52 @@ class FlashTransport:
              "fourier_inverted_orders": [1, 2],
              "radial_range_m": list(map(float, self.config.radial_range_m)),
              "readout_precision": self.mode, "route": "lighthit_b200.flash"})
+
+
+def _main(argv=None):
+    """``python -m lighthit_b200.flash --flashes N --repeat K``: run the fused
+    flash launch on the seed-11 calibration workload (48-OM synthetic array,
+    450 nm table, 2-250 m) K times and print the mean CUDA-event time. Used to
+    profile one kernel on a chosen batch size."""
+    import argparse
+    from pathlib import Path
+
+    import torch
+
+    from .model import KernelConfig, synthetic_detector
+    from .workloads import flash_positions
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--flashes", type=int, default=4096)
+    ap.add_argument("--repeat", type=int, default=3)
+    ap.add_argument("--mode", default="split-bf16", choices=sorted(_lib.MODES))
+    ap.add_argument("--block-threads", type=int, default=0)
+    args = ap.parse_args(argv)
+    det = synthetic_detector()
+    cfg = KernelConfig(omega_per_ns=np.linspace(0, 1.2, 65),
+                       readout_omega_per_ns=np.linspace(0, 1.2, 321),
+                       relative_time_edges_ns=np.arange(-60.0, 745.0, 5.0),
+                       radial_range_m=(2.0, 250.0), threshold_pe=0.01)
+    table = FlashTable.load(Path(__file__).resolve().parent / "tables" / "flash_450nm_2-250m.npz")
+    ft = FlashTransport(det, cfg, table, device="cuda", mode=args.mode)
+    F = args.flashes
+    pos = torch.tensor(flash_positions(F, det.positions_m.mean(axis=0), seed=11,
+                                       om_positions=det.positions_m), device=ft.device)
+    ph = torch.full((F,), 1e10, dtype=torch.float64, device=ft.device)
+    tt = torch.zeros(F, dtype=torch.float64, device=ft.device)
+    out = ft.allocate(F)
+    ft.launch(pos, ph, tt, out, block_threads=args.block_threads)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.repeat):
+        ft.launch(pos, ph, tt, out, block_threads=args.block_threads)
+    e1.record()
+    torch.cuda.synchronize()
+    ft.raise_for_status(out)
+    ms = e0.elapsed_time(e1) / max(args.repeat, 1)
+    print(f"flashes {F} mode {args.mode}: {ms:.4f} ms per launch, "
+          f"{F * ft.n_om * (ft.n_omega * 24 + 3 * ft.n_bins * 4 + 33) / ms / 1e6:.1f} GB/s of outputs")
+
+
+if __name__ == "__main__":
+    _main()
