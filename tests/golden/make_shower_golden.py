@@ -41,7 +41,8 @@ READOUT = np.linspace(0.0, 1.2, 321)
 EDGES = np.arange(-60.0, 745.0, 5.0)
 
 
-def main():
+def setup():
+    """The README-example kernel (built tables in the work folder) and shower."""
     cache = WORK / "shower-c0"
     medium = synthetic_medium_model()
     detector = baikal_like_detector(clusters=1)
@@ -59,6 +60,11 @@ def main():
     if not (cache / "ge2-pack" / "pack.json").exists():
         kernel.build(source=shower)
         kernel.ge2_kernel_store().save(str(cache / "ge2-pack"))
+    return kernel, shower, cache
+
+
+def main():
+    kernel, shower, cache = setup()
     route = ShowerTransport(kernel, ShowerData.of(str(cache), str(cache / "ge2-pack")))
     response = route(shower)
     tables = route.tables()
