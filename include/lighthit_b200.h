@@ -173,6 +173,71 @@ size_t lh_ge2_workspace_bytes(const lh_ge2_table* t, const lh_ge2_problem* p);
 int lh_ge2_apply(const lh_ge2_table* t, const lh_ge2_problem* p, void* workspace,
                  size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------------------ order 0
+ * Replaces PreparedBallistic.charge() / .bins(ids, origins, edges)
+ * (_surface_ballistic.py:95-118, the first-entry order 0 of transport_prompt,
+ * prompt.py:640-660 and 896-903): direct Cherenkov light of spectral elements to
+ * the first glass entry of each OM sphere, over the candidate pairs of
+ * interval_candidates (_ballistic_interval_numba.py:449-519), integrated by the
+ * reference's direct ray form _surface_ballistic_rays.evaluate
+ * (_surface_ballistic_rays.py:36-156) at a fixed Gauss order.
+ * The optical panels are those of prepare_optics(..., exact_response=True)
+ * (ballistic_interval.py:64-161), built once by the reference.
+ */
+#define LH_STATUS_ON_TRACK 8u             /* point receiver on an emitting track        */
+#define LH_STATUS_INSIDE_GLASS 16u        /* emitting segment intersects the glass      */
+#define LH_STATUS_NEGATIVE_ACCEPTANCE 32u /* negative ballistic angular response        */
+#define LH_STATUS_OVERFLOW 64u            /* more bin cuts in one s / phi range than the
+                                             kernel holds (bins finer than the arrival
+                                             spread by > 10x): result incomplete        */
+
+typedef struct {
+  int32_t n_om;
+  const double* om_pos;        /* [n_om][3]                                            */
+  const double* om_look;       /* [n_om][3] looks = -orientations                      */
+  const double* om_area;       /* [n_om] effective area m^2                            */
+  const double* om_radius;     /* [n_om] glass sphere radius m (> 0)                   */
+  int32_t n_alpha;             /* acceptance Legendre coefficients (<= 8)              */
+  const double* alpha;
+  int32_t n_panel_edges;       /* optical panels + 1 (<= 129)                          */
+  const double* panel_edges;   /* [n_panel_edges] wavelength nm                        */
+  const double* phase;         /* [n_panel_edges] phase index                          */
+  const double* group;         /* [n_panel_edges] group index                          */
+  const double* extinction;    /* [n_panel_edges] mu_a + mu_s 1/m                      */
+  int32_t eff_cols;            /* 4 (cubic) or 6 (cubic x exp(linear))                 */
+  const double* efficiency;    /* [n_panel_edges - 1][eff_cols]                        */
+  int32_t order;               /* Gauss-Legendre order of every quadrature (<= 32)     */
+  const double* gauss_x;       /* [order] nodes on (-1, 1)                             */
+  const double* gauss_w;       /* [order] weights                                      */
+} lh_order0_optics;
+
+typedef struct {
+  int32_t n_events;
+  const int64_t* element_offset; /* [n_events + 1] event e owns elements [off[e], off[e+1]) */
+  const int64_t* chunk_offset;   /* [n_events + 1] from lh_order0_chunks                  */
+  int64_t n_chunks;              /* host: chunk_offset[n_events]                          */
+  const double* start;           /* [n_el][3] m                                           */
+  const double* direction;       /* [n_el][3] unit                                        */
+  const double* length;          /* [n_el] m                                              */
+  const double* c0;              /* [n_el] Cherenkov C0                                   */
+  const double* c2;              /* [n_el] Cherenkov C2 (= -C0 / beta^2)                  */
+  const double* beta;            /* [n_el]                                                */
+  const double* t0;              /* [n_el] start ns                                       */
+  const double* t1;              /* [n_el] end ns                                         */
+  const double* origins;         /* [n_events][n_om] time origin ns                       */
+  int32_t n_edges;               /* relative time edges; charge only: 2 edges (-1e100, 1e100) */
+  const double* edges;           /* [n_edges] ns                                          */
+  double* charge;                /* [n_events][n_om] pe (overwritten)                     */
+  double* bins;                  /* [n_events][n_om][n_edges-1] pe (overwritten) or NULL  */
+  int32_t* status;               /* [1] LH_STATUS_* flags (or-ed in)                      */
+} lh_order0_batch;
+
+/* Chunks of the element lists (host helper): fills chunk_offset_host[n_events+1]
+ * and returns the total. */
+size_t lh_order0_chunks(const int64_t* element_counts, int32_t n_events, int64_t* chunk_offset_host);
+
+int lh_order0(const lh_order0_optics* optics, const lh_order0_batch* batch, void* stream);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

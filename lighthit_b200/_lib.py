@@ -13,6 +13,8 @@ LIB_PATH = _HERE / "liblh_b200.so"
 
 LH_OK, LH_EINVAL, LH_ECUDA, LH_ENOMEM, LH_ETIMEDOUT, LH_EUNSUPPORTED = 0, 1, 2, 3, 4, 5
 LH_STATUS_COINCIDENT, LH_STATUS_UNSAFE, LH_STATUS_TIMEOUT = 1, 2, 4
+LH_STATUS_ON_TRACK, LH_STATUS_INSIDE_GLASS, LH_STATUS_NEGATIVE_ACCEPTANCE = 8, 16, 32
+LH_STATUS_OVERFLOW = 64
 LH_MODE_PLAIN_FP32, LH_MODE_SPLIT_BF16, LH_MODE_BF16 = 0, 1, 2
 MODES = {"fp32": LH_MODE_PLAIN_FP32, "split-bf16": LH_MODE_SPLIT_BF16, "bf16": LH_MODE_BF16}
 
@@ -60,6 +62,22 @@ class Ge2Problem(C.Structure):
                 ("radial_high", C.c_double), ("reference_ns", C.c_double), ("result", P)]
 
 
+class Order0Optics(C.Structure):
+    _fields_ = [("n_om", C.c_int32), ("om_pos", P), ("om_look", P), ("om_area", P),
+                ("om_radius", P), ("n_alpha", C.c_int32), ("alpha", P),
+                ("n_panel_edges", C.c_int32), ("panel_edges", P), ("phase", P), ("group", P),
+                ("extinction", P), ("eff_cols", C.c_int32), ("efficiency", P),
+                ("order", C.c_int32), ("gauss_x", P), ("gauss_w", P)]
+
+
+class Order0Batch(C.Structure):
+    _fields_ = [("n_events", C.c_int32), ("element_offset", P), ("chunk_offset", P),
+                ("n_chunks", C.c_int64), ("start", P), ("direction", P), ("length", P),
+                ("c0", P), ("c2", P), ("beta", P), ("t0", P), ("t1", P), ("origins", P),
+                ("n_edges", C.c_int32), ("edges", P), ("charge", P), ("bins", P),
+                ("status", P)]
+
+
 # name -> (restype, argtypes); every symbol the header declares
 SIGNATURES = {
     "lh_version": (C.c_char_p, []),
@@ -76,6 +94,8 @@ SIGNATURES = {
                                              C.POINTER(FlashBatch), P]),
     "lh_ge2_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem)]),
     "lh_ge2_apply": (C.c_int, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem), P, C.c_size_t, P]),
+    "lh_order0_chunks": (C.c_size_t, [P, C.c_int32, P]),
+    "lh_order0": (C.c_int, [C.POINTER(Order0Optics), C.POINTER(Order0Batch), P]),
 }
 LH_ESCRATCH = 6
 

@@ -1,0 +1,611 @@
+// Order 0: direct Cherenkov light of spectral elements to the first glass
+// entry of each OM sphere, summed over elements, OMs and the continuous
+// wavelength spectrum.
+//
+// Reference: PreparedBallistic (_surface_ballistic.py:20-353) integrates this
+// with control variates; its direct form, used there for the geometry the
+// control variates cannot invert, is _surface_ballistic_rays.evaluate
+// (_surface_ballistic_rays.py:36-156) over the pairs of interval_candidates
+// (_ballistic_interval_numba.py:449-519). This file evaluates that direct
+// form for every pair at a fixed Gauss order:
+//
+//   q_d = sum_pairs sum_panels sum_lambda w_l  S(lambda) A / (pi R^2)
+//         int ds int dphi/(2 pi) [acc(+) + acc(-)] exp(-mu_t(lambda) d_entry)
+//
+// with the element's Cherenkov cone at the spectral phase index n(lambda),
+// s along the element where the cone meets the sphere, phi the azimuth of the
+// cone ray about the element axis and d_entry the distance to the first glass
+// entry. Bins split the s and phi ranges at the bin edges (arrival time).
+//
+// Precision: the pair, wavelength-node and s-node geometry (cone, sphere
+// window, arrival times, bin cuts and the bin index) are float64; the
+// innermost azimuth quadrature (acceptance, entry distance, attenuation) is
+// float32 with the entry distance written without cancellation:
+//   d = B / (dot + sqrt(R^2 - |w x k|^2)),  |w x k|^2 = sin^2(th) sin^2(phi) |w|^2
+//       + (E0 - along sin(th) 2 sin^2(phi/2))^2,
+// E0 = along sin(th) - rho cos(th) formed in float64.
+//
+// Launch: one CTA per (OM, chunk of 32 elements of one event). Warp 0 tests
+// the chunk's elements (candidates) and forms each pair's frame; the CTA then
+// lists the (pair, panel, piece) work, spreads (piece x wavelength node) over
+// its threads, accumulates bins in shared memory and the charge by a block
+// reduction, and adds both to the outputs once.
+#include "lh_common.cuh"
+
+namespace lh {
+
+constexpr int kO0Chunk = 32;
+constexpr int kO0Threads = 256;
+constexpr int kO0MaxOrder = 32;
+constexpr int kO0MaxPanels = 128;
+constexpr int kO0MaxSCuts = 64;
+constexpr int kO0MaxPhiCuts = 32;
+constexpr int kO0MaxAlpha = 8;
+
+struct O0Pair {
+  double z, rho, axial, across, side, nmin, nmax, cut0, cut1, tau;
+  int el;
+};
+
+LH_DEVICE double o0_clamp1(double x) { return x < -1.0 ? -1.0 : (x > 1.0 ? 1.0 : x); }
+
+// _ballistic_interval_numba.py:151-185 (_support): phase-index window of the
+// cone rays that meet the sphere, and the two inner cuts.
+LH_DEVICE bool o0_support(double z, double rho, double length, double beta, double radius,
+                          double& nmin, double& nmax, double& cut0, double& cut1) {
+  if (radius == 0.0) {
+    if (z <= 0.0) return false;
+    nmin = hypot(z, rho) / (beta * z);
+    nmax = INFINITY;
+    if (z > length) {
+      double rz = z - length;
+      nmax = hypot(rz, rho) / (beta * rz);
+    }
+    cut0 = cut1 = INFINITY;
+    return true;
+  }
+  const double quarter = 0.5 * kPi;
+  double psi0 = atan2(rho, z), psi1 = atan2(rho, z - length);
+  double r0 = radius / hypot(z, rho), r1 = radius / hypot(z - length, rho);
+  double a0 = asin(r0 < 1.0 ? r0 : 1.0), a1 = asin(r1 < 1.0 ? r1 : 1.0);
+  double low = psi0 - a0, high = psi1 + a1;
+  if (low >= quarter) return false;
+  double floor_n = (1.0 + 1e-9) / beta;
+  if (low <= 0.0) {
+    nmin = floor_n;
+  } else {
+    double v = 1.0 / (beta * cos(low));
+    nmin = floor_n > v ? floor_n : v;
+  }
+  nmax = high >= quarter ? INFINITY : 1.0 / (beta * cos(high));
+  double inner0 = psi0 + a0, inner1 = psi1 - a1;
+  cut0 = inner0 >= quarter ? INFINITY : 1.0 / (beta * cos(inner0));
+  cut1 = (inner1 <= 0.0 || inner1 >= quarter) ? INFINITY : 1.0 / (beta * cos(inner1));
+  return true;
+}
+
+// _ballistic_interval_numba.py:226-251 (_cone_can_reach_sphere)
+LH_DEVICE bool o0_cone_reaches(double z, double rho, double length, double beta, double radius,
+                               double pmin, double pmax) {
+  if (z <= -radius || beta * pmax <= 1.0) return false;
+  double c_hi = 1.0 / (beta * pmax);
+  double t = (1.0 - c_hi) * (1.0 + c_hi);
+  double s_hi = sqrt(t > 0.0 ? t : 0.0);
+  double c_lo = 1.0 / (beta * pmin);
+  if (c_lo > 1.0) c_lo = 1.0;
+  t = (1.0 - c_lo) * (1.0 + c_lo);
+  double s_lo = sqrt(t > 0.0 ? t : 0.0);
+  double q_hi = rho * c_hi - z * s_hi;
+  double other = rho * c_lo - z * s_lo;
+  double minimum = z >= 0.0 ? q_hi : (q_hi < other ? q_hi : other);
+  double rounding = 16 * 2.220446049250313e-16 * (fabs(z) + rho + length + radius);
+  if (minimum > radius + rounding) return false;
+  double end_z = z - length;
+  if (end_z >= 0.0 && rho * c_lo - end_z * s_lo < -radius - rounding) return false;
+  return true;
+}
+
+// _surface_ballistic_rays.py:14-30: real roots of a s^2 + b s + c inside (low, high)
+LH_DEVICE int o0_quadratic_cuts(double* cuts, int count, double a, double b, double c, double low,
+                                double high) {
+  double r[2];
+  int nr = 0;
+  if (a == 0.0) {
+    if (b != 0.0) r[nr++] = -c / b;
+  } else {
+    double disc = b * b - 4 * a * c;
+    if (disc < 0.0) return count;
+    double q = -0.5 * (b + copysign(sqrt(disc), b));
+    if (q == 0.0) {
+      r[nr++] = -b / (2 * a);
+    } else {
+      r[nr++] = q / a;
+      r[nr++] = c / q;
+    }
+  }
+  for (int k = 0; k < nr; ++k)
+    if (low < r[k] && r[k] < high) {
+      if (count < kO0MaxSCuts) cuts[count] = r[k];
+      ++count;
+    }
+  return count;
+}
+
+LH_DEVICE double o0_entry(double B, double dot) {
+  double t = dot * dot - B;
+  return B / (dot + sqrt(t > 0.0 ? t : 0.0));
+}
+
+LH_DEVICE int o0_search_right(const double* e, int n, double x) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (e[mid] > x) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+LH_DEVICE int o0_search_left(const double* e, int n, double x) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (e[mid] >= x) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+template <typename T>
+LH_DEVICE void o0_sort(T* v, int count) {
+  for (int k = 1; k < count; ++k) {
+    T value = v[k];
+    int m = k - 1;
+    while (m >= 0 && v[m] > value) {
+      v[m + 1] = v[m];
+      --m;
+    }
+    v[m + 1] = value;
+  }
+}
+
+// Legendre acceptance sum_l (2l+1) alpha_l P_l(x) / (4 pi), clipped at zero
+// (_ballistic_interval_numba.py:21-37); `bad` is raised below -1e-12 max(1, sum|alpha|).
+LH_DEVICE float o0_acceptance(const float* alpha, int n_alpha, float x, float alpha_abs,
+                              bool& bad) {
+  constexpr float inv4pi = 0.0795774715459476679f;
+  float result = alpha[0] * inv4pi;
+  float previous = 1.0f, current = x;
+  if (n_alpha > 1) result += 3.0f * alpha[1] * current * inv4pi;
+  for (int ell = 2; ell < n_alpha; ++ell) {
+    float value = ((2 * ell - 1) * x * current - (ell - 1) * previous) / ell;
+    result += (2 * ell + 1) * alpha[ell] * value * inv4pi;
+    previous = current;
+    current = value;
+  }
+  if (result < 0.0f) {
+    // float32 rounding of a zero of the polynomial is not a negative response
+    if (result < -1e-6f * alpha_abs) bad = true;
+    return 0.0f;
+  }
+  return result;
+}
+
+struct O0Shared {
+  double gx[kO0MaxOrder], gw[kO0MaxOrder];
+  float alpha[kO0MaxAlpha];
+  O0Pair pair[kO0Chunk];
+  double warp_charge[kO0Threads / 32];
+  int n_pairs;
+  int n_combos;
+};
+
+__global__ void __launch_bounds__(kO0Threads)
+order0_kernel(const lh_order0_optics O, const lh_order0_batch B) {
+  extern __shared__ __align__(16) unsigned char o0_smem[];
+  O0Shared& S = *reinterpret_cast<O0Shared*>(o0_smem);
+  const int n_panels = O.n_panel_edges - 1;
+  const int nb = B.n_edges - 1;
+  const bool want_bins = B.bins != nullptr;
+  double* sbins = reinterpret_cast<double*>(o0_smem + sizeof(O0Shared));
+  uint32_t* combos = reinterpret_cast<uint32_t*>(sbins + (want_bins ? nb : 0));
+  const int tid = threadIdx.x;
+
+  // chunk -> event
+  const int64_t chunk = blockIdx.x;
+  int lo = 0, hi = B.n_events;  // last event with chunk_offset[ev] <= chunk
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (B.chunk_offset[mid] <= chunk) lo = mid; else hi = mid;
+  }
+  const int ev = lo;
+  const int om = blockIdx.y;
+  const int64_t el_begin = B.element_offset[ev] + (chunk - B.chunk_offset[ev]) * kO0Chunk;
+  const int64_t el_end = min(B.element_offset[ev + 1], el_begin + kO0Chunk);
+  if (el_begin >= el_end) return;
+
+  const int order = O.order;
+  for (int k = tid; k < order; k += blockDim.x) {
+    S.gx[k] = O.gauss_x[k];
+    S.gw[k] = O.gauss_w[k];
+  }
+  for (int k = tid; k < O.n_alpha; k += blockDim.x) S.alpha[k] = (float)O.alpha[k];
+  if (want_bins)
+    for (int k = tid; k < nb; k += blockDim.x) sbins[k] = 0.0;
+  if (tid == 0) S.n_combos = 0;
+
+  double pmin = O.phase[0], pmax = O.phase[0];
+  for (int k = 1; k < O.n_panel_edges; ++k) {
+    pmin = fmin(pmin, O.phase[k]);
+    pmax = fmax(pmax, O.phase[k]);
+  }
+  const double ox = O.om_pos[3 * om], oy = O.om_pos[3 * om + 1], oz = O.om_pos[3 * om + 2];
+  const double radius = O.om_radius[om];
+  uint32_t flags = 0;
+
+  // ---- phase 0: candidates of the chunk (warp 0) and their frames
+  if (tid < 32) {
+    const int64_t i = el_begin + tid;
+    bool keep = false;
+    O0Pair P{};
+    if (i < el_end) {
+      const double beta = B.beta[i], len = B.length[i];
+      const double ux = B.direction[3 * i], uy = B.direction[3 * i + 1], uz = B.direction[3 * i + 2];
+      const double wx = ox - B.start[3 * i], wy = oy - B.start[3 * i + 1], wz = oz - B.start[3 * i + 2];
+      const double z = wx * ux + wy * uy + wz * uz;
+      const bool sphere = radius > 0.0;
+      // interval_candidates with the sphere always in reach and the axis included
+      if (B.c0[i] != 0.0 && beta * pmax > 1.0 && !(z <= 0.0 && (!sphere || z <= -radius))) {
+        const double cx = wy * uz - wz * uy, cy = wz * ux - wx * uz, cz = wx * uy - wy * ux;
+        const double rho_c = sqrt(cx * cx + cy * cy + cz * cz);
+        const double rad = sphere ? radius : 0.0;
+        if (!(z <= 0.0 && rad == 0.0)) {
+          if (rho_c == 0.0) {
+            if (rad == 0.0) {
+              if (0.0 < z && z < len) flags |= LH_STATUS_ON_TRACK;
+            } else {
+              keep = true;
+            }
+          } else if (rad == 0.0) {
+            keep = false;  // a point receiver has no first-entry window: no light on this path
+          } else if (o0_cone_reaches(z, rho_c, len, beta, rad, pmin, pmax)) {
+            double a, b, c, d;
+            keep = o0_support(z, rho_c, len, beta, rad, a, b, c, d) && !(a > pmax || b <= pmin);
+          }
+        }
+      }
+      if (keep) {
+        // _surface_ballistic_rays.py:52-80: frame and support of the pair
+        const double tx = wx - z * ux, ty = wy - z * uy, tz = wz - z * uz;
+        const double rho = sqrt(tx * tx + ty * ty + tz * tz);
+        double nmin, nmax, cut0, cut1;
+        if (!o0_support(z, rho, len, beta, radius, nmin, nmax, cut0, cut1) || nmin > pmax ||
+            nmax <= pmin) {
+          keep = false;
+        } else {
+          const double along_min = z < 0.0 ? z : (z > len ? z - len : 0.0);
+          if (rho * rho + along_min * along_min <= radius * radius) {
+            flags |= LH_STATUS_INSIDE_GLASS;
+            keep = false;
+          } else {
+            double e1x, e1y, e1z;
+            if (rho > 0.0) {
+              e1x = tx / rho; e1y = ty / rho; e1z = tz / rho;
+            } else {
+              double ax = 0, ay = 0, az = 0;
+              if (fabs(ux) < 0.9) ax = 1.0; else ay = 1.0;
+              e1x = uy * az - uz * ay; e1y = uz * ax - ux * az; e1z = ux * ay - uy * ax;
+              double nn = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+              e1x /= nn; e1y /= nn; e1z /= nn;
+            }
+            const double e2x = uy * e1z - uz * e1y, e2y = uz * e1x - ux * e1z,
+                         e2z = ux * e1y - uy * e1x;
+            const double lx = O.om_look[3 * om], ly = O.om_look[3 * om + 1], lz = O.om_look[3 * om + 2];
+            P.z = z; P.rho = rho;
+            P.axial = ux * lx + uy * ly + uz * lz;
+            P.across = e1x * lx + e1y * ly + e1z * lz;
+            P.side = e2x * lx + e2y * ly + e2z * lz;
+            P.nmin = nmin; P.nmax = nmax; P.cut0 = cut0; P.cut1 = cut1;
+            P.tau = (B.t1[i] - B.t0[i]) / len;
+            P.el = (int)(i - el_begin);
+          }
+        }
+      }
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, keep);
+    if (keep) S.pair[__popc(mask & ((1u << tid) - 1u))] = P;
+    if (tid == 0) S.n_pairs = __popc(mask);
+  }
+  __syncthreads();
+  const int n_pairs = S.n_pairs;
+  if (n_pairs == 0) {
+    if (flags) atomicOr(reinterpret_cast<unsigned*>(B.status), flags);
+    return;
+  }
+
+  // ---- phase 1: (pair, panel, piece) work list
+  for (int item = tid; item < n_pairs * n_panels; item += blockDim.x) {
+    const int p = item / n_panels, panel = item - p * n_panels;
+    const O0Pair& P = S.pair[p];
+    const double left = O.panel_edges[panel], width = O.panel_edges[panel + 1] - left;
+    const double n0 = O.phase[panel], dn = O.phase[panel + 1] - n0;
+    double a = left, b = left + width;
+    if (dn == 0.0) {
+      if (n0 < P.nmin || n0 >= P.nmax) continue;
+    } else {
+      double x0 = (P.nmin - n0) / dn, x1 = (P.nmax - n0) / dn;
+      double l = fmin(x0, x1), h = fmax(x0, x1);
+      a = left + width * fmax(l, 0.0);
+      b = left + width * fmin(h, 1.0);
+    }
+    if (a >= b) continue;
+    int pieces = 1;
+    if (dn != 0.0) {
+      double vals[2] = {P.cut0, P.cut1};
+      for (int v = 0; v < 2; ++v)
+        if (isfinite(vals[v])) {
+          double lam = left + width * (vals[v] - n0) / dn;
+          if (a < lam && lam < b) ++pieces;
+        }
+    }
+    const int slot = atomicAdd(&S.n_combos, pieces);
+    for (int k = 0; k < pieces; ++k)
+      combos[slot + k] = (uint32_t)p | ((uint32_t)panel << 8) | ((uint32_t)k << 24);
+  }
+  __syncthreads();
+  const int n_combos = S.n_combos;
+
+  // ---- phase 2: (piece, wavelength node) items
+  const double area_scale = O.om_area[om] / (kPi * radius * radius);
+  const double origin = B.origins[(int64_t)ev * O.n_om + om];
+  const double* edges = B.edges;
+  const int n_edges = B.n_edges;
+  const int64_t el0 = el_begin;
+  float alpha_abs = 0.0f;
+  for (int k = 0; k < O.n_alpha; ++k) alpha_abs += fabsf(S.alpha[k]);
+  alpha_abs = fmaxf(alpha_abs, 1.0f);
+  bool bad_acceptance = false;
+  double charge = 0.0;
+  double scuts[kO0MaxSCuts];
+  double phicuts[kO0MaxPhiCuts];
+
+  for (int item = tid; item < n_combos * order; item += blockDim.x) {
+    const int ci = item / order, ilam = item - ci * order;
+    const uint32_t code = combos[ci];
+    const int p = code & 0xff, panel = (code >> 8) & 0xffff, piece = code >> 24;
+    const O0Pair& P = S.pair[p];
+    const int64_t i = el0 + P.el;
+    const double left = O.panel_edges[panel], width = O.panel_edges[panel + 1] - left;
+    const double n0 = O.phase[panel], dn = O.phase[panel + 1] - n0;
+    double cuts[4];
+    int count = 2;
+    if (dn == 0.0) {
+      cuts[0] = left; cuts[1] = left + width;
+    } else {
+      double x0 = (P.nmin - n0) / dn, x1 = (P.nmax - n0) / dn;
+      cuts[0] = left + width * fmax(fmin(x0, x1), 0.0);
+      cuts[1] = left + width * fmin(fmax(x0, x1), 1.0);
+      double vals[2] = {P.cut0, P.cut1};
+      const double lo_c = cuts[0], hi_c = cuts[1];
+      for (int v = 0; v < 2; ++v)
+        if (isfinite(vals[v])) {
+          double lam = left + width * (vals[v] - n0) / dn;
+          if (lo_c < lam && lam < hi_c) cuts[count++] = lam;
+        }
+      o0_sort(cuts, count);
+    }
+    const double low = cuts[piece], high = cuts[piece + 1];
+    const double beta = B.beta[i], L = B.length[i];
+    const double lam = (low + high) / 2 + (high - low) / 2 * S.gx[ilam];
+    const double q = (lam - left) / width, n = n0 + dn * q, bn = beta * n;
+    if (bn <= 1.0) continue;
+    const double cosine = 1 / bn, sine = sqrt(1 - cosine * cosine);
+    const double z = P.z, rho = P.rho;
+    const double centre = z - rho * cosine / sine, spread = radius / sine;
+    const double slo = fmax(centre - spread, 0.0), shi = fmin(centre + spread, L);
+    if (slo >= shi) continue;
+    const double absorption = O.extinction[panel] + q * (O.extinction[panel + 1] - O.extinction[panel]);
+    const double group = O.group[panel] + q * (O.group[panel + 1] - O.group[panel]);
+    const double velocity = kCVacuumMPerNs / group;
+    const double* ef = O.efficiency + (int64_t)panel * O.eff_cols;
+    double eta = ((ef[3] * q + ef[2]) * q + ef[1]) * q + ef[0];
+    if (O.eff_cols > 4) eta *= exp(ef[4] + q * ef[5]);
+    const double spectral = (B.c0[i] + B.c2[i] / (n * n)) / L / (lam * lam) * eta;
+    const double scale = (high - low) / 2 * S.gw[ilam] * spectral * area_scale;
+    const double t0 = B.t0[i], tau = P.tau;
+
+    // s cuts where a cone ray's entry time crosses a bin edge (_surface_ballistic_rays.py:96-118)
+    scuts[0] = slo;
+    scuts[1] = shi;
+    int ns = 2;
+    {
+      const double d0 = (z - slo) * (z - slo), d1 = (z - shi) * (z - shi);
+      const double rmax = sqrt(rho * rho + fmax(d0, d1));
+      const double rmin = sqrt(rho * rho + ((slo < z && z < shi) ? 0.0 : fmin(d0, d1)));
+      const double e_lo = t0 + tau * slo, e_hi = t0 + tau * shi;
+      const double earliest = fmin(e_lo, e_hi) + (rmin - radius) / velocity - origin;
+      const double latest = fmax(e_lo, e_hi) + rmax / velocity - origin;
+      const int first_edge = o0_search_right(edges, n_edges, earliest);
+      const int last_edge = o0_search_left(edges, n_edges, latest);
+      for (int edge = first_edge; edge < last_edge; ++edge) {
+        const double A = (origin + edges[edge] - t0) * velocity, Bv = tau * velocity;
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+          const double D = cosine * z + sgn * sine * rho;
+          ns = o0_quadratic_cuts(scuts, ns, 1 + Bv * Bv - 2 * Bv * cosine,
+                                 -2 * z - 2 * A * Bv + 2 * (A * cosine + Bv * D),
+                                 z * z + rho * rho - radius * radius + A * A - 2 * A * D, slo, shi);
+        }
+        ns = o0_quadratic_cuts(scuts, ns, Bv * Bv - 1., -2 * A * Bv + 2 * z,
+                               A * A - z * z - rho * rho + radius * radius, slo, shi);
+      }
+    }
+    if (ns > kO0MaxSCuts) {
+      flags |= LH_STATUS_OVERFLOW;
+      continue;
+    }
+    o0_sort(scuts, ns);
+
+    const float cos_f = (float)cosine, sin_f = (float)sine;
+    const float axial = (float)P.axial, across = (float)P.across, side = (float)P.side;
+    const float R2 = (float)(radius * radius);
+    const float absorption_f = (float)absorption;
+    for (int sp = 0; sp < ns - 1; ++sp) {
+      const double sa = scuts[sp], sb = scuts[sp + 1];
+      if (sa >= sb) continue;
+      for (int j = 0; j < order; ++j) {
+        double sin_psi, cos_psi;
+        sincospi(0.5 * S.gx[j], &sin_psi, &cos_psi);
+        const double s = (sa + sb) / 2 + (sb - sa) / 2 * sin_psi;
+        const double ds = (sb - sa) / 2 * cos_psi * kPi / 2 * S.gw[j];
+        const double along = z - s, W2 = rho * rho + along * along, Bq = W2 - radius * radius;
+        double half;
+        if (rho > 0.0) {
+          half = acos(o0_clamp1((sqrt(Bq) - cosine * along) / (sine * rho)));
+        } else {
+          half = cosine * along >= sqrt(Bq) ? kPi : 0.0;
+        }
+        if (half == 0.0) continue;
+        const double emission = t0 + tau * s - origin;
+        const double tmin = emission + o0_entry(Bq, cosine * along + sine * rho) / velocity;
+        const double tmax = emission + o0_entry(Bq, cosine * along + sine * rho * cos(half)) / velocity;
+        phicuts[0] = 0.0;
+        int nphi = 1;
+        if (rho > 0.0) {
+          const int first = o0_search_right(edges, n_edges, tmin);
+          const int last = o0_search_left(edges, n_edges, tmax);
+          for (int edge = first; edge < last; ++edge) {
+            const double distance = (edges[edge] - emission) * velocity;
+            const double dot = (Bq + distance * distance) / (2 * distance);
+            const double phi = acos(o0_clamp1((dot - cosine * along) / (sine * rho)));
+            const double r = phi / half;
+            if (nphi < kO0MaxPhiCuts - 1) phicuts[nphi] = asin(r < 1.0 ? r : 1.0);
+            ++nphi;
+          }
+        }
+        if (nphi > kO0MaxPhiCuts - 1) {
+          flags |= LH_STATUS_OVERFLOW;
+          continue;
+        }
+        phicuts[nphi++] = kPi / 2;
+        // float32 azimuth integrand, entry distance without cancellation
+        const float half_f = (float)half;
+        const float W2_f = (float)W2, B_f = (float)Bq;
+        const float E0 = (float)(along * sine - rho * cosine);
+        const float Sa = (float)(along * sine);
+        const float along_cos = (float)(cosine * along), rho_sin = (float)(sine * rho);
+        const float sin2W2 = sin_f * sin_f * W2_f;
+        for (int pp = 0; pp < nphi - 1; ++pp) {
+          const double pa = phicuts[pp], pb = phicuts[pp + 1];
+          if (pa >= pb) continue;
+          const float mid = (float)((pa + pb) / 2), hw = (float)((pb - pa) / 2);
+          float integral = 0.0f;
+          for (int jp = 0; jp < order; ++jp) {
+            float s_eta, c_eta;
+            sincosf(mid + hw * (float)S.gx[jp], &s_eta, &c_eta);
+            const float phi = half_f * s_eta;
+            const float dphi = half_f * c_eta * hw * (float)S.gw[jp];
+            float ss, cp;
+            sincosf(phi, &ss, &cp);
+            const float sh = sinf(0.5f * phi);
+            const float E = E0 - Sa * (2.0f * sh * sh);
+            const float D = R2 - (sin2W2 * ss * ss + E * E);
+            const float dot = along_cos + rho_sin * cp;
+            const float distance = B_f / (dot + sqrtf(fmaxf(D, 0.0f)));
+            const float x1 = cos_f * axial + sin_f * (cp * across + ss * side);
+            const float x2 = cos_f * axial + sin_f * (cp * across - ss * side);
+            const float accept = o0_acceptance(S.alpha, O.n_alpha, x1, alpha_abs, bad_acceptance) +
+                                 o0_acceptance(S.alpha, O.n_alpha, x2, alpha_abs, bad_acceptance);
+            integral += dphi * accept * expf(-absorption_f * distance);
+          }
+          const double value = scale * ds * (double)integral * (1.0 / (2 * kPi));
+          charge += value;
+          if (want_bins) {
+            const double phi_mid = half * sin((pa + pb) / 2);
+            const double arrival =
+                emission + o0_entry(Bq, cosine * along + sine * rho * cos(phi_mid)) / velocity;
+            const int slot = o0_search_right(edges, n_edges, arrival) - 1;
+            if (slot >= 0 && slot < nb) atomicAdd(&sbins[slot], value);
+          }
+        }
+      }
+    }
+  }
+  if (bad_acceptance) flags |= LH_STATUS_NEGATIVE_ACCEPTANCE;
+
+  // ---- charge: warp shuffles, then one add per CTA; bins: one add per nonzero bin
+  for (int off = 16; off > 0; off >>= 1) charge += __shfl_xor_sync(0xffffffffu, charge, off);
+  if ((tid & 31) == 0) S.warp_charge[tid >> 5] = charge;
+  __syncthreads();
+  if (tid == 0) {
+    double total = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += S.warp_charge[w];
+    if (total != 0.0) atomicAdd(&B.charge[(int64_t)ev * O.n_om + om], total);
+  }
+  if (want_bins) {
+    double* out = B.bins + ((int64_t)ev * O.n_om + om) * nb;
+    for (int k = tid; k < nb; k += blockDim.x)
+      if (sbins[k] != 0.0) atomicAdd(&out[k], sbins[k]);
+  }
+  if (flags) atomicOr(reinterpret_cast<unsigned*>(B.status), flags);
+}
+
+size_t order0_shared_bytes(const lh_order0_optics& O, const lh_order0_batch& B) {
+  const int n_panels = O.n_panel_edges - 1;
+  size_t bytes = sizeof(O0Shared);
+  if (B.bins) bytes += sizeof(double) * (size_t)(B.n_edges - 1);
+  bytes += sizeof(uint32_t) * (size_t)kO0Chunk * n_panels * 3;
+  return bytes;
+}
+
+int order0_launch(const lh_order0_optics& O, const lh_order0_batch& B, cudaStream_t s) {
+  const size_t smem = order0_shared_bytes(O, B);
+  if (smem > 200 * 1024) return LH_EUNSUPPORTED;
+  if (cudaFuncSetAttribute(order0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return LH_ECUDA;
+  cudaMemsetAsync(B.charge, 0, sizeof(double) * (size_t)B.n_events * O.n_om, s);
+  if (B.bins)
+    cudaMemsetAsync(B.bins, 0, sizeof(double) * (size_t)B.n_events * O.n_om * (B.n_edges - 1), s);
+  if (B.n_chunks == 0) return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+  dim3 grid((unsigned)B.n_chunks, (unsigned)O.n_om);
+  order0_kernel<<<grid, kO0Threads, smem, s>>>(O, B);
+  return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+}
+
+bool order0_valid(const lh_order0_optics* O, const lh_order0_batch* B) {
+  if (!O || !B) return false;
+  if (O->n_om < 1 || O->n_om > 65535 || !O->om_pos || !O->om_look || !O->om_area || !O->om_radius)
+    return false;
+  if (O->n_alpha < 1 || O->n_alpha > kO0MaxAlpha || !O->alpha) return false;
+  if (O->n_panel_edges < 2 || O->n_panel_edges - 1 > kO0MaxPanels || !O->panel_edges ||
+      !O->phase || !O->group || !O->extinction || !O->efficiency)
+    return false;
+  if (O->eff_cols != 4 && O->eff_cols != 6) return false;
+  if (O->order < 1 || O->order > kO0MaxOrder || !O->gauss_x || !O->gauss_w) return false;
+  if (B->n_events < 1 || !B->element_offset || !B->chunk_offset || B->n_chunks < 0 ||
+      B->n_chunks > 0x7fffffff)
+    return false;
+  if (B->n_edges < 2 || !B->edges || !B->origins || !B->charge || !B->status) return false;
+  if (B->n_chunks && (!B->start || !B->direction || !B->length || !B->c0 || !B->c2 || !B->beta ||
+                      !B->t0 || !B->t1))
+    return false;
+  return true;
+}
+
+}  // namespace lh
+
+extern "C" size_t lh_order0_chunks(const int64_t* element_counts, int32_t n_events,
+                                   int64_t* chunk_offset_host) {
+  if (!element_counts || n_events < 1) return 0;
+  int64_t total = 0;
+  for (int e = 0; e < n_events; ++e) {
+    if (chunk_offset_host) chunk_offset_host[e] = total;
+    total += (element_counts[e] + lh::kO0Chunk - 1) / lh::kO0Chunk;
+  }
+  if (chunk_offset_host) chunk_offset_host[n_events] = total;
+  return (size_t)total;
+}
+
+extern "C" int lh_order0(const lh_order0_optics* optics, const lh_order0_batch* batch,
+                         void* stream) {
+  if (!lh::order0_valid(optics, batch)) return LH_EINVAL;
+  return lh::order0_launch(*optics, *batch, static_cast<cudaStream_t>(stream));
+}
