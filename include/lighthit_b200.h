@@ -238,6 +238,96 @@ size_t lh_order0_chunks(const int64_t* element_counts, int32_t n_events, int64_t
 
 int lh_order0(const lh_order0_optics* optics, const lh_order0_batch* batch, void* stream);
 
+/* ------------------------------------------------------------------ order 1
+ * Replaces the grouped order 1 of transport_prompt (prompt.py:1020-1258):
+ * stage A `compress` (prompt.py:1317-1402; _prompt_numba.py:1094-1232 and
+ * finish_pencils :2247-2354) turns elements into (cell, pixel) pencils;
+ * stage B `grouped_pencils_order1` (_prompt_numba.py:1750-2086) merges them per
+ * OM into (tau, r, theta) groups and deposits each (tau, r) batch's single-
+ * scattering profile into the bins. All float64.
+ */
+typedef struct {
+  int32_t n_om;
+  const double* om_pos;        /* [n_om][3]                                         */
+  const double* om_look;       /* [n_om][3] looks = -orientations                   */
+  const double* om_area;       /* [n_om] effective area m^2                         */
+  int32_t n_bands;             /* wavelength bands of the unit (<= 8)               */
+  const double* mus;           /* [n_bands] scattering 1/m                          */
+  const double* mut;           /* [n_bands] extinction 1/m                          */
+  const double* speed;         /* [n_bands] group speed m/ns                        */
+  const double* s0w;           /* [n_bands] C0 spectral weight (prompt.py:429)      */
+  const double* s2w;           /* [n_bands] C2 spectral weight                       */
+  double g;                    /* Henyey-Greenstein asymmetry                        */
+  int32_t n_mono;              /* acceptance monomials (prompt.py:380-399) (<= 10)   */
+  const double* coef;          /* [n_mono]                                          */
+  const int32_t* ipow;         /* [n_mono]                                          */
+  const int32_t* jpow;         /* [n_mono]                                          */
+  int32_t max_power;           /* acceptance degree (<= 4)                           */
+  int32_t n_edges;
+  const double* edges;         /* [n_edges] relative time edges ns                   */
+  const double* eedge;         /* [n_bands][n_edges] exp(kappa edges), kappa = -mut v */
+  const double* itab;          /* [n_bands][n_edges-1][3] interval_table             */
+  int32_t compute_bins;        /* 0: charge only                                     */
+  /* PromptConfig (prompt.py:154-196) */
+  double cell_m;               /* pencil position cell                               */
+  int32_t pixel_face;          /* cube-sphere pixels per face edge                   */
+  int32_t ring_nodes;          /* Cherenkov ring azimuths per sub-segment            */
+  double path_step, path_step_tail, tail_exponent;
+  int32_t direct_bins, max_path_nodes;  /* max_path_nodes <= 2048                    */
+  double smoothing_factor;
+  double theta_lo, theta_ratio, tau_step, log_r_step;  /* merge_theta_min/ratio/tau/log_r */
+  int32_t theta_bins;          /* 2 + int(log(pi / theta_lo) / log(1 + theta_ratio)) */
+  double speed_ref;            /* max band speed                                     */
+  int32_t n_gauss;             /* nodes of the Gaussian 1/theta mean (48)            */
+  const double* gauss_tau;     /* [n_gauss] on [0, pi/2]                              */
+  const double* gauss_w;       /* [n_gauss]                                          */
+  int32_t group_capacity;      /* group table slots per OM (power of two, <= 16384)  */
+} lh_order1_config;
+
+typedef struct {
+  int32_t n_el;
+  int64_t n_subseg;            /* sum of max(1, ceil(length / (cell_m / 2)))         */
+  const int64_t* subseg_offset;/* [n_el + 1] device                                  */
+  const double* start;         /* [n_el][3]                                          */
+  const double* direction;     /* [n_el][3]                                          */
+  const double* length;        /* [n_el]                                             */
+  const double* c0;            /* [n_el]                                             */
+  const double* c2;            /* [n_el]                                             */
+  const double* cone_cos;      /* [n_el] frozen cone cosine 1/(beta n_cone)          */
+  const double* t0;            /* [n_el]                                             */
+  const double* t1;            /* [n_el]                                             */
+  double grid_origin[3];       /* host values: cell grid origin (prompt.py:1321-1326) */
+  int64_t grid_dims[3];        /* host values: cells per axis                        */
+} lh_order1_elements;
+
+typedef struct {
+  int32_t capacity;            /* rows allocated                                     */
+  double* position;            /* [capacity][3]                                      */
+  double* direction;           /* [capacity][3]                                      */
+  double* w0;                  /* [capacity]                                         */
+  double* w2;                  /* [capacity]                                         */
+  double* time;                /* [capacity]                                         */
+  double* major;               /* [capacity][3]                                      */
+  double* var_major;           /* [capacity]                                         */
+  double* var_minor;           /* [capacity]                                         */
+  double* pos_cov;             /* [capacity][6] xx yy zz xy xz yz                    */
+} lh_order1_pencil_table;
+
+/* Workspace for n_subseg sub-segments and n_work OMs (both stages). */
+size_t lh_order1_workspace_bytes(const lh_order1_config* config, int64_t n_subseg, int32_t n_work);
+
+/* Stage A: pencils of the elements; *n_pencils_device receives the count. */
+int lh_order1_pencils(const lh_order1_config* config, const lh_order1_elements* elements,
+                      const lh_order1_pencil_table* pencils, int32_t* n_pencils_device,
+                      void* workspace, size_t workspace_bytes, int32_t* status, void* stream);
+
+/* Stage B: charge[n_om] and bins[n_om][n_edges-1] of the OMs in work[n_work]
+ * (others zero), clocks origins[n_om]. */
+int lh_order1_grouped(const lh_order1_config* config, const lh_order1_pencil_table* pencils,
+                      int32_t n_pencils, const int32_t* work, int32_t n_work,
+                      const double* origins, double* charge, double* bins, void* workspace,
+                      size_t workspace_bytes, int32_t* status, void* stream);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

@@ -78,6 +78,33 @@ class Order0Batch(C.Structure):
                 ("status", P)]
 
 
+class Order1Config(C.Structure):
+    _fields_ = [("n_om", C.c_int32), ("om_pos", P), ("om_look", P), ("om_area", P),
+                ("n_bands", C.c_int32), ("mus", P), ("mut", P), ("speed", P), ("s0w", P),
+                ("s2w", P), ("g", C.c_double), ("n_mono", C.c_int32), ("coef", P), ("ipow", P),
+                ("jpow", P), ("max_power", C.c_int32), ("n_edges", C.c_int32), ("edges", P),
+                ("eedge", P), ("itab", P), ("compute_bins", C.c_int32), ("cell_m", C.c_double),
+                ("pixel_face", C.c_int32), ("ring_nodes", C.c_int32), ("path_step", C.c_double),
+                ("path_step_tail", C.c_double), ("tail_exponent", C.c_double),
+                ("direct_bins", C.c_int32), ("max_path_nodes", C.c_int32),
+                ("smoothing_factor", C.c_double), ("theta_lo", C.c_double),
+                ("theta_ratio", C.c_double), ("tau_step", C.c_double), ("log_r_step", C.c_double),
+                ("theta_bins", C.c_int32), ("speed_ref", C.c_double), ("n_gauss", C.c_int32),
+                ("gauss_tau", P), ("gauss_w", P), ("group_capacity", C.c_int32)]
+
+
+class Order1Elements(C.Structure):
+    _fields_ = [("n_el", C.c_int32), ("n_subseg", C.c_int64), ("subseg_offset", P),
+                ("start", P), ("direction", P), ("length", P), ("c0", P), ("c2", P),
+                ("cone_cos", P), ("t0", P), ("t1", P), ("grid_origin", C.c_double * 3),
+                ("grid_dims", C.c_int64 * 3)]
+
+
+class Order1PencilTable(C.Structure):
+    _fields_ = [("capacity", C.c_int32), ("position", P), ("direction", P), ("w0", P), ("w2", P),
+                ("time", P), ("major", P), ("var_major", P), ("var_minor", P), ("pos_cov", P)]
+
+
 # name -> (restype, argtypes); every symbol the header declares
 SIGNATURES = {
     "lh_version": (C.c_char_p, []),
@@ -96,6 +123,11 @@ SIGNATURES = {
     "lh_ge2_apply": (C.c_int, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem), P, C.c_size_t, P]),
     "lh_order0_chunks": (C.c_size_t, [P, C.c_int32, P]),
     "lh_order0": (C.c_int, [C.POINTER(Order0Optics), C.POINTER(Order0Batch), P]),
+    "lh_order1_workspace_bytes": (C.c_size_t, [C.POINTER(Order1Config), C.c_int64, C.c_int32]),
+    "lh_order1_pencils": (C.c_int, [C.POINTER(Order1Config), C.POINTER(Order1Elements),
+                                    C.POINTER(Order1PencilTable), P, P, C.c_size_t, P, P]),
+    "lh_order1_grouped": (C.c_int, [C.POINTER(Order1Config), C.POINTER(Order1PencilTable),
+                                    C.c_int32, P, C.c_int32, P, P, P, P, C.c_size_t, P, P]),
 }
 LH_ESCRATCH = 6
 

@@ -1,0 +1,1085 @@
+// Order 1 (single scattering) of spectral elements, grouped pencils.
+//
+// Reference: transport_prompt's grouped order 1 (prompt.py:1020-1258) with
+//   stage A  compress (prompt.py:1317-1402): subsegment_cells,
+//            compress_subsegments, finish_pencils (_prompt_numba.py:1094-1232,
+//            2247-2354): every element is cut into ceil(L / a_step)
+//            sub-segments, each sub-segment's Cherenkov ring is sampled at
+//            `ring_nodes` azimuths, and the nodes are summed into
+//            (0.5 m position cell, cube-sphere direction pixel) pencils that
+//            carry 23 moments (weights, mean position/time/direction and their
+//            covariances);
+//   stage B  grouped_pencils_order1 (_prompt_numba.py:1750-2086): for each OM
+//            the pencils are merged into (tau, log r, hemisphere, theta) groups
+//            carrying acceptance moments; the groups of one (tau, r) batch
+//            share a path grid in asinh((S - r) / sigma), their single-
+//            scattering profile is summed on it, and the profile is deposited
+//            per wavelength band as exact exp x quadratic panels into the bins
+//            (_batch_grid, _batch_add_moments, _batch_deposit, _deposit_panel,
+//            _finalize: _prompt_numba.py:157-632).
+//
+// B200 layout. Stage A: one thread per ring node writes its moments into a
+// global open-addressing table keyed by (cell, pixel) with float64 atomics;
+// one thread per occupied slot then forms the pencil. Stage B: one thread per
+// (OM, pencil) computes the pencil's geometry against the OM and adds its
+// moments into that OM's group table (atomics); one CTA per OM sorts its
+// group keys in shared memory (bitonic) and emits its batches; a persistent
+// grid of CTAs takes batches from the global list, builds each batch's path
+// grid and profile in shared memory and deposits its panels; one CTA per OM
+// finishes the bins with the prefix pass. Everything is float64, as the
+// deposit's global quadratic coefficients in t cancel strongly.
+#include <algorithm>
+
+#include "lh_common.cuh"
+
+namespace lh {
+
+constexpr int kO1MaxNodes = 2048;
+constexpr int kO1MaxMono = 10;
+constexpr int kO1MaxValues = 2 * kO1MaxMono + 6;
+constexpr int kO1MaxBands = 8;
+constexpr int kO1MaxGauss = 64;
+constexpr int kO1Moments = 23;
+constexpr int kO1GroupSort = 8192;  // groups per OM sorted in one CTA
+constexpr int kO1BatchThreads = 128;
+
+LH_DEVICE uint64_t o1_mix(uint64_t v) {
+  v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ull;
+  v = (v ^ (v >> 27)) * 0x94d049bb133111ebull;
+  return v ^ (v >> 31);
+}
+
+// Insert `key` (>= 0) into an open-addressing table of `capacity` (power of
+// two) slots holding -1 when free. Returns the slot, or -1 when full; `fresh`
+// tells whether this call claimed it.
+LH_DEVICE int64_t o1_insert(long long* keys, int64_t capacity, long long key, bool& fresh) {
+  const uint64_t mask = (uint64_t)capacity - 1;
+  uint64_t slot = o1_mix((uint64_t)key) & mask;
+  fresh = false;
+  for (int64_t probe = 0; probe < capacity; ++probe) {
+    long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(keys + slot),
+                               (unsigned long long)(-1ll), (unsigned long long)key);
+    if (prev == -1ll) {
+      fresh = true;
+      return (int64_t)slot;
+    }
+    if (prev == key) return (int64_t)slot;
+    slot = (slot + 1) & mask;
+  }
+  return -1;
+}
+
+// ------------------------------------------------------------------ stage A
+
+// Equi-angular cube-sphere pixel (_prompt_numba.py:1015-1043)
+LH_DEVICE int o1_pixel(double sx, double sy, double sz, int n_face) {
+  const double ax = fabs(sx), ay = fabs(sy), az = fabs(sz);
+  int face;
+  double u, v;
+  if (ax >= ay && ax >= az) {
+    face = sx > 0 ? 0 : 1; u = sy / ax; v = sz / ax;
+  } else if (ay >= az) {
+    face = sy > 0 ? 2 : 3; u = sx / ay; v = sz / ay;
+  } else {
+    face = sz > 0 ? 4 : 5; u = sx / az; v = sy / az;
+  }
+  const double quarter = 0.25 * kPi;
+  int i = (int)((atan(u) + quarter) / (2.0 * quarter) * n_face);
+  int j = (int)((atan(v) + quarter) / (2.0 * quarter) * n_face);
+  i = min(max(i, 0), n_face - 1);
+  j = min(max(j, 0), n_face - 1);
+  return (face * n_face + i) * n_face + j;
+}
+
+struct O1Subseg {
+  double px, py, pz, t;
+};
+
+LH_DEVICE O1Subseg o1_subseg(const lh_order1_elements& E, int64_t i, int64_t ia, int64_t n_a) {
+  const double frac = (ia + 0.5) / n_a;
+  O1Subseg s;
+  s.px = E.start[3 * i] + frac * E.length[i] * E.direction[3 * i];
+  s.py = E.start[3 * i + 1] + frac * E.length[i] * E.direction[3 * i + 1];
+  s.pz = E.start[3 * i + 2] + frac * E.length[i] * E.direction[3 * i + 2];
+  s.t = E.t0[i] + frac * (E.t1[i] - E.t0[i]);
+  return s;
+}
+
+// One thread per (sub-segment, ring node): compress_subsegments
+// (_prompt_numba.py:1122-1232) with the ring rotation evaluated directly.
+__global__ void o1_ring_kernel(const lh_order1_config C, const lh_order1_elements E,
+                               const int64_t* subseg_offset, int64_t n_subseg,
+                               long long* keys, int64_t capacity, double* rows,
+                               int32_t* status) {
+  const int64_t total = n_subseg * C.ring_nodes;
+  const int n_pix = 6 * C.pixel_face * C.pixel_face;
+  const double golden = 0.6180339887498949;
+  const double two_pi = 2.0 * kPi;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t sub = k / C.ring_nodes;
+    const int q = (int)(k - sub * C.ring_nodes);
+    // element of this sub-segment: last i with subseg_offset[i] <= sub
+    int64_t lo = 0, hi = E.n_el;
+    while (hi - lo > 1) {
+      int64_t mid = (lo + hi) >> 1;
+      if (subseg_offset[mid] <= sub) lo = mid; else hi = mid;
+    }
+    const int64_t i = lo;
+    const int64_t ia = sub - subseg_offset[i];
+    const int64_t n_a = subseg_offset[i + 1] - subseg_offset[i];
+    const double ux = E.direction[3 * i], uy = E.direction[3 * i + 1], uz = E.direction[3 * i + 2];
+    double hx, hy, hz;
+    if (fabs(uz) < 0.9) { hx = 0.0; hy = 0.0; hz = 1.0; } else { hx = 1.0; hy = 0.0; hz = 0.0; }
+    double e1x = uy * hz - uz * hy, e1y = uz * hx - ux * hz, e1z = ux * hy - uy * hx;
+    const double norm = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+    e1x /= norm; e1y /= norm; e1z /= norm;
+    const double e2x = uy * e1z - uz * e1y, e2y = uz * e1x - ux * e1z, e2z = ux * e1y - uy * e1x;
+    const double cc = E.cone_cos[i];
+    const double cs = sqrt(fmax(1.0 - cc * cc, 0.0));
+    const double share = 1.0 / ((double)n_a * C.ring_nodes);
+    const double arc = two_pi * cs / C.ring_nodes;
+    const double arc2 = arc * arc / 12.0;
+    const double sl = E.length[i] / n_a;
+    const double sub2 = sl * sl / 12.0;
+    const double w0 = E.c0[i] * share, w2 = E.c2[i] * share;
+    const double ig = (double)i * golden;
+    const double offset = (ig - floor(ig)) * two_pi / C.ring_nodes;
+    const O1Subseg P = o1_subseg(E, i, ia, n_a);
+    const long long cx = min(max((long long)floor((P.px - E.grid_origin[0]) / C.cell_m), 0ll), (long long)E.grid_dims[0] - 1);
+    const long long cy = min(max((long long)floor((P.py - E.grid_origin[1]) / C.cell_m), 0ll), (long long)E.grid_dims[1] - 1);
+    const long long cz = min(max((long long)floor((P.pz - E.grid_origin[2]) / C.cell_m), 0ll), (long long)E.grid_dims[2] - 1);
+    const long long cell = (cx * E.grid_dims[1] + cy) * E.grid_dims[2] + cz;
+    double sp, cp;
+    sincos(offset + two_pi * q / C.ring_nodes, &sp, &cp);
+    const double sx = cc * ux + cs * (cp * e1x + sp * e2x);
+    const double sy = cc * uy + cs * (cp * e1y + sp * e2y);
+    const double sz = cc * uz + cs * (cp * e1z + sp * e2z);
+    const long long key = cell * n_pix + o1_pixel(sx, sy, sz, C.pixel_face);
+    bool fresh;
+    const int64_t slot = o1_insert(keys, capacity, key, fresh);
+    if (slot < 0) {
+      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+      continue;
+    }
+    double* row = rows + slot * kO1Moments;
+    const double px = P.px, py = P.py, pz = P.pz, t = P.t;
+    const double tx = -sp * e1x + cp * e2x, ty = -sp * e1y + cp * e2y, tz = -sp * e1z + cp * e2z;
+    atomicAdd(row + 0, w0);
+    atomicAdd(row + 1, w2);
+    atomicAdd(row + 2, w0 * px);
+    atomicAdd(row + 3, w0 * py);
+    atomicAdd(row + 4, w0 * pz);
+    atomicAdd(row + 5, w0 * t);
+    atomicAdd(row + 6, w0 * sx);
+    atomicAdd(row + 7, w0 * sy);
+    atomicAdd(row + 8, w0 * sz);
+    atomicAdd(row + 9, w0 * (px * px + py * py + pz * pz + sub2));
+    atomicAdd(row + 10, w0 * t * t);
+    atomicAdd(row + 11, w0 * (sx * sx + arc2 * tx * tx));
+    atomicAdd(row + 12, w0 * (sy * sy + arc2 * ty * ty));
+    atomicAdd(row + 13, w0 * (sz * sz + arc2 * tz * tz));
+    atomicAdd(row + 14, w0 * (sx * sy + arc2 * tx * ty));
+    atomicAdd(row + 15, w0 * (sx * sz + arc2 * tx * tz));
+    atomicAdd(row + 16, w0 * (sy * sz + arc2 * ty * tz));
+    atomicAdd(row + 17, w0 * (px * px + sub2 * ux * ux));
+    atomicAdd(row + 18, w0 * (py * py + sub2 * uy * uy));
+    atomicAdd(row + 19, w0 * (pz * pz + sub2 * uz * uz));
+    atomicAdd(row + 20, w0 * (px * py + sub2 * ux * uy));
+    atomicAdd(row + 21, w0 * (px * pz + sub2 * ux * uz));
+    atomicAdd(row + 22, w0 * (py * pz + sub2 * uy * uz));
+  }
+}
+
+// One thread per table slot: finish_pencils (_prompt_numba.py:2247-2354) for
+// slots with a positive weight, compacted into the pencil table.
+__global__ void o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
+                                 lh_order1_pencil_table Pn, int32_t* count, int32_t* status) {
+  for (int64_t slot = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; slot < capacity;
+       slot += (int64_t)gridDim.x * blockDim.x) {
+    if (keys[slot] == -1ll) continue;
+    const double* a = rows + slot * kO1Moments;
+    const double w = a[0];
+    if (!(w > 0.0)) continue;
+    const int q = atomicAdd(count, 1);
+    if (q >= Pn.capacity) {
+      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+      continue;
+    }
+    const double mx = a[2] / w, my = a[3] / w, mz = a[4] / w;
+    Pn.position[3 * q] = mx; Pn.position[3 * q + 1] = my; Pn.position[3 * q + 2] = mz;
+    Pn.time[q] = a[5] / w;
+    Pn.w0[q] = w;
+    Pn.w2[q] = a[1];
+    const double rx = a[6] / w, ry = a[7] / w, rz = a[8] / w;
+    const double norm = sqrt(rx * rx + ry * ry + rz * rz);
+    const double dx = rx / norm, dy = ry / norm, dz = rz / norm;
+    Pn.direction[3 * q] = dx; Pn.direction[3 * q + 1] = dy; Pn.direction[3 * q + 2] = dz;
+    const double cxx = a[11] / w - rx * rx, cyy = a[12] / w - ry * ry, czz = a[13] / w - rz * rz;
+    const double cxy = a[14] / w - rx * ry, cxz = a[15] / w - rx * rz, cyz = a[16] / w - ry * rz;
+    double hx, hy, hz;
+    if (fabs(dz) < 0.9) { hx = 0.0; hy = 0.0; hz = 1.0; } else { hx = 1.0; hy = 0.0; hz = 0.0; }
+    double e1x = dy * hz - dz * hy, e1y = dz * hx - dx * hz, e1z = dx * hy - dy * hx;
+    const double nn = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+    e1x /= nn; e1y /= nn; e1z /= nn;
+    const double e2x = dy * e1z - dz * e1y, e2y = dz * e1x - dx * e1z, e2z = dx * e1y - dy * e1x;
+    const double c11 = e1x * (cxx * e1x + cxy * e1y + cxz * e1z) + e1y * (cxy * e1x + cyy * e1y + cyz * e1z) +
+                       e1z * (cxz * e1x + cyz * e1y + czz * e1z);
+    const double c22 = e2x * (cxx * e2x + cxy * e2y + cxz * e2z) + e2y * (cxy * e2x + cyy * e2y + cyz * e2z) +
+                       e2z * (cxz * e2x + cyz * e2y + czz * e2z);
+    const double c12 = e1x * (cxx * e2x + cxy * e2y + cxz * e2z) + e1y * (cxy * e2x + cyy * e2y + cyz * e2z) +
+                       e1z * (cxz * e2x + cyz * e2y + czz * e2z);
+    const double half = 0.5 * (c11 + c22);
+    const double disc = sqrt(fmax(0.25 * (c11 - c22) * (c11 - c22) + c12 * c12, 0.0));
+    Pn.var_major[q] = fmax(half + disc, 0.0);
+    Pn.var_minor[q] = fmax(half - disc, 0.0);
+    double sa, ca;
+    sincos(0.5 * atan2(2.0 * c12, c11 - c22), &sa, &ca);
+    Pn.major[3 * q] = ca * e1x + sa * e2x;
+    Pn.major[3 * q + 1] = ca * e1y + sa * e2y;
+    Pn.major[3 * q + 2] = ca * e1z + sa * e2z;
+    Pn.pos_cov[6 * q] = fmax(a[17] / w - mx * mx, 0.0);
+    Pn.pos_cov[6 * q + 1] = fmax(a[18] / w - my * my, 0.0);
+    Pn.pos_cov[6 * q + 2] = fmax(a[19] / w - mz * mz, 0.0);
+    Pn.pos_cov[6 * q + 3] = a[20] / w - mx * my;
+    Pn.pos_cov[6 * q + 4] = a[21] / w - mx * mz;
+    Pn.pos_cov[6 * q + 5] = a[22] / w - my * mz;
+  }
+}
+
+// ------------------------------------------------------------------ stage B
+
+// gauss_inverse_mean_prepared (_prompt_numba.py:115-129)
+LH_DEVICE double o1_gauss_inverse_mean(double u, double v, double var_u, double var_v,
+                                       const double* tangent, const double* wsec2, int n) {
+  const double scale = 2.0 * (var_u + var_v) + u * u + v * v;
+  if (scale <= 0.0) return 1e300;
+  const double s0 = 1.0 / sqrt(scale);
+  double total = 0.0;
+  for (int k = 0; k < n; ++k) {
+    const double s = s0 * tangent[k], s2 = s * s;
+    const double a = 1.0 + 2.0 * s2 * var_u, b = 1.0 + 2.0 * s2 * var_v;
+    total += wsec2[k] * exp(-s2 * (u * u / a + v * v / b)) / sqrt(a * b);
+  }
+  return 2.0 / sqrt(kPi) * s0 * total;
+}
+
+struct O1GroupShared {
+  double tangent[kO1MaxGauss], wsec2[kO1MaxGauss];
+  double coef[kO1MaxMono];
+  int ipow[kO1MaxMono], jpow[kO1MaxMono];
+};
+
+// One thread per (work OM, pencil): _grouped_pencils_order1_block's pencil
+// loop (_prompt_numba.py:1827-1921) with the generic moment layout.
+__global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
+                                int32_t n_pencils, const int32_t* work, int32_t n_work,
+                                const double* origins, long long* gkeys, double* grows,
+                                int32_t* gcount, int32_t* status) {
+  __shared__ O1GroupShared S;
+  for (int k = threadIdx.x; k < C.n_gauss; k += blockDim.x) {
+    const double t = tan(C.gauss_tau[k]);
+    S.tangent[k] = t;
+    S.wsec2[k] = C.gauss_w[k] * (1.0 + t * t);
+  }
+  for (int k = threadIdx.x; k < C.n_mono; k += blockDim.x) {
+    S.coef[k] = C.coef[k];
+    S.ipow[k] = C.ipow[k];
+    S.jpow[k] = C.jpow[k];
+  }
+  __syncthreads();
+  const int n_values = 2 * C.n_mono + 6;
+  const double log_theta_ratio = log(1.0 + C.theta_ratio);
+  const int theta_bins = C.theta_bins;
+  const int64_t cap = C.group_capacity;
+  const int64_t total = (int64_t)n_work * n_pencils;
+  for (int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; item < total;
+       item += (int64_t)gridDim.x * blockDim.x) {
+    const int w = (int)(item / n_pencils);
+    const int p = (int)(item - (int64_t)w * n_pencils);
+    const int d = work[w];
+    const double rx = C.om_pos[3 * d], ry = C.om_pos[3 * d + 1], rz = C.om_pos[3 * d + 2];
+    const double nx = C.om_look[3 * d], ny = C.om_look[3 * d + 1], nz = C.om_look[3 * d + 2];
+    // _prepare_receiver_geometry (_prompt_numba.py:1590-1612)
+    const double dx = rx - Pn.position[3 * p], dy = ry - Pn.position[3 * p + 1],
+                 dz = rz - Pn.position[3 * p + 2];
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const double hx = dx / r, hy = dy / r, hz = dz / r;
+    const double t_emit = Pn.time[p] - origins[d];
+    const double tau = t_emit + r / C.speed_ref;
+    const double log_r = log(r);
+    const long long key0 = (long long)floor(log_r / C.log_r_step) + (1ll << 20);
+    const long long key1 =
+        min(max((long long)floor(tau / C.tau_step) + (1ll << 20), 0ll), (1ll << 21) - 1);
+    const long long base = ((key1 << 21) + key0) * 2 * theta_bins;
+    // _pencil_frame_from_ray_cached_look (_prompt_numba.py:594-606)
+    const double sx = Pn.direction[3 * p], sy = Pn.direction[3 * p + 1], sz = Pn.direction[3 * p + 2];
+    const double c1 = sx * nx + sy * ny + sz * nz;
+    const double cosine = hx * sx + hy * sy + hz * sz;
+    const double qx = hx - cosine * sx, qy = hy - cosine * sy, qz = hz - cosine * sz;
+    const double sine = sqrt(qx * qx + qy * qy + qz * qz);
+    const double c3 = sine > 1e-300 ? (qx * nx + qy * ny + qz * nz) / sine : 0.0;
+    double theta = atan2(sine, cosine);
+    const bool backward = theta > 0.5 * kPi;
+    double weight;
+    bool averaged = false;
+    const double ax = Pn.major[3 * p], ay = Pn.major[3 * p + 1], az = Pn.major[3 * p + 2];
+    const double* cov = Pn.pos_cov + 6 * p;
+    // _prepare_pencil_shape (_prompt_numba.py:1347-1370)
+    const double bx = sy * az - sz * ay, by = sz * ax - sx * az, bz = sx * ay - sy * ax;
+    const double trace = cov[0] + cov[1] + cov[2];
+    if (backward) {
+      weight = 1.0 / r;
+    } else {
+      const double bound = Pn.var_major[p] + Pn.var_minor[p] + trace / (r * r);
+      if (sine > 1e-300 && bound < 1e-4 * sine * sine) {
+        weight = (1.0 / sine) / r;
+      } else {
+        // _pencil_shape_factor_from_ray (_prompt_numba.py:1389-1436)
+        const double caa = ax * (cov[0] * ax + cov[3] * ay + cov[4] * az) +
+                           ay * (cov[3] * ax + cov[1] * ay + cov[5] * az) +
+                           az * (cov[4] * ax + cov[5] * ay + cov[2] * az);
+        const double cbb = bx * (cov[0] * bx + cov[3] * by + cov[4] * bz) +
+                           by * (cov[3] * bx + cov[1] * by + cov[5] * bz) +
+                           bz * (cov[4] * bx + cov[5] * by + cov[2] * bz);
+        const double cab = ax * (cov[0] * bx + cov[3] * by + cov[4] * bz) +
+                           ay * (cov[3] * bx + cov[1] * by + cov[5] * bz) +
+                           az * (cov[4] * bx + cov[5] * by + cov[2] * bz);
+        const double inv_r2 = 1.0 / (r * r);
+        const double m11 = Pn.var_major[p] + caa * inv_r2;
+        const double m22 = Pn.var_minor[p] + cbb * inv_r2;
+        const double m12 = cab * inv_r2;
+        const double upper = fmax(m11, m22) + fabs(m12);
+        const double sf = C.smoothing_factor;
+        const bool far = fmax(fmax(fabs(m11), fabs(m22)), fabs(m12)) < 1e150 &&
+                         theta * theta > sf * sf * fmax(upper, 0.0) * (1.0 + 1e-12);
+        double mu1 = 0.0, mu2 = 0.0, extent = 0.0;
+        if (!far) {
+          const double half_tr = 0.5 * (m11 + m22);
+          const double disc = sqrt(fmax(0.25 * (m11 - m22) * (m11 - m22) + m12 * m12, 0.0));
+          mu1 = half_tr + disc;
+          mu2 = fmax(half_tr - disc, 1e-16 * mu1 + 1e-300);
+          extent = sqrt(fmax(mu1, 0.0));
+        }
+        const double u_ = hx * ax + hy * ay + hz * az, v_ = hx * bx + hy * by + hz * bz;
+        double factor;
+        if (!far && extent > 0.0 && theta < sf * extent) {
+          double sa, ca;
+          sincos(0.5 * atan2(2.0 * m12, m11 - m22), &sa, &ca);
+          const double mean = o1_gauss_inverse_mean(ca * u_ + sa * v_, -sa * u_ + ca * v_, mu1,
+                                                    mu2, S.tangent, S.wsec2, C.n_gauss);
+          factor = mean * (sine > 1e-300 ? theta / sine : 1.0);
+          const bool avg = theta < extent;
+          theta = factor > 1.0 ? asin(fmin(1.0, 1.0 / factor)) : theta;
+          averaged = avg;
+        } else {
+          if (sine <= 1e-300) continue;
+          const double d2 = u_ * u_ + v_ * v_;
+          factor = 1.0 / sine;
+          if (d2 > 0.0) {
+            const double qf = m11 * u_ * u_ + 2.0 * m12 * u_ * v_ + m22 * v_ * v_;
+            factor *= 1.0 + 0.5 * (3.0 * qf / d2 - (m11 + m22)) / d2;
+          }
+        }
+        weight = factor / r;
+      }
+    }
+    // theta index (scalar_theta_index, _prompt_numba.py:1628-1631)
+    int i_theta;
+    if (!(theta >= C.theta_lo)) i_theta = 0;
+    else i_theta = min(1 + (int)(log(theta / C.theta_lo) / log_theta_ratio), theta_bins - 1);
+    const long long key = base + (backward ? theta_bins : 0) + i_theta;
+    bool fresh;
+    long long* keys = gkeys + (int64_t)w * cap;
+    const int64_t slot = o1_insert(keys, cap, key, fresh);
+    if (slot < 0) {
+      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+      continue;
+    }
+    if (fresh && atomicAdd(gcount + w, 1) >= kO1GroupSort)
+      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+    double* row = grows + ((int64_t)w * cap + slot) * kO1MaxValues;
+    // _fill_moments_averaged_pair (_prompt_numba.py:1260-1277)
+    double cpw[5], spw[5];
+    cpw[0] = 1.0;
+    spw[0] = 1.0;
+    const double perp2 = fmax(1.0 - c1 * c1, 0.0);
+    for (int q = 1; q <= C.max_power; ++q) {
+      cpw[q] = cpw[q - 1] * c1;
+      if (averaged) spw[q] = (q & 1) ? 0.0 : spw[q - 2] * perp2 * (q - 1.0) / q;
+      else spw[q] = spw[q - 1] * c3;
+    }
+    const double weight0 = weight * Pn.w0[p], weight2 = weight * Pn.w2[p];
+    const int nm = C.n_mono;
+    double omega = 0.0;
+    for (int m = 0; m < nm; ++m) {
+      const double basis = cpw[S.ipow[m]] * spw[S.jpow[m]];
+      const double v0 = weight0 * basis;
+      if (m == 0) omega = fabs(v0);
+      atomicAdd(row + m, v0);
+      atomicAdd(row + nm + m, weight2 * basis);
+    }
+    atomicAdd(row + 2 * nm, omega);
+    atomicAdd(row + 2 * nm + 1, omega * theta);
+    atomicAdd(row + 2 * nm + 2, omega * r);
+    atomicAdd(row + 2 * nm + 3, omega * t_emit);
+    atomicAdd(row + 2 * nm + 4, omega * tau);
+    atomicAdd(row + 2 * nm + 5, omega * tau * tau);
+    (void)n_values;
+  }
+}
+
+// One CTA per work OM: sort the OM's group keys and list its (tau, r) batches.
+__global__ void __launch_bounds__(1024)
+o1_batches_kernel(const lh_order1_config C, int32_t n_work, const long long* gkeys,
+                  int32_t* sorted_slots, int32_t* batch_list, int32_t* batch_total,
+                  int32_t* status) {
+  extern __shared__ __align__(16) unsigned char o1b_smem[];
+  unsigned long long* v = reinterpret_cast<unsigned long long*>(o1b_smem);
+  __shared__ int n_used;
+  const int w = blockIdx.x;
+  const int64_t cap = C.group_capacity;
+  const long long* keys = gkeys + (int64_t)w * cap;
+  if (threadIdx.x == 0) n_used = 0;
+  __syncthreads();
+  for (int64_t slot = threadIdx.x; slot < cap; slot += blockDim.x) {
+    const long long key = keys[slot];
+    if (key == -1ll) continue;
+    const int k = atomicAdd(&n_used, 1);
+    if (k < kO1GroupSort) v[k] = ((unsigned long long)key << 14) | (unsigned long long)slot;
+  }
+  __syncthreads();
+  const int used = min(n_used, kO1GroupSort);
+  if (n_used > kO1GroupSort && threadIdx.x == 0)
+    atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+  int n = 1;
+  while (n < used) n <<= 1;
+  for (int k = used + threadIdx.x; k < n; k += blockDim.x) v[k] = ~0ull;
+  __syncthreads();
+  // bitonic sort, ascending
+  for (int size = 2; size <= n; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int partner = k ^ stride;
+        if (partner > k) {
+          const bool up = (k & size) == 0;
+          const unsigned long long a = v[k], b = v[partner];
+          if ((a > b) == up) {
+            v[k] = b;
+            v[partner] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  int32_t* out = sorted_slots + (int64_t)w * kO1GroupSort;
+  const long long tb = C.theta_bins;
+  for (int k = threadIdx.x; k < used; k += blockDim.x) {
+    out[k] = (int32_t)(v[k] & 0x3fffull);
+    const long long bk = (long long)(v[k] >> 14) / tb;
+    if (k == 0 || (long long)(v[k - 1] >> 14) / tb != bk) {
+      int stop = k + 1;
+      while (stop < used && (long long)(v[stop] >> 14) / tb == bk) ++stop;
+      const int b = atomicAdd(batch_total, 1);
+      batch_list[3 * b] = w;
+      batch_list[3 * b + 1] = k;
+      batch_list[3 * b + 2] = stop;
+    }
+  }
+}
+
+// _ifuncs (_prompt_numba.py:139-154): I_k(z) = int_0^1 x^k e^{z x} dx, k = 0, 1, 2
+LH_DEVICE void o1_ifuncs(double z, double ez, double& i0, double& i1, double& i2) {
+  if (fabs(z) < 1.0) {
+    // Taylor coefficients 1 / (n! (n + j + 1)), Horner from n = 23
+    double f = 1.0;  // 1/n!
+    double c0[24], c1[24], c2[24];
+    for (int n = 0; n < 24; ++n) {
+      if (n > 0) f /= n;
+      c0[n] = f / (n + 1.0);
+      c1[n] = f / (n + 2.0);
+      c2[n] = f / (n + 3.0);
+    }
+    i0 = c0[23]; i1 = c1[23]; i2 = c2[23];
+    for (int n = 22; n >= 0; --n) {
+      i0 = i0 * z + c0[n];
+      i1 = i1 * z + c1[n];
+      i2 = i2 * z + c2[n];
+    }
+    return;
+  }
+  i0 = (ez - 1.0) / z;
+  i1 = (ez * (z - 1.0) + 1.0) / (z * z);
+  i2 = (ez * (z * z - 2.0 * z + 2.0) - 2.0) / (z * z * z);
+}
+
+// _quad_integral (_prompt_numba.py:158-163)
+LH_DEVICE double o1_quad(double e_start, double alpha, double beta, double gamma, double width,
+                         double kappa, double e_end) {
+  const double z = kappa * width;
+  const double ez = e_start > 0.0 ? e_end / e_start : exp(z);
+  double i0, i1, i2;
+  o1_ifuncs(z, ez, i0, i1, i2);
+  return e_start * width * (alpha * i0 + width * (beta * i1 + width * gamma * i2));
+}
+
+// _find_bin (_prompt_numba.py:167-182)
+LH_DEVICE int o1_find_bin(const double* edges, int nb, double t) {
+  if (t < edges[0]) return -1;
+  if (t >= edges[nb]) return nb;
+  int low = 0, high = nb;
+  while (high - low > 1) {
+    const int middle = (low + high) / 2;
+    if (t < edges[middle]) high = middle; else low = middle;
+  }
+  return low;
+}
+
+// _deposit_panel (_prompt_numba.py:186-254) into the OM's accumulators
+// pre[3] and acc[nb][4] of one band.
+LH_DEVICE void o1_deposit_panel(double t_a, double t_b, double e_a, double e_b, double alpha,
+                                double beta, double gamma, double kappa, const double* edges,
+                                const double* eedge, int nb, double* pre, double* acc,
+                                int direct_bins) {
+  const double lo = t_a > edges[0] ? t_a : edges[0];
+  const double hi = t_b < edges[nb] ? t_b : edges[nb];
+  if (hi <= lo) return;
+  const int k_lo = o1_find_bin(edges, nb, lo);
+  int k_hi = o1_find_bin(edges, nb, hi);
+  if (k_hi >= nb || (k_hi > k_lo && hi <= edges[k_hi])) k_hi -= 1;
+  if (k_hi - k_lo + 1 <= direct_bins) {
+    for (int k = k_lo; k <= k_hi; ++k) {
+      const double s_lo = lo > edges[k] ? lo : edges[k];
+      const double s_hi = hi < edges[k + 1] ? hi : edges[k + 1];
+      if (s_hi <= s_lo) continue;
+      double e_lo = s_lo == t_a ? e_a : eedge[k];
+      if (s_lo != t_a && s_lo != edges[k]) e_lo = exp(kappa * s_lo);
+      double e_hi = s_hi == t_b ? e_b : eedge[k + 1];
+      if (s_hi != t_b && s_hi != edges[k + 1]) e_hi = exp(kappa * s_hi);
+      const double shift = s_lo - t_a;
+      const double a_loc = alpha + shift * (beta + shift * gamma);
+      const double b_loc = beta + 2.0 * gamma * shift;
+      atomicAdd(acc + 4 * k + 3, o1_quad(e_lo, a_loc, b_loc, gamma, s_hi - s_lo, kappa, e_hi));
+    }
+    return;
+  }
+  const double big_a = alpha - t_a * (beta - gamma * t_a);
+  const double big_b = beta - 2.0 * gamma * t_a;
+  const double big_c = gamma;
+  if (t_a < edges[0]) {
+    atomicAdd(pre + 0, big_a);
+    atomicAdd(pre + 1, big_b);
+    atomicAdd(pre + 2, big_c);
+  } else {
+    const int k = k_lo;
+    atomicAdd(acc + 4 * k + 0, big_a);
+    atomicAdd(acc + 4 * k + 1, big_b);
+    atomicAdd(acc + 4 * k + 2, big_c);
+    atomicAdd(acc + 4 * k + 3, o1_quad(e_a, alpha, beta, gamma, edges[k + 1] - t_a, kappa, eedge[k + 1]));
+  }
+  if (t_b < edges[nb]) {
+    const int k = o1_find_bin(edges, nb, t_b);
+    atomicAdd(acc + 4 * k + 0, -big_a);
+    atomicAdd(acc + 4 * k + 1, -big_b);
+    atomicAdd(acc + 4 * k + 2, -big_c);
+    const double shift = t_b - t_a;
+    const double a_loc = alpha + shift * (beta + shift * gamma);
+    const double b_loc = beta + 2.0 * gamma * shift;
+    atomicAdd(acc + 4 * k + 3,
+              -o1_quad(e_b, a_loc, b_loc, gamma, edges[k + 1] - t_b, kappa, eedge[k + 1]));
+  }
+}
+
+struct O1BatchShared {
+  double s[kO1MaxNodes];
+  double g0[kO1MaxNodes];
+  double g2[kO1MaxNodes];
+  double t[kO1MaxNodes];
+  double h[kO1MaxNodes];
+  double mom[kO1MaxValues * 128];  // moments of the batch's theta groups (<= 128)
+  double coef[kO1MaxMono];
+  int ipow[kO1MaxMono], jpow[kO1MaxMono];
+  double red[kO1BatchThreads / 32];
+  double stats[8];
+  int n, last;
+};
+
+// Persistent CTAs over the batch list: _grouped_pencils_order1_block's batch
+// loop (_prompt_numba.py:1934-1993) with _batch_grid, _batch_add_moments and
+// _batch_deposit (_prompt_numba.py:258-551).
+__global__ void __launch_bounds__(kO1BatchThreads)
+o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* gkeys,
+                const double* grows, const int32_t* sorted_slots, const int32_t* batch_list,
+                const int32_t* batch_total, double* accum, int32_t* status) {
+  extern __shared__ __align__(16) unsigned char o1_smem[];
+  O1BatchShared& S = *reinterpret_cast<O1BatchShared*>(o1_smem);
+  const int tid = threadIdx.x;
+  const int nm = C.n_mono;
+  const int nv = 2 * nm + 6;
+  const int nb = C.n_edges - 1;
+  const int NL = C.n_bands;
+  const int64_t cap = C.group_capacity;
+  for (int k = tid; k < nm; k += blockDim.x) {
+    S.coef[k] = C.coef[k];
+    S.ipow[k] = C.ipow[k];
+    S.jpow[k] = C.jpow[k];
+  }
+  double mut_min = C.mut[0], speed_max = C.speed[0];
+  for (int l = 1; l < NL; ++l) {
+    mut_min = fmin(mut_min, C.mut[l]);
+    speed_max = fmax(speed_max, C.speed[l]);
+  }
+  const double g = C.g;
+  const double y_g = g != 0.0 ? (1.0 - fabs(g)) / (1.0 + fabs(g)) : 1.0;
+  const int total = *batch_total;
+  const int64_t per_om = (int64_t)NL * (3 + 4 * nb + 1);
+  for (int b = blockIdx.x; b < total; b += gridDim.x) {
+    __syncthreads();
+    const int w = batch_list[3 * b], start = batch_list[3 * b + 1], stop = batch_list[3 * b + 2];
+    const int count = stop - start;
+    const int32_t* slots = sorted_slots + (int64_t)w * kO1GroupSort + start;
+    const double* rows = grows + (int64_t)w * cap * kO1MaxValues;
+    if (count > 128) {
+      if (tid == 0) atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+      continue;
+    }
+    for (int k = tid; k < count * nv; k += blockDim.x) {
+      const int q = k / nv, c = k - q * nv;
+      S.mom[q * kO1MaxValues + c] = rows[(int64_t)slots[q] * kO1MaxValues + c];
+    }
+    const long long key0 = gkeys[(int64_t)w * cap + slots[0]];
+    const bool backward = ((key0 / C.theta_bins) & 1) == 1;
+    __syncthreads();
+    if (tid == 0) {
+      double omega_sum = 0, r_sum = 0, t_sum = 0, tau_sum = 0, tau2_sum = 0, theta_small = kPi;
+      for (int q = 0; q < count; ++q) {
+        const double* row = S.mom + q * kO1MaxValues;
+        const double omega = row[2 * nm];
+        if (omega > 0.0) {
+          omega_sum += omega;
+          r_sum += row[2 * nm + 2];
+          t_sum += row[2 * nm + 3];
+          tau_sum += row[2 * nm + 4];
+          tau2_sum += row[2 * nm + 5];
+          theta_small = fmin(theta_small, row[2 * nm + 1] / omega);
+        }
+      }
+      S.n = 0;
+      if (omega_sum > 0.0) {
+        const double r_b = r_sum / omega_sum;
+        const double t_b = t_sum / omega_sum;
+        const double tau_mean = tau_sum / omega_sum;
+        const double tau_var = fmax(tau2_sum / omega_sum - tau_mean * tau_mean, 0.0);
+        theta_small = fmax(theta_small, 1e-9);
+        double sigma;
+        if (backward) {
+          sigma = fmax(0.5 * r_b * sin(theta_small) * y_g, 0.25 * r_b * (1.0 - cos(theta_small)));
+        } else {
+          // _batch_sigma (_prompt_numba.py:290-292)
+          sigma = fmax(0.5 * r_b * sin(theta_small) * fmax(y_g, 0.5 * tan(0.5 * theta_small)),
+                       1e-9 * r_b);
+        }
+        // _batch_grid (_prompt_numba.py:258-286): node counts
+        const double ext_end = C.tail_exponent / mut_min;
+        double ext_win = speed_max * (C.edges[nb] - t_b) - r_b;
+        ext_win = fmin(fmax(ext_win, 0.0), ext_end);
+        const double u_end = asinh(ext_end / sigma), u_win = asinh(ext_win / sigma);
+        if (!(u_win >= 0.0) || !(u_end >= u_win) || !(u_end < 1e6)) {
+          atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+          S.n = 0;
+          goto stats_done;
+        }
+        long long n_in = u_win > 0.0 ? (long long)ceil(u_win / C.path_step) : 0;
+        long long n_out = u_end > u_win ? (long long)ceil((u_end - u_win) / C.path_step_tail) : 0;
+        const int capacity = C.max_path_nodes;
+        if (n_in + n_out + 1 > capacity) {
+          const double scale = (capacity - 1.0) / (double)(n_in + n_out);
+          n_in = (long long)(n_in * scale);
+          n_out = capacity - 1 - n_in;
+        }
+        S.n = (int)(n_in + n_out + 1);
+        S.stats[0] = r_b; S.stats[1] = t_b; S.stats[2] = sqrt(12.0 * tau_var);
+        S.stats[3] = sigma; S.stats[4] = u_win; S.stats[5] = u_end;
+        S.stats[6] = (double)n_in; S.stats[7] = (double)n_out;
+      }
+    }
+  stats_done:
+    __syncthreads();
+    const int n = S.n;
+    if (n == 0) continue;
+    const double r_b = S.stats[0], t_b = S.stats[1], front_extra = S.stats[2];
+    const double sigma = S.stats[3], u_win = S.stats[4], u_end = S.stats[5];
+    const int n_in = (int)S.stats[6], n_out = (int)S.stats[7];
+    for (int k = tid; k < n; k += blockDim.x) {
+      double s;
+      if (k == 0) s = r_b;
+      else if (k <= n_in) s = r_b + sigma * sinh(u_win * k / n_in);
+      else s = r_b + sigma * sinh(u_win + (u_end - u_win) * (k - n_in) / n_out);
+      S.s[k] = s;
+    }
+    __syncthreads();
+    // profile: _batch_add_moments (_prompt_numba.py:394-447), generic monomials
+    const double g1 = 1.0 + g * g, gg = 2.0 * g, norm = (1.0 - g * g) / (4.0 * kPi);
+    for (int k = tid; k < n; k += blockDim.x) {
+      double a0s = 0.0, a2s = 0.0;
+      for (int q = 0; q < count; ++q) {
+        const double* row = S.mom + q * kO1MaxValues;
+        const double omega = row[2 * nm];
+        if (omega <= 0.0) continue;
+        const double theta = fmax(row[2 * nm + 1] / omega, 1e-9);
+        double sin_t, cos_t;
+        sincos(theta, &sin_t, &cos_t);
+        const double rs = r_b * sin_t;
+        double c, s, path_jacobian;
+        if (backward) {
+          const double shift = S.s[k] - r_b * cos_t;
+          const double den = rs * rs + shift * shift;
+          c = (rs * rs - shift * shift) / den;
+          s = 2.0 * rs * shift / den;
+          path_jacobian = 2.0 * r_b / den;
+        } else {
+          const double y = (S.s[k] - r_b) / rs + sin_t / (1.0 + cos_t);
+          const double inv = 1.0 / (1.0 + y * y);
+          c = (1.0 - y * y) * inv;
+          s = 2.0 * y * inv;
+          path_jacobian = 2.0 / (r_b * sin_t) * inv;
+        }
+        double cpw[5], spw[5];
+        cpw[0] = 1.0;
+        spw[0] = 1.0;
+        for (int pw = 1; pw <= C.max_power; ++pw) {
+          cpw[pw] = cpw[pw - 1] * c;
+          spw[pw] = spw[pw - 1] * s;
+        }
+        double a0 = 0.0, a2 = 0.0;
+        for (int m = 0; m < nm; ++m) {
+          const double basis = S.coef[m] * cpw[S.ipow[m]] * spw[S.jpow[m]];
+          a0 += basis * row[m];
+          a2 += basis * row[nm + m];
+        }
+        const double den = g1 - gg * c;
+        const double value = path_jacobian * norm / (den * sqrt(den));
+        a0s += a0 * value;
+        a2s += a2 * value;
+      }
+      S.g0[k] = a0s;
+      S.g2[k] = a2s;
+    }
+    __syncthreads();
+    // _batch_deposit (_prompt_numba.py:451-551), every band
+    const int d = work[w];
+    double* accw = accum + (int64_t)w * per_om;
+    for (int lam = 0; lam < NL; ++lam) {
+      if (C.mus[lam] == 0.0) continue;
+      const double v = C.speed[lam];
+      const double kappa = -C.mut[lam] * v;
+      int last = n - 1;
+      const double limit = r_b + C.tail_exponent / C.mut[lam];
+      while (last > 2 && S.s[last - 1] > limit) last -= 1;
+      if (last < 2) continue;
+      const double spread = fmin(front_extra, (S.s[last] - r_b) / v);
+      const double front_time = t_b + r_b / v;
+      const double end_time = t_b + S.s[last] / v;
+      const bool outside = front_time - 0.5 * spread >= C.edges[nb] ||
+                           end_time + 0.5 * spread <= C.edges[0];
+      const double t_base = outside ? 0.0 : t_b;
+      const double e_emit = exp(kappa * t_base);
+      const double h_scale = C.mus[lam] * v / e_emit;
+      const double w0 = C.s0w[lam] * h_scale, w2 = C.s2w[lam] * h_scale;
+      for (int j = tid; j <= last; j += blockDim.x) {
+        S.t[j] = t_base + S.s[j] / v;
+        S.h[j] = w0 * S.g0[j] + w2 * S.g2[j];
+      }
+      __syncthreads();
+      const double h_front = S.h[0];
+      __syncthreads();
+      for (int j = tid; j <= last; j += blockDim.x) S.h[j] -= h_front;
+      __syncthreads();
+      const double* eedge = C.eedge + (int64_t)lam * C.n_edges;
+      double* pre = accw + (int64_t)lam * (3 + 4 * nb + 1);
+      double* acc = pre + 3;
+      double* chg = acc + 4 * nb;
+      const bool bins = C.compute_bins != 0;
+      // panels start at even nodes with step 2; an odd `last` ends with one step
+      const int n_pairs = last / 2;
+      const int n_panels = n_pairs + (last & 1);
+      double total = 0.0;
+      for (int pi = tid; pi < n_panels; pi += blockDim.x) {
+        double t_a, t_b2, alpha, beta, gamma, e_a, e_b;
+        if (pi < n_pairs) {
+          const int j = 2 * pi;
+          t_a = S.t[j];
+          const double t_m = S.t[j + 1];
+          t_b2 = S.t[j + 2];
+          const double u_m = t_m - t_a, u_b = t_b2 - t_a;
+          const double d1 = (S.h[j + 1] - S.h[j]) / u_m;
+          const double d2 = ((S.h[j + 2] - S.h[j + 1]) / (t_b2 - t_m) - d1) / u_b;
+          alpha = S.h[j];
+          beta = d1 - d2 * u_m;
+          gamma = d2;
+          e_a = e_emit * exp(-C.mut[lam] * S.s[j]);
+          e_b = e_emit * exp(-C.mut[lam] * S.s[j + 2]);
+        } else {
+          const int j = last - 1;
+          const double t_p = S.t[j - 1];
+          t_a = S.t[j];
+          t_b2 = S.t[j + 1];
+          const double u_m = t_a - t_p, u_b = t_b2 - t_p;
+          const double d1 = (S.h[j] - S.h[j - 1]) / u_m;
+          const double d2 = ((S.h[j + 1] - S.h[j]) / (t_b2 - t_a) - d1) / u_b;
+          alpha = S.h[j];
+          beta = d1 - d2 * u_m + 2.0 * d2 * u_m;
+          gamma = d2;
+          e_a = e_emit * exp(-C.mut[lam] * S.s[j]);
+          e_b = e_emit * exp(-C.mut[lam] * S.s[j + 1]);
+        }
+        total += o1_quad(e_a, alpha, beta, gamma, t_b2 - t_a, kappa, e_b);
+        if (bins && !outside)
+          o1_deposit_panel(t_a, t_b2, e_a, e_b, alpha, beta, gamma, kappa, C.edges, eedge, nb,
+                           pre, acc, C.direct_bins);
+      }
+      for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
+      if ((tid & 31) == 0) S.red[tid >> 5] = total;
+      __syncthreads();
+      if (tid == 0) {
+        double sum = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) sum += S.red[k];
+        // front step as a mass-normalised ramp of width `spread`
+        const double e_first = e_emit * exp(-C.mut[lam] * S.s[0]);
+        const double e_last = e_emit * exp(-C.mut[lam] * S.s[last]);
+        const double t_f = S.t[0], t_end = S.t[last];
+        const double exact = o1_quad(e_first, h_front, 0.0, 0.0, t_end - t_f, kappa, e_last);
+        sum += exact;
+        if (bins && spread > 0.0 && !outside) {
+          const double t_1 = t_f - 0.5 * spread, t_2 = t_f + 0.5 * spread;
+          const double e_1 = exp(kappa * t_1), e_2 = exp(kappa * t_2);
+          const double ramp = o1_quad(e_1, 0.0, 1.0 / spread, 0.0, spread, kappa, e_2);
+          const double flat = t_end > t_2 ? o1_quad(e_2, 1.0, 0.0, 0.0, t_end - t_2, kappa, e_last) : 0.0;
+          const double height = ramp + flat != 0.0 ? exact / (ramp + flat) : 0.0;
+          o1_deposit_panel(t_1, t_2, e_1, e_2, 0.0, height / spread, 0.0, kappa, C.edges, eedge,
+                           nb, pre, acc, C.direct_bins);
+          if (t_end > t_2)
+            o1_deposit_panel(t_2, t_end, e_2, e_last, height, 0.0, 0.0, kappa, C.edges, eedge, nb,
+                             pre, acc, C.direct_bins);
+        } else if (bins && t_end > t_f && !outside) {
+          o1_deposit_panel(t_f, t_end, e_first, e_last, h_front, 0.0, 0.0, kappa, C.edges, eedge,
+                           nb, pre, acc, C.direct_bins);
+        }
+        atomicAdd(chg, sum);
+      }
+      __syncthreads();
+    }
+    (void)d;
+  }
+}
+
+// _finalize (_prompt_numba.py:610-632): one CTA per work OM.
+__global__ void o1_finalize_kernel(const lh_order1_config C, const int32_t* work, int32_t n_work,
+                                   const double* accum, double* charge, double* bins) {
+  const int w = blockIdx.x;
+  const int d = work[w];
+  const int nb = C.n_edges - 1;
+  const int NL = C.n_bands;
+  const int64_t per_om = (int64_t)NL * (3 + 4 * nb + 1);
+  const double* accw = accum + (int64_t)w * per_om;
+  const double area = C.om_area[d];
+  if (threadIdx.x == 0) {
+    double total = 0.0;
+    for (int lam = 0; lam < NL; ++lam) total += accw[(int64_t)lam * (3 + 4 * nb + 1) + 3 + 4 * nb];
+    charge[d] = area * total;
+  }
+  if (!C.compute_bins || !bins) return;
+  // one thread per band runs the prefix; the bands are summed in order
+  extern __shared__ __align__(16) unsigned char o1f_smem[];
+  double* band_bins = reinterpret_cast<double*>(o1f_smem);
+  for (int lam = threadIdx.x; lam < NL; lam += blockDim.x) {
+    const double* pre = accw + (int64_t)lam * (3 + 4 * nb + 1);
+    const double* acc = pre + 3;
+    const double* eedge = C.eedge + (int64_t)lam * C.n_edges;
+    const double* itab = C.itab + (int64_t)lam * nb * 3;
+    double a = pre[0], b = pre[1], c = pre[2];
+    for (int k = 0; k < nb; ++k) {
+      const double e_k = C.edges[k];
+      const double width = C.edges[k + 1] - e_k;
+      const double a_loc = a + e_k * (b + c * e_k);
+      const double b_loc = b + 2.0 * c * e_k;
+      const double value = eedge[k] * width *
+                           (a_loc * itab[3 * k] + width * (b_loc * itab[3 * k + 1] + width * c * itab[3 * k + 2]));
+      band_bins[(int64_t)lam * nb + k] = area * (value + acc[4 * k + 3]);
+      a += acc[4 * k];
+      b += acc[4 * k + 1];
+      c += acc[4 * k + 2];
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    double sum = 0.0;
+    for (int lam = 0; lam < NL; ++lam) sum += band_bins[(int64_t)lam * nb + k];
+    bins[(int64_t)d * nb + k] = sum;
+  }
+}
+
+// ------------------------------------------------------------------ host side
+
+struct O1Workspace {
+  long long* pkeys;
+  double* prows;
+  int32_t* pcount;
+  long long* gkeys;
+  double* grows;
+  int32_t* gcount;
+  int32_t* sorted;
+  int32_t* batch_list;
+  int32_t* batch_total;
+  double* accum;
+  size_t bytes;
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static O1Workspace o1_layout(const lh_order1_config& C, int64_t pencil_capacity, int64_t ring_capacity,
+                             int32_t n_work, unsigned char* base) {
+  O1Workspace W{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    unsigned char* p = base ? base + off : nullptr;
+    off += align256(bytes);
+    return p;
+  };
+  const int nb = C.n_edges - 1;
+  W.pkeys = reinterpret_cast<long long*>(take(sizeof(long long) * ring_capacity));
+  W.prows = reinterpret_cast<double*>(take(sizeof(double) * kO1Moments * ring_capacity));
+  W.pcount = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 4));
+  W.gkeys = reinterpret_cast<long long*>(take(sizeof(long long) * (size_t)n_work * C.group_capacity));
+  W.grows = reinterpret_cast<double*>(
+      take(sizeof(double) * kO1MaxValues * (size_t)n_work * C.group_capacity));
+  W.gcount = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (size_t)n_work));
+  W.sorted = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (size_t)n_work * kO1GroupSort));
+  W.batch_list = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 3 * (size_t)n_work * kO1GroupSort));
+  W.batch_total = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 4));
+  W.accum = reinterpret_cast<double*>(take(sizeof(double) * (size_t)n_work * C.n_bands * (3 + 4 * nb + 1)));
+  (void)pencil_capacity;
+  W.bytes = off;
+  return W;
+}
+
+static int64_t next_pow2(int64_t x) {
+  int64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+int64_t o1_ring_capacity(int64_t n_subseg, int32_t ring_nodes) {
+  return next_pow2(std::max<int64_t>(4096, n_subseg * ring_nodes));
+}
+
+static int grid_for(int64_t items, int threads) {
+  int64_t blocks = (items + threads - 1) / threads;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  return (int)blocks;
+}
+
+}  // namespace lh
+
+namespace {
+bool o1_config_valid(const lh_order1_config* C) {
+  if (!C) return false;
+  if (C->n_om < 1 || !C->om_pos || !C->om_look || !C->om_area) return false;
+  if (C->n_bands < 1 || C->n_bands > lh::kO1MaxBands || !C->mus || !C->mut || !C->speed ||
+      !C->s0w || !C->s2w)
+    return false;
+  if (C->n_mono < 1 || C->n_mono > lh::kO1MaxMono || C->max_power < 0 || C->max_power > 4 ||
+      !C->coef || !C->ipow || !C->jpow)
+    return false;
+  if (C->n_edges < 2 || !C->edges || !C->eedge || !C->itab) return false;
+  if (C->max_path_nodes < 4 || C->max_path_nodes > lh::kO1MaxNodes) return false;
+  if (C->n_gauss < 1 || C->n_gauss > lh::kO1MaxGauss || !C->gauss_tau || !C->gauss_w) return false;
+  if (C->group_capacity < 1024 || C->group_capacity > (1 << 14) ||
+      (C->group_capacity & (C->group_capacity - 1)))
+    return false;
+  if (C->theta_bins < 2 || C->theta_bins > 128 || !(C->theta_lo > 0) || !(C->theta_ratio > 0) ||
+      !(C->tau_step > 0) || !(C->log_r_step > 0))
+    return false;
+  if (C->pixel_face < 1 || C->ring_nodes < 1 || !(C->cell_m > 0)) return false;
+  return true;
+}
+}  // namespace
+
+extern "C" size_t lh_order1_workspace_bytes(const lh_order1_config* C, int64_t n_subseg,
+                                            int32_t n_work) {
+  if (!o1_config_valid(C) || n_subseg < 0 || n_work < 0) return 0;
+  const int64_t ring_cap = lh::o1_ring_capacity(n_subseg, C->ring_nodes);
+  return lh::o1_layout(*C, 0, ring_cap, n_work, nullptr).bytes;
+}
+
+extern "C" int lh_order1_pencils(const lh_order1_config* C, const lh_order1_elements* E,
+                                 const lh_order1_pencil_table* P, int32_t* n_pencils_device,
+                                 void* workspace, size_t workspace_bytes, int32_t* status,
+                                 void* stream) {
+  if (!o1_config_valid(C) || !E || !P || !n_pencils_device || !status) return LH_EINVAL;
+  if (E->n_el < 0 || E->n_subseg < 0 || (E->n_el && (!E->subseg_offset || !E->start ||
+                                                     !E->direction || !E->length || !E->c0 ||
+                                                     !E->c2 || !E->cone_cos || !E->t0 || !E->t1)))
+    return LH_EINVAL;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int64_t ring_cap = lh::o1_ring_capacity(E->n_subseg, C->ring_nodes);
+  lh::O1Workspace W = lh::o1_layout(*C, 0, ring_cap, 0, static_cast<unsigned char*>(workspace));
+  if (!workspace || workspace_bytes < W.bytes) return LH_ENOMEM;
+  cudaMemsetAsync(n_pencils_device, 0, sizeof(int32_t), s);
+  if (E->n_el == 0 || E->n_subseg == 0) return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+  cudaMemsetAsync(W.pkeys, 0xff, sizeof(long long) * ring_cap, s);
+  cudaMemsetAsync(W.prows, 0, sizeof(double) * lh::kO1Moments * ring_cap, s);
+  const int64_t nodes = E->n_subseg * C->ring_nodes;
+  lh::o1_ring_kernel<<<lh::grid_for(nodes, 256), 256, 0, s>>>(*C, *E, E->subseg_offset, E->n_subseg,
+                                                               W.pkeys, ring_cap, W.prows, status);
+  lh::o1_finish_kernel<<<lh::grid_for(ring_cap, 256), 256, 0, s>>>(W.pkeys, ring_cap, W.prows, *P,
+                                                                   n_pencils_device, status);
+  return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+}
+
+extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_pencil_table* P,
+                                 int32_t n_pencils, const int32_t* work, int32_t n_work,
+                                 const double* origins, double* charge, double* bins,
+                                 void* workspace, size_t workspace_bytes, int32_t* status,
+                                 void* stream) {
+  if (!o1_config_valid(C) || !P || n_pencils < 0 || n_work < 0 || !status || !charge) return LH_EINVAL;
+  if (n_work && (!work || !origins)) return LH_EINVAL;
+  if (C->compute_bins && !bins) return LH_EINVAL;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the grouped stage reuses the workspace from its start (pencils live elsewhere)
+  lh::O1Workspace W = lh::o1_layout(*C, 0, 0, n_work, static_cast<unsigned char*>(workspace));
+  if (!workspace || workspace_bytes < W.bytes) return LH_ENOMEM;
+  const int nb = C->n_edges - 1;
+  cudaMemsetAsync(charge, 0, sizeof(double) * C->n_om, s);
+  if (C->compute_bins) cudaMemsetAsync(bins, 0, sizeof(double) * (size_t)C->n_om * nb, s);
+  if (n_work == 0 || n_pencils == 0) return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+  const int64_t cap = C->group_capacity;
+  cudaMemsetAsync(W.gkeys, 0xff, sizeof(long long) * (size_t)n_work * cap, s);
+  cudaMemsetAsync(W.grows, 0, sizeof(double) * lh::kO1MaxValues * (size_t)n_work * cap, s);
+  cudaMemsetAsync(W.gcount, 0, sizeof(int32_t) * (size_t)n_work, s);
+  cudaMemsetAsync(W.batch_total, 0, sizeof(int32_t) * 4, s);
+  cudaMemsetAsync(W.accum, 0, sizeof(double) * (size_t)n_work * C->n_bands * (3 + 4 * nb + 1), s);
+  lh::o1_group_kernel<<<lh::grid_for((int64_t)n_work * n_pencils, 256), 256, 0, s>>>(
+      *C, *P, n_pencils, work, n_work, origins, W.gkeys, W.grows, W.gcount, status);
+  const size_t sort_smem = sizeof(unsigned long long) * lh::kO1GroupSort;
+  if (cudaFuncSetAttribute(lh::o1_batches_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sort_smem) != cudaSuccess)
+    return LH_ECUDA;
+  lh::o1_batches_kernel<<<n_work, 1024, sort_smem, s>>>(*C, n_work, W.gkeys, W.sorted, W.batch_list,
+                                                        W.batch_total, status);
+  const size_t batch_smem = sizeof(lh::O1BatchShared);
+  if (cudaFuncSetAttribute(lh::o1_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)batch_smem) != cudaSuccess)
+    return LH_ECUDA;
+  lh::o1_batch_kernel<<<148 * 2, lh::kO1BatchThreads, batch_smem, s>>>(
+      *C, work, W.gkeys, W.grows, W.sorted, W.batch_list, W.batch_total, W.accum, status);
+  const size_t fin_smem = sizeof(double) * C->n_bands * nb;
+  if (fin_smem > 200 * 1024) return LH_EUNSUPPORTED;
+  if (cudaFuncSetAttribute(lh::o1_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)fin_smem) != cudaSuccess)
+    return LH_ECUDA;
+  lh::o1_finalize_kernel<<<n_work, 128, fin_smem, s>>>(*C, work, n_work, W.accum, charge, bins);
+  return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+}
