@@ -328,6 +328,55 @@ int lh_order1_grouped(const lh_order1_config* config, const lh_order1_pencil_tab
                       const double* origins, double* charge, double* bins, void* workspace,
                       size_t workspace_bytes, int32_t* status, void* stream);
 
+/* ------------------------------------------------------------------ order >= 2 source
+ * Replaces node_sources (shower/ge2.py:35-67) -> compile_axial_slices
+ * (_shower_basis.py:188-645) with the shower basis: axial slices x cubic
+ * Lagrange weights x 5-moment transverse stencil x real harmonics P_l(mu_C) Y_lm,
+ * deposited on a linear time lattice and transformed to the route frequencies.
+ * Every element must emit in every node band (one lattice for all bands).
+ * Small per-problem tables are passed by value; pointers are device memory.
+ */
+typedef struct {
+  int32_t n_el;
+  const double* start;          /* [n_el][3]                                          */
+  const double* direction;      /* [n_el][3]                                          */
+  const double* length;         /* [n_el]                                             */
+  const double* c0;             /* [n_el]                                             */
+  const double* c2;             /* [n_el]                                             */
+  const double* beta;           /* [n_el]                                             */
+  const double* t0;             /* [n_el]                                             */
+  const double* t1;             /* [n_el]                                             */
+  int32_t n_bands;              /* node bands (<= 8)                                  */
+  double band_s0[8];            /* 1 / lambda^2 (shower/ge2.py:30)                    */
+  double band_s2[8];            /* 1 / (lambda^2 n^2)                                 */
+  double band_phase[8];         /* phase index n of the band (cone 1 / (beta n))      */
+  double band_scale[8];         /* fold scale of the band (shower/ge2.py:66)          */
+  double centre[3], first[3], second[3], axis[3];  /* AxisFrame of the prompt steps     */
+  int32_t degree, max_m, nch;   /* source degree, azimuthal degree, kept channels     */
+  int32_t starts[18];           /* first kept channel of each degree (axial_fast._layout) */
+  int32_t channel_degree[153];  /* degree l of each kept channel                      */
+  double aa[85], bb[85];        /* [(degree+1)(max_m+1)] Legendre recurrences        */
+  int32_t element_order;        /* Gauss nodes per chord (1 or 2)                     */
+  double node_fraction[2], node_weight[2];
+  double cell_m, stencil_m, stencil_threshold_m, time_step_ns;
+  double reference_ns;          /* earliest emission (time lattice origin)            */
+  double z_origin;              /* slice lattice origin (min node z - 2 cells)        */
+  int64_t n_slices, kmax;       /* slice and tick lattice sizes                       */
+  int32_t n_omega;
+  const double* omega;          /* [n_omega] rad/ns                                   */
+} lh_source_problem;
+
+typedef struct {
+  int64_t capacity;             /* points per band allocated (>= 5 n_slices)          */
+  double* points;               /* [n_bands][capacity][3] (z, x, y) in the frame      */
+  float* channels;              /* complex64 [n_bands][capacity][nch][n_omega]         */
+  int32_t* n_points;            /* [n_bands] points written per band                  */
+} lh_source_output;
+
+size_t lh_source_workspace_bytes(const lh_source_problem* problem);
+int lh_source_compile(const lh_source_problem* problem, const lh_source_output* output,
+                      void* workspace, size_t workspace_bytes, int32_t* status, void* stream);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

@@ -105,6 +105,26 @@ class Order1PencilTable(C.Structure):
                 ("time", P), ("major", P), ("var_major", P), ("var_minor", P), ("pos_cov", P)]
 
 
+class SourceProblem(C.Structure):
+    _fields_ = [("n_el", C.c_int32), ("start", P), ("direction", P), ("length", P), ("c0", P),
+                ("c2", P), ("beta", P), ("t0", P), ("t1", P), ("n_bands", C.c_int32),
+                ("band_s0", C.c_double * 8), ("band_s2", C.c_double * 8),
+                ("band_phase", C.c_double * 8), ("band_scale", C.c_double * 8),
+                ("centre", C.c_double * 3), ("first", C.c_double * 3), ("second", C.c_double * 3),
+                ("axis", C.c_double * 3), ("degree", C.c_int32), ("max_m", C.c_int32),
+                ("nch", C.c_int32), ("starts", C.c_int32 * 18), ("channel_degree", C.c_int32 * 153),
+                ("aa", C.c_double * 85), ("bb", C.c_double * 85), ("element_order", C.c_int32),
+                ("node_fraction", C.c_double * 2), ("node_weight", C.c_double * 2),
+                ("cell_m", C.c_double), ("stencil_m", C.c_double),
+                ("stencil_threshold_m", C.c_double), ("time_step_ns", C.c_double),
+                ("reference_ns", C.c_double), ("z_origin", C.c_double), ("n_slices", C.c_int64),
+                ("kmax", C.c_int64), ("n_omega", C.c_int32), ("omega", P)]
+
+
+class SourceOutput(C.Structure):
+    _fields_ = [("capacity", C.c_int64), ("points", P), ("channels", P), ("n_points", P)]
+
+
 # name -> (restype, argtypes); every symbol the header declares
 SIGNATURES = {
     "lh_version": (C.c_char_p, []),
@@ -128,6 +148,9 @@ SIGNATURES = {
                                     C.POINTER(Order1PencilTable), P, P, C.c_size_t, P, P]),
     "lh_order1_grouped": (C.c_int, [C.POINTER(Order1Config), C.POINTER(Order1PencilTable),
                                     C.c_int32, P, C.c_int32, P, P, P, P, C.c_size_t, P, P]),
+    "lh_source_workspace_bytes": (C.c_size_t, [C.POINTER(SourceProblem)]),
+    "lh_source_compile": (C.c_int, [C.POINTER(SourceProblem), C.POINTER(SourceOutput), P,
+                                    C.c_size_t, P, P]),
 }
 LH_ESCRATCH = 6
 

@@ -1,0 +1,200 @@
+"""Order >=2 source compile on the B200: the axial-slice basis of a shower.
+
+Reference: ``node_sources`` (``shower/ge2.py:35-67``) compiling each node band
+of the band fold with ``compile_axial_slices`` (``_shower_basis.py:188-645``)
+and the shower basis (``ShowerBasis``: 0.25 m slices, cubic axial weights,
+5-moment stencil of 0.2 m for slices wider than 0.03 m, 0.02 ns linear time
+lattice). The lattice sizes and the frame are small host computations; the
+deposit, time-lattice transform and stencil run in ``liblh_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["ShowerBasisSettings", "SourceCompiler", "axis_frame", "harmonic_layout"]
+
+
+@dataclass(frozen=True)
+class ShowerBasisSettings:
+    """The ``ShowerBasis`` fields the compile reads (``shower_basis.py:61-76``)."""
+    cell_m: float = 0.25
+    stencil_m: float = 0.2
+    stencil_threshold_m: float = 0.03
+    time_step_ns: float = 0.02
+
+
+def harmonic_layout(degree, max_m):
+    """``(starts, aa, bb, kept, channel_degree)`` of ``axial_fast._layout``."""
+    starts, kept, ell_of = [0], [], []
+    for ell in range(degree + 1):
+        for m in range(-min(ell, max_m), min(ell, max_m) + 1):
+            kept.append(ell * ell + ell + m)
+            ell_of.append(ell)
+        starts.append(len(kept))
+    aa = np.zeros((degree + 1, max_m + 1))
+    bb = aa.copy()
+    for m in range(max_m + 1):
+        for ell in range(m + 2, degree + 1):
+            aa[ell, m] = np.sqrt((4 * ell * ell - 1) / (ell * ell - m * m))
+            bb[ell, m] = np.sqrt(((2 * ell + 1) * ((ell - 1) ** 2 - m * m))
+                                 / ((2 * ell - 3) * (ell * ell - m * m)))
+    return (np.asarray(starts, np.int64), aa, bb, np.asarray(kept, np.int64),
+            np.asarray(ell_of, np.int64))
+
+
+def axis_frame(start, direction, length, weights):
+    """``AxisFrame.of`` (``axial_source.py:88-118``): centre, axis, first, second."""
+    start, direction = np.asarray(start, float), np.asarray(direction, float)
+    points = start + 0.5 * np.asarray(length, float)[:, None] * direction
+    share = np.asarray(weights, float) / np.sum(weights)
+    centre = (share[:, None] * points).sum(axis=0)
+    offset = points - centre
+    covariance = np.einsum("i,ij,ik->jk", share, offset, offset)
+    values, vectors = np.linalg.eigh(covariance)
+    if np.max(np.abs(values)) <= 1e-24:
+        axis = np.sum(share[:, None] * direction, axis=0)
+        if np.linalg.norm(axis) <= 1e-12:
+            _, angular = np.linalg.eigh(np.einsum("i,ij,ik->jk", share, direction, direction))
+            axis = angular[:, -1]
+    else:
+        axis = vectors[:, int(np.argmax(values))]
+    axis = axis / np.linalg.norm(axis)
+    if float((share * (direction @ axis)).sum()) < 0:
+        axis = -axis
+    helper = np.array([0.0, 0.0, 1.0])
+    if abs(float(axis @ helper)) > 0.9:
+        helper = np.array([1.0, 0.0, 0.0])
+    first = np.cross(axis, helper)
+    first /= np.linalg.norm(first)
+    return centre, axis, first, np.cross(axis, first)
+
+
+class SourceCompiler:
+    """Node bands (wavelength, phase index, fold scale) and layout on the device."""
+
+    def __init__(self, wavelengths_nm, phase_index, scale, degree, azimuthal_degree, omega, *,
+                 settings=ShowerBasisSettings(), device="cuda"):
+        import torch
+        self.device = torch.device(device)
+        self.wavelengths = np.asarray(wavelengths_nm, float)
+        self.phase = np.asarray(phase_index, float)
+        self.scale = np.asarray(scale, float)
+        if not (len(self.wavelengths) == len(self.phase) == len(self.scale) <= 8):
+            raise ValueError("one wavelength, phase index and scale per node band (<= 8)")
+        self.degree, self.azimuthal_degree = int(degree), int(azimuthal_degree)
+        self.max_m = min(self.degree, self.azimuthal_degree)
+        self.starts, self.aa, self.bb, self.kept, self.channel_degree = harmonic_layout(
+            self.degree, self.max_m)
+        self.nch = len(self.kept)
+        self.settings = settings
+        self.omega = np.asarray(omega, float)
+        self._omega = torch.tensor(self.omega, dtype=torch.float64, device=self.device)
+        self._workspace = None
+
+    def problem(self, arrays, frame, n_el, order, fractions, weights, reference, z_origin,
+                n_slices, kmax):
+        p = _lib.SourceProblem()
+        p.n_el = n_el
+        for name in ("start", "direction", "length", "c0", "c2", "beta", "t0", "t1"):
+            setattr(p, name, arrays[name].data_ptr())
+        nb = len(self.wavelengths)
+        p.n_bands = nb
+        s0 = 1.0 / self.wavelengths ** 2
+        s2 = s0 / self.phase ** 2
+        for k in range(nb):
+            p.band_s0[k], p.band_s2[k] = float(s0[k]), float(s2[k])
+            p.band_phase[k], p.band_scale[k] = float(self.phase[k]), float(self.scale[k])
+        centre, axis, first, second = frame
+        for k in range(3):
+            p.centre[k], p.first[k], p.second[k], p.axis[k] = centre[k], first[k], second[k], axis[k]
+        p.degree, p.max_m, p.nch = self.degree, self.max_m, self.nch
+        for k, v in enumerate(self.starts):
+            p.starts[k] = int(v)
+        for k, v in enumerate(self.channel_degree):
+            p.channel_degree[k] = int(v)
+        for k, (a, b) in enumerate(zip(self.aa.ravel(), self.bb.ravel())):
+            p.aa[k], p.bb[k] = float(a), float(b)
+        p.element_order = order
+        for k in range(order):
+            p.node_fraction[k], p.node_weight[k] = float(fractions[k]), float(weights[k])
+        s = self.settings
+        p.cell_m, p.stencil_m = s.cell_m, s.stencil_m
+        p.stencil_threshold_m, p.time_step_ns = s.stencil_threshold_m, s.time_step_ns
+        p.reference_ns, p.z_origin = reference, z_origin
+        p.n_slices, p.kmax = n_slices, kmax
+        p.n_omega = len(self.omega)
+        p.omega = self._omega.data_ptr()
+        return p
+
+    def compile(self, elements, frame=None, *, stream=None, check=True):
+        """Points and channels of every node band (device), the emission reference.
+
+        ``elements``: reference ``SpectralLightElements`` or a dict with its
+        field names, every element above threshold in every node band.
+        Returns ``(points (band, P, 3) [z, x, y], channels (band, P, nch, W)
+        complex64, n_points (band,), reference_ns, frame)``.
+        """
+        import torch
+
+        def field(name):
+            return np.asarray(elements[name] if isinstance(elements, dict)
+                              else getattr(elements, name), float)
+
+        start, direction, length = field("start_m"), field("direction"), field("length_m")
+        c0, c2, beta = field("coefficient0"), field("coefficient2"), field("beta")
+        t0, t1 = field("start_ns"), field("end_ns")
+        if np.any(beta[:, None] * self.phase[None, :] <= 1):
+            raise NotImplementedError("device source compile needs every element above the "
+                                      "Cherenkov threshold in every node band")
+        if frame is None:
+            frame = axis_frame(start, direction, length, c0)
+        centre, axis = np.asarray(frame[0], float), np.asarray(frame[1], float)
+        s = self.settings
+        order = 1 if float(np.max(length)) <= s.cell_m / 10 else 2
+        x, w = np.polynomial.legendre.leggauss(order)
+        fractions, weights = (x + 1) / 2, w / 2
+        reference = float(t0.min())
+        z_mid = (start + 0.5 * length[:, None] * direction - centre) @ axis
+        z_origin = float(z_mid.min()) - 2 * s.cell_m
+        z_nodes = np.concatenate([(start + f * length[:, None] * direction - centre) @ axis
+                                  for f in fractions])
+        t_nodes = np.concatenate([t0 + f * (t1 - t0) for f in fractions])
+        kmax = int(np.floor((float(t_nodes.max()) - reference) / s.time_step_ns)) + 3
+        zb = np.floor((z_nodes - z_origin) / s.cell_m)
+        if zb.min() < 1:
+            raise NotImplementedError("chord nodes reach below the slice lattice origin")
+        n_slices = int(zb.max()) + 3
+        dev = self.device
+        arrays = {k: torch.tensor(np.ascontiguousarray(v), dtype=torch.float64, device=dev)
+                  for k, v in dict(start=start, direction=direction, length=length, c0=c0, c2=c2,
+                                   beta=beta, t0=t0, t1=t1).items()}
+        p = self.problem(arrays, frame, len(length), order, fractions, weights, reference,
+                         z_origin, n_slices, kmax)
+        nb = len(self.wavelengths)
+        capacity = 5 * n_slices
+        points = torch.empty((nb, capacity, 3), dtype=torch.float64, device=dev)
+        channels = torch.empty((nb, capacity, self.nch, len(self.omega)), dtype=torch.complex64,
+                               device=dev)
+        n_points = torch.zeros(nb, dtype=torch.int32, device=dev)
+        out = _lib.SourceOutput(capacity, points.data_ptr(), channels.data_ptr(),
+                                n_points.data_ptr())
+        lib = _lib.load()
+        need = int(lib.lh_source_workspace_bytes(C.byref(p)))
+        if need == 0:
+            raise ValueError("source compile problem rejected by the device library")
+        if self._workspace is None or self._workspace.numel() < need:
+            self._workspace = torch.empty(need, dtype=torch.uint8, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        sp = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
+        _lib.check(lib.lh_source_compile(C.byref(p), C.byref(out), self._workspace.data_ptr(),
+                                         self._workspace.numel(), status.data_ptr(), sp),
+                   "lh_source_compile")
+        self._keep = arrays
+        if check and int(status.item()) & _lib.LH_STATUS_OVERFLOW:
+            raise ValueError("element nodes fall outside the source lattice")
+        return points, channels, n_points, reference, frame
