@@ -377,6 +377,28 @@ size_t lh_source_workspace_bytes(const lh_source_problem* problem);
 int lh_source_compile(const lh_source_problem* problem, const lh_source_output* output,
                       void* workspace, size_t workspace_bytes, int32_t* status, void* stream);
 
+/* ------------------------------------------------------------------ per-OM geometry
+ * Replaces min_distance_to_segments (_prompt_numba.py:2221-2243, the module
+ * selection of transport_prompt, prompt.py:603-631) and
+ * earliest_element_arrival (_shower_basis.py:50-78, the clock of an extended
+ * source, shower/api.py:466-473), float64 bit-identical, for several events.
+ */
+typedef struct {
+  int32_t n_om;
+  const double* om_pos;          /* [n_om][3]                                         */
+  int32_t n_events;              /* <= 65535                                          */
+  const int64_t* element_offset; /* [n_events + 1]                                    */
+  const double* start;           /* [n_el][3]                                         */
+  const double* direction;       /* [n_el][3] unit                                    */
+  const double* length;          /* [n_el]                                            */
+  const double* start_ns;        /* [n_el]                                            */
+  double group_index;            /* fastest group index (flight n_g / c)              */
+  double* min_distance;          /* [n_events][n_om] or NULL                          */
+  double* earliest_ns;           /* [n_events][n_om] or NULL                          */
+} lh_om_geometry_problem;
+
+int lh_om_geometry(const lh_om_geometry_problem* geometry, void* stream);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

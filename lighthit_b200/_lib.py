@@ -125,6 +125,13 @@ class SourceOutput(C.Structure):
     _fields_ = [("capacity", C.c_int64), ("points", P), ("channels", P), ("n_points", P)]
 
 
+class OmGeometry(C.Structure):
+    _fields_ = [("n_om", C.c_int32), ("om_pos", P), ("n_events", C.c_int32),
+                ("element_offset", P), ("start", P), ("direction", P), ("length", P),
+                ("start_ns", P), ("group_index", C.c_double), ("min_distance", P),
+                ("earliest_ns", P)]
+
+
 # name -> (restype, argtypes); every symbol the header declares
 SIGNATURES = {
     "lh_version": (C.c_char_p, []),
@@ -148,6 +155,7 @@ SIGNATURES = {
                                     C.POINTER(Order1PencilTable), P, P, C.c_size_t, P, P]),
     "lh_order1_grouped": (C.c_int, [C.POINTER(Order1Config), C.POINTER(Order1PencilTable),
                                     C.c_int32, P, C.c_int32, P, P, P, P, C.c_size_t, P, P]),
+    "lh_om_geometry": (C.c_int, [C.POINTER(OmGeometry), P]),
     "lh_source_workspace_bytes": (C.c_size_t, [C.POINTER(SourceProblem)]),
     "lh_source_compile": (C.c_int, [C.POINTER(SourceProblem), C.POINTER(SourceOutput), P,
                                     C.c_size_t, P, P]),

@@ -14,6 +14,7 @@ geometry (float64) and the contraction (float32) run in ``liblh_b200.so``.
 from __future__ import annotations
 
 from dataclasses import dataclass
+import ctypes as C
 from math import exp, lgamma
 
 import numpy as np
@@ -116,6 +117,22 @@ class Ge2Table:
     @classmethod
     def load(cls, path, alpha, **kw):
         return cls(dict(np.load(path)), alpha, **kw)
+
+    def band(self, b):
+        """A view of node band ``b`` alone (for bands whose point sets differ)."""
+        import copy
+        view = copy.copy(self)
+        per_band = self._coef[0].numel() * self._coef.element_size()
+        st = _lib.Ge2Table()
+        C.pointer(st)[0] = self.struct
+        st.n_bands = 1
+        st.coef = self._coef.data_ptr() + b * per_band
+        st.absorption = self._abs.data_ptr() + 8 * b
+        st.speed = self._speed.data_ptr() + 8 * b
+        view.struct = st
+        view.n_bands = 1
+        view._workspace = None
+        return view
 
     def radial_limits(self):
         return float(np.exp(self.log_r[0])), float(np.exp(self.log_r[-1]))

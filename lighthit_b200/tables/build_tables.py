@@ -1,0 +1,130 @@
+"""Build the read-only tables of the shower route with the reference (run once, here).
+
+    python lighthit_b200/tables/build_tables.py c0     # 48 OMs, 2-150 m, 48 radial nodes
+    python lighthit_b200/tables/build_tables.py c2     # 384 OMs, 2-450 m, 60 radial nodes
+
+The reference (LightHit, pure Python + Numba) builds its RTE caches
+(``TransportKernel.build``) and the order >=2 kernel pack
+(``ge2_kernel_store().save``); ``ShowerTransport.tables()`` folds them onto the
+rank-3 node bands (``band_fold.py:155-208``). This script stores, for the
+device route:
+* ``ge2_fold_<n>om_<lo>-<hi>m.npz``: the folded order >=2 kernels;
+* ``route_<config>.npz``: the kernel's medium and detector constants the route
+  reads (wavelength nodes and weights, phase/group indices, absorption and
+  scattering, detector spectral weights, the spectral-cut phase index of
+  ``prompt.py:542-550``, the node bands' wavelengths, phases and fold scales,
+  the prompt tables of ``prompt.py:412-434``, the first-entry optical panels of
+  ``prepare_optics(..., exact_response=True)``, the acceptance coefficients,
+  OM geometry and the kernel configuration).
+It needs the reference sources (``LIGHTHIT_REFERENCE_SRC``) and a writable
+Numba cache; the device route reads only the files it writes.
+"""
+import json
+import os
+import sys
+from dataclasses import replace
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+SRC = Path(os.environ.get("LIGHTHIT_REFERENCE_SRC", "/root/reference/src"))
+WORK = Path(os.environ.get("LIGHTHIT_TABLE_WORK", REPO / "_work" / "tables"))
+
+CONFIGS = {
+    "c0": dict(clusters=1, radial_range_m=(2.0, 150.0), radial_nodes=48, k_panel_per_m=0.1),
+    "c2": dict(clusters=8, radial_range_m=(2.0, 450.0), radial_nodes=60,
+               k_panel_per_m=2 * np.pi / 450.0),
+}
+
+
+def main(name):
+    os.environ.setdefault("NUMBA_CACHE_DIR", str(REPO / "_work" / "numba-cache"))
+    sys.path.insert(0, str(SRC))
+    import lighthit as lh
+    from lighthit.ballistic_interval import BallisticIntervalConfig, prepare_optics
+    from lighthit.examples.synthetic import baikal_like_detector, synthetic_medium_model
+    from lighthit.prompt import _spectral_tables
+    from lighthit.shower import ShowerData, ShowerTransport
+
+    c = CONFIGS[name]
+    cache = WORK / f"shower-{name}"
+    medium = synthetic_medium_model()
+    detector = baikal_like_detector(clusters=c["clusters"])
+    omega = np.linspace(0.0, 1.2, 65)
+    config = lh.KernelConfig(
+        omega_per_ns=omega, readout_omega_per_ns=np.linspace(0.0, 1.2, 321),
+        relative_time_edges_ns=np.arange(-60.0, 745.0, 5.0), wavelength_nodes=3,
+        scattering_degree=8, source_degree=8, azimuthal_degree=2,
+        radial_range_m=c["radial_range_m"], radial_nodes=c["radial_nodes"], k_max_per_m=4.0,
+        k_panel_per_m=float(c["k_panel_per_m"]), k_order=6, threshold_pe=0.01,
+        cache_directory=str(cache), cache_policy="build")
+    kernel = lh.TransportKernel(medium, detector, config)
+    centre = lh.describe_geometry(detector).centroid_m
+    pose = lh.SourcePose(centre + np.asarray([-12.0, 8.0, 0.0]), [0.35, -0.15, 0.925])
+    shower = replace(lh.SyntheticShower.gaussian(pose, charged_track_length_m=300.0,
+                                                 elements=2000, seed=7).elements,
+                     cone_model="spectral")
+    if not (cache / "ge2-pack" / "pack.json").exists():
+        kernel.build(source=shower)
+        kernel.ge2_kernel_store().save(str(cache / "ge2-pack"))
+    route = ShowerTransport(kernel, ShowerData.of(str(cache), str(cache / "ge2-pack")))
+    tables = route.tables()
+    folded, fold = tables["folded"], tables["fold"]
+    k = route.kernel
+    lo, hi = c["radial_range_m"]
+    n_om = len(detector)
+    np.savez_compressed(
+        HERE / f"ge2_fold_{n_om}om_{lo:g}-{hi:g}m.npz",
+        coefficients=np.asarray(folded["coefficients"], np.complex64),
+        log_r=np.asarray(folded["log_r"], float), omega=np.asarray(folded["omega"], float),
+        absorption=np.asarray(folded["absorption"], float), speed=np.asarray(folded["speed"], float),
+        degree=int(folded["degree"]), acceptance_degree=int(folded["acceptance_degree"]),
+        pair_lambda=np.asarray(folded["pair_lambda"], np.int64),
+        pair_mu=np.asarray(folded["pair_mu"], np.int64), phase=str(folded["phase"]),
+        bands=np.asarray(fold.bands, np.int64), scale=np.asarray(fold.scale, float),
+        provenance=json.dumps({"built_by": "lighthit ShowerTransport.tables() (BandFold rank 3)",
+                               "kernel": {"radial_range_m": [lo, hi],
+                                          "radial_nodes": c["radial_nodes"],
+                                          "k_panel_per_m": float(c["k_panel_per_m"])}}))
+    wl = np.asarray(k.wavelength.wavelength_nm, float)
+    sample = k.medium.sample(wl)
+    low, high = k.config.wavelength_range_nm or k.medium.wavelength_range_nm
+    native = k.medium.wavelength_nm
+    critical = np.r_[low, native[(native > low) & (native < high)], high]
+    prompt = _spectral_tables(k)
+    optics = prepare_optics(k, BallisticIntervalConfig(), exact_response=True)
+    d = k.detector
+    np.savez_compressed(
+        HERE / f"route_{name}.npz",
+        wavelength_nm=wl, weight_nm=np.asarray(k.wavelength.weight_nm, float),
+        phase_index=np.asarray(sample["phase_index"], float),
+        group_index=np.asarray(sample["group_index"], float),
+        absorption_per_m=np.asarray(sample["absorption_per_m"], float),
+        scattering_per_m=np.asarray(sample["scattering_per_m"], float),
+        efficiency=np.asarray(d.spectral_weight(wl), float),
+        threshold_phase=float(np.max(k.medium.sample(critical)["phase_index"])),
+        g=float(k.medium.g), fold_bands=np.asarray(fold.bands, np.int64),
+        fold_scale=np.asarray(fold.scale, float), fold_phase=np.asarray(fold.phase_index, float),
+        mus=prompt["mus"], mut=prompt["mut"], speed=prompt["speed"], s0w=prompt["s0w"],
+        s2w=prompt["s2w"], **{f"optics_{key}": optics[key] for key in (
+            "panel_edges", "phase_nodes", "group_nodes", "extinction_nodes",
+            "efficiency_coefficients")},
+        alpha=np.asarray(k.acceptance()["alpha"], float),
+        peak_acceptance=float(np.max(np.abs(np.asarray(
+            d.angular_acceptance(np.linspace(-1, 1, 257)), float)))),
+        positions_m=np.asarray(d.positions_m, float),
+        looks=np.asarray(-d.orientations, float),
+        areas_m2=np.broadcast_to(np.asarray(d.effective_area_m2, float), (n_om,)).copy(),
+        radii_m=np.broadcast_to(np.asarray(d.receiver_surface.radii(n_om), float), (n_om,)).copy(),
+        omega_per_ns=omega, readout_omega_per_ns=np.asarray(k.config.readout_omega_per_ns, float),
+        edges_ns=np.asarray(k.config.relative_time_edges_ns, float),
+        radial_range_m=np.asarray(k.config.radial_range_m, float),
+        threshold_pe=float(k.config.threshold_pe), source_degree=int(k.config.source_degree),
+        azimuthal_degree=int(k.config.azimuthal_degree))
+    print("wrote", name, "fold", fold.bands, fold.scale)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "c0")

@@ -1,0 +1,83 @@
+"""The device shower route against the reference's own ShowerTransport response (``-m gpu``).
+
+Fixture: ``tests/golden/shower_c0.npz`` (``make_shower_golden.py``): the
+README-example shower (48 OMs, 2000 elements) through the reference's
+float64 route. Tolerances, per order, relative to the reference's per-OM
+charge for OMs at or above threshold: order 0 ORDER0 (ray quadrature vs the
+reference's control variates, float32 azimuth), order 1 ORDER1 (identical
+grouping; the reference's coarse-screened OMs are below threshold), order >=2
+ORDER2 of the OM's total charge (complex64 channels, float32 contraction,
+split-BF16 readout). Clocks are bit-identical and the active mask identical
+away from threshold.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+ORDER0 = 1e-4
+ORDER1 = 1e-5
+ORDER2 = 1e-4
+BINS_L1 = 1e-3
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def route_response():
+    from lighthit_b200.shower import ShowerTables, ShowerTransport
+    el = np.load(GOLDEN / "order0_c0.npz")
+    source = {k: el[k] for k in ("start_m", "direction", "length_m", "coefficient0",
+                                 "coefficient2", "beta", "start_ns", "end_ns")}
+    route = ShowerTransport(ShowerTables.synthetic("c0"))
+    return route(source), np.load(GOLDEN / "shower_c0.npz")
+
+
+def test_clock_is_bit_identical(route_response):
+    r, g = route_response
+    np.testing.assert_array_equal(r.time_origin_ns, g["time_origin_ns"])
+
+
+def test_active_mask_and_levels(route_response):
+    r, g = route_response
+    total = g["charge_components_pe"].sum(axis=1)
+    thr = float(g["threshold_pe"])
+    clear = np.abs(total - thr) > 1e-3 * thr
+    np.testing.assert_array_equal(r.active[clear], g["active"][clear])
+    np.testing.assert_array_equal(np.asarray(r.metadata["ge2_charge_level"]), g["ge2_charge_level"])
+
+
+def test_charge_per_order_matches_reference(route_response):
+    r, g = route_response
+    ref = g["charge_components_pe"]
+    total = ref.sum(axis=1)
+    big = total >= float(g["threshold_pe"])
+    q = r.charge_components_pe
+    e0 = np.abs(q[big, 0] - ref[big, 0]) / np.maximum(ref[big, 0], 1e-30)
+    e1 = np.abs(q[big, 1] - ref[big, 1]) / np.maximum(ref[big, 1], 1e-30)
+    e2 = np.abs(q[big, 2] - ref[big, 2]) / total[big]
+    et = np.abs(q[big].sum(axis=1) - total[big]) / total[big]
+    print(f"max rel error: order0 {e0.max():.2e} order1 {e1.max():.2e} order>=2 {e2.max():.2e} "
+          f"total {et.max():.2e}")
+    assert e0.max() < ORDER0 and e1.max() < ORDER1 and e2.max() < ORDER2
+    assert et.max() < 1e-3
+
+
+def test_bins_per_order_match_reference(route_response):
+    r, g = route_response
+    act = g["active"] & r.active
+    ref = g["components_pe"].astype(float)
+    total = g["charge_components_pe"].sum(axis=1)
+    for order in range(3):
+        l1 = np.abs(r.components_pe[act, :, order] - ref[act, :, order]).sum(axis=1) / total[act]
+        print(f"order {order} bins L1 / charge max {l1.max():.2e}")
+        assert l1.max() < BINS_L1, order
+
+
+def test_ge2_spectrum_matches_reference(route_response):
+    r, g = route_response
+    act = g["active"] & r.active
+    ref = g["spectrum_ge2_pe"][:, act]
+    got = r.spectrum_ge2_pe[:, act]
+    scale = np.abs(ref).max(axis=0)
+    assert (np.abs(got - ref).max(axis=0) / scale).max() < 1e-3
