@@ -54,6 +54,14 @@ class PromptSettings:
                    merge_theta_ratio=config.merge_theta_ratio,
                    merge_tau_ns=config.merge_tau_ns, merge_log_r=config.merge_log_r)
 
+    def screen(self):
+        """The coarse charge screen's pencils and merge (``prompt.py:1155-1160``,
+        ``_prompt_screen.compress_screen``: 2 m cells, 8-pixel faces, 24 ring
+        nodes; merge ratio 0.3 and 2 ns)."""
+        from dataclasses import replace
+        return replace(self, cell_m=2.0, pixel_face=8, ring_nodes=24, merge_theta_ratio=0.3,
+                       merge_tau_ns=2.0)
+
 
 def _ifuncs(z):
     """``I_k(z) = int_0^1 x^k e^{z x} dx``, k = 0, 1, 2 (``_prompt_numba.py:139-154``)."""
@@ -96,7 +104,8 @@ class Order1Tables:
     """Band constants, acceptance monomials, OMs and bin tables on the device."""
 
     def __init__(self, bands, g, monomials, positions_m, looks, areas_m2, edges, *,
-                 settings=PromptSettings(), group_capacity=8192, device="cuda"):
+                 settings=PromptSettings(), group_capacity=8192, compute_bins=True,
+                 device="cuda"):
         import torch
         self.device = torch.device(device)
         dev = self.device
@@ -134,12 +143,14 @@ class Order1Tables:
             t["mus"].data_ptr(), t["mut"].data_ptr(), t["speed"].data_ptr(), t["s0w"].data_ptr(),
             t["s2w"].data_ptr(), float(g), len(coef), t["coef"].data_ptr(), t["ipow"].data_ptr(),
             t["jpow"].data_ptr(), int(degree), len(edges), t["edges"].data_ptr(),
-            t["eedge"].data_ptr(), t["itab"].data_ptr(), 1, float(s.cell_m), int(s.pixel_face),
+            t["eedge"].data_ptr(), t["itab"].data_ptr(), int(bool(compute_bins)),
+            float(s.cell_m), int(s.pixel_face),
             int(s.ring_nodes), float(s.path_step), float(s.path_step_tail),
             float(s.tail_exponent), int(s.direct_bins), int(s.max_path_nodes),
             float(s.smoothing_factor), float(s.merge_theta_min), float(s.merge_theta_ratio),
             float(s.merge_tau_ns), float(s.merge_log_r), self.theta_bins, float(np.max(speed)),
             GAUSS_NODES, t["gauss_tau"].data_ptr(), t["gauss_w"].data_ptr(), int(group_capacity))
+        self.compute_bins = bool(compute_bins)
         self._workspace = None
 
     def workspace(self, n_subseg, n_work):
@@ -252,13 +263,16 @@ def grouped(tables: Order1Tables, table: "PencilTable", work, origins, *, n_penc
     origins_t = torch.as_tensor(np.asarray(origins, float) if not isinstance(origins, torch.Tensor)
                                 else origins, dtype=torch.float64, device=dev).contiguous()
     charge = torch.empty(n, dtype=torch.float64, device=dev)
-    bins = torch.empty((n, len(tables.edges) - 1), dtype=torch.float64, device=dev)
+    bins = (torch.empty((n, len(tables.edges) - 1), dtype=torch.float64, device=dev)
+            if tables.compute_bins else None)
     ws = tables.workspace(0, len(work))
     st = status if status is not None else torch.zeros(1, dtype=torch.int32, device=dev)
     sp = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
     _lib.check(_lib.load().lh_order1_grouped(tables.struct, table.struct, n_p,
                                              work_t.data_ptr(), len(work), origins_t.data_ptr(),
-                                             charge.data_ptr(), bins.data_ptr(), ws.data_ptr(),
+                                             charge.data_ptr(),
+                                             bins.data_ptr() if bins is not None else None,
+                                             ws.data_ptr(),
                                              ws.numel(), st.data_ptr(), sp),
                "lh_order1_grouped")
     if status is None:

@@ -18,9 +18,13 @@ Tables are built once by the reference and stored under ``tables/``
 detector constants. What the device route does not cover raises
 ``NotImplementedError`` with the reason (delayed light groups, basis points
 inside the table's inner radius, elements below threshold in a node band).
-Order 1 is evaluated at full resolution for every OM in reach: the
-reference's coarse screen (``_prompt_screen.py``) only lowers the accuracy of
-OMs it proves to be below threshold.
+Order 1 follows the reference's global screen (``prompt.py:720-812``): a
+coarse charge pass (2 m cells, 8-pixel faces, 24 ring nodes) for every OM in
+reach, full resolution where ``q0 + extra + 3 q1_coarse`` reaches threshold,
+widened when the coarse pass underestimated. The coarse pass is the grouped
+evaluator on coarse pencils; the reference refines its coarse pixels near each
+OM (``_prompt_screen.py``), so coarse-only OMs (below threshold by
+construction) carry a different coarse order-1 charge.
 """
 from __future__ import annotations
 
@@ -55,6 +59,8 @@ class ShowerSettings:
     min_distance_m: float = 0.1          # PromptConfig.min_distance_m
     readout_mode: str = "split-bf16"
     order0_gauss: int = 8
+    screen: bool = True                  # PromptConfig.screen
+    screen_margin: float = 3.0           # PromptConfig.screen_margin
 
 
 @dataclass
@@ -122,6 +128,10 @@ class ShowerTables:
         self.order1 = Order1Tables(self.prompt, self.g, acceptance_monomials(self.alpha),
                                    self.positions, self.looks, self.areas, self.edges,
                                    settings=PromptSettings(), device=device)
+        self.order1_screen = Order1Tables(self.prompt, self.g, acceptance_monomials(self.alpha),
+                                          self.positions, self.looks, self.areas, self.edges,
+                                          settings=PromptSettings().screen(), compute_bins=False,
+                                          device=device)
         bands = self.fold_bands
         self.source = SourceCompiler(self.wavelengths[bands], self.fold_phase,
                                      self.fold_scale[bands], self.source_degree,
@@ -384,8 +394,12 @@ class ShowerTransport:
         spectrum[0] = charge[:, 2] - late_charge
         components = np.zeros((n, len(edges) - 1, 3))
         if np.any(active):
-            if not np.all(computed[active]):
-                raise ValueError("prompt did not compute every active OM")
+            missing = np.flatnonzero(active & ~computed)
+            if len(missing):
+                # the reference recomputes the prompt without its screen (shower/api.py:592-599)
+                q1m, b1m = self._fine_order1(prompt_el, origins, missing)
+                charge[missing, 1] = q1m
+                b1[missing] = b1m
             ids = np.flatnonzero(active)
             # order-0 bins of the active OMs (PreparedBallistic.bins, prompt.py:896-903);
             # their charge is the binned integral's, as in the reference
@@ -416,6 +430,14 @@ class ShowerTransport:
             "elapsed_seconds": perf_counter() - began}
         return HybridTransportResponse(None, omega.copy(), edges.copy(), spectrum, components,
                                        charge, origins, active, "shower", metadata)
+
+    def _fine_order1(self, el, origins, ids):
+        """Full-resolution order 1 (charge, bins) of the OMs ``ids``."""
+        T = self.tables
+        cone = float(np.sum(T.prompt["s0w"] * T.phase) / np.sum(T.prompt["s0w"]))
+        table = pencils(T.order1, el, 1.0 / (el["beta"] * cone))
+        q1, bins1 = grouped(T.order1, table, ids, origins)
+        return q1.cpu().numpy()[ids], bins1.cpu().numpy()[ids]
 
     def _prompt(self, el, origins, extra):
         """Orders 0 and 1 charges (``transport_prompt``, ``prompt.py:500-947``)."""
@@ -459,8 +481,36 @@ class ShowerTransport:
             raise NotImplementedError("elements above threshold in only some bands need the "
                                       "per-band order-1 units")
         cone = float(np.sum(T.prompt["s0w"] * T.phase) / np.sum(T.prompt["s0w"]))
-        table = pencils(T.order1, el, 1.0 / (el["beta"] * cone))
-        q1, b1 = grouped(T.order1, table, work, origins)
-        charge[work, 1] = q1.cpu().numpy()[work]
-        level[work] = 2
-        return charge, b1.cpu().numpy(), inside, level, el
+        cone_cos = 1.0 / (el["beta"] * cone)
+        # coarse charge screen and the reference's decision rule (prompt.py:720-812):
+        # full resolution where q0 + extra + margin * q1_coarse reaches threshold
+        fine_work = work
+        coarse = None
+        if cfg.screen and threshold > 0:
+            coarse = grouped(T.order1_screen, pencils(T.order1_screen, el, cone_cos), work,
+                             origins)[0].cpu().numpy()
+            charge[work, 1] = coarse[work]
+            level[work] = 1
+            fine_work = work[(charge[work, 0] + extra[work] + cfg.screen_margin
+                              * np.maximum(coarse[work], 0.0)) >= threshold]
+        b1 = np.zeros((n, len(edges) - 1))
+        if len(fine_work):
+            table = pencils(T.order1, el, cone_cos)
+            q1, bins1 = grouped(T.order1, table, fine_work, origins)
+            q1, bins1 = q1.cpu().numpy(), bins1.cpu().numpy()
+            charge[fine_work, 1] = q1[fine_work]
+            b1[fine_work] = bins1[fine_work]
+            level[fine_work] = 2
+            if coarse is not None:
+                worst = float(np.min(coarse[fine_work] / np.maximum(q1[fine_work], 1e-300)))
+                if worst * cfg.screen_margin < 1.0:
+                    wider = 1.5 / max(worst, 1e-3)
+                    more = work[(level[work] == 1) & (charge[work, 0] + extra[work] + wider
+                                                      * np.maximum(coarse[work], 0.0)
+                                                      >= threshold)]
+                    if len(more):
+                        q1, bins1 = grouped(T.order1, table, more, origins)
+                        charge[more, 1] = q1.cpu().numpy()[more]
+                        b1[more] = bins1.cpu().numpy()[more]
+                        level[more] = 2
+        return charge, b1, level == 2, level, el
