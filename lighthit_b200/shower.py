@@ -207,12 +207,36 @@ def _subset(el, mask):
     return {k: v[mask] for k, v in el.items()}
 
 
-class ShowerTransport:
-    """``ShowerTransport(kernel, data)(source, ...)`` on the device route."""
+class _Stages:
+    """Wall time per route stage (``metadata['timings']``); with ``sync`` the
+    device is synchronised at every boundary so each stage owns its GPU time."""
 
-    def __init__(self, tables: ShowerTables, config: ShowerSettings | None = None):
+    def __init__(self, sync):
+        self.sync = sync
+        self.times = {}
+        self.last = perf_counter()
+
+    def __call__(self, name):
+        if self.sync:
+            import torch
+            torch.cuda.synchronize()
+        now = perf_counter()
+        self.times[name] = self.times.get(name, 0.0) + now - self.last
+        self.last = now
+
+
+class ShowerTransport:
+    """``ShowerTransport(kernel, data)(source, ...)`` on the device route.
+
+    ``profile=True`` synchronises the device between stages so that
+    ``metadata['timings']`` attributes the GPU time to each stage.
+    """
+
+    def __init__(self, tables: ShowerTables, config: ShowerSettings | None = None, *,
+                 profile=False):
         self.tables = tables
         self.config = config or tables.settings
+        self.profile = profile
 
     def _apply(self, points, channels, reference, frame, oms, *, zero_frequency):
         """``apply_folded`` (``shower/ge2.py:99-119``) for the OMs ``oms``: (frequency, OM)."""
@@ -242,6 +266,7 @@ class ShowerTransport:
         if receivers is not None:
             raise NotImplementedError("receiver subsets: build ShowerTables for those OMs")
         began = perf_counter()
+        stage = _Stages(self.profile)
         T, cfg = self.tables, self.config
         n = T.n_om
         omega, edges, threshold = T.omega, T.edges, T.threshold
@@ -264,6 +289,7 @@ class ShowerTransport:
         if np.any(delay > cfg.prompt_delay_ns):
             raise NotImplementedError("delayed light groups (steps more than prompt_delay_ns "
                                       "behind the light front) are not on the device route")
+        stage("setup")
         # ---- order >=2 source on the node bands (shower/api.py:373-402)
         frame = axis_frame(el["start_m"], el["direction"], el["length_m"], el["coefficient0"])
         pts_d, ch_d, npts_d, reference, frame = T.source.compile(el, frame)
@@ -280,26 +306,31 @@ class ShowerTransport:
         else:
             channels = [ch_d[b, :int(npts[b])] for b in range(nb_bands)]
         zero_ch = [ch_d[b, :int(npts[b]), :, 0].cpu().numpy() for b in range(nb_bands)]
+        stage("source_compile")
         # ---- radial windows (shower/api.py:322-340, shower_basis.py:408-439)
         used = np.zeros(n, np.int64)
         near = np.zeros(n, bool)
         tail = np.zeros(n)
         weight_ratio = float(np.sum(T.fold_scale) / np.sum(T.fold_scale[T.fold_bands]))
+        radius = None
         for b, band in enumerate(T.fold_bands):
             photons = np.sqrt(4 * np.pi) * np.abs(zero_ch[b][:, 0]) / T.efficiency[band]
-            radius = np.linalg.norm(points[b][None] - T.positions[:, None], axis=2)
-            n_near = np.count_nonzero(radius < low, axis=1)
-            far_mask = radius > high
-            used = np.maximum(used, len(points[b]) - n_near - np.count_nonzero(far_mask, axis=1))
+            if radius is None or not np.array_equal(points[b], points[b - 1]):
+                radius = np.sqrt(((points[b][None] - T.positions[:, None]) ** 2).sum(axis=2))
+                n_near = np.count_nonzero(radius < low, axis=1)
+                om, pt = np.nonzero(radius > high)
+                n_far = np.bincount(om, minlength=n)
+                far_factor = T.attenuation(radius[om, pt]) / (4 * np.pi * radius[om, pt] ** 2)
+            used = np.maximum(used, len(points[b]) - n_near - n_far)
             near |= n_near > 0
-            dist = np.where(far_mask, radius, 1.0)
             tail += weight_ratio * (10 * T.areas * T.peak_acceptance * T.efficiency[band]
-                                    * np.sum(np.where(far_mask, photons[None] * T.attenuation(dist)
-                                                      / (4 * np.pi * dist ** 2), 0.0), axis=1))
+                                    * np.bincount(om, weights=photons[pt] * far_factor,
+                                                  minlength=n))
         if np.any(near):
             raise NotImplementedError("basis points inside the table's inner radius need the "
                                       "near-field clamp (near_field.py), not on the device route")
         reach = np.flatnonzero(used > 0)
+        stage("radial_window")
         # ---- predictor (shower/ge2.py:70-96) and its zero-frequency charge
         predicted = np.zeros(n)
         late_charge = np.zeros(n)
@@ -311,24 +342,26 @@ class ShowerTransport:
                 keys = np.floor(coords / float(cfg.predictor_cell_m)).astype(np.int64)
                 _, inverse = np.unique(keys, axis=0, return_inverse=True)
                 inverse = np.asarray(inverse).ravel()
+                groups = int(inverse.max()) + 1
                 wgt = np.abs(zero_ch[b][:, 0])
-                zs, ts, chs = [], [], []
-                for grp in range(int(inverse.max()) + 1):
-                    chunk = np.flatnonzero(inverse == grp)
-                    tot = wgt[chunk].sum()
-                    share = wgt[chunk] / tot if tot > 0 else np.full(len(chunk), 1.0 / len(chunk))
-                    zs.append(np.sum(share * coords[chunk, 0]))
-                    ts.append(share @ coords[chunk, 1:])
-                    chs.append(zero_ch[b][chunk].sum(axis=0))
-                zs, ts = np.asarray(zs), np.asarray(ts)
-                c_points.append(centre + zs[:, None] * axis + ts[:, :1] * e1 + ts[:, 1:2] * e2)
-                c_channels.append(np.asarray(chs)[:, :, None])
+                total = np.bincount(inverse, weights=wgt, minlength=groups)
+                count = np.bincount(inverse, minlength=groups)
+                share = np.where(total[inverse] > 0, wgt / np.where(total > 0, total, 1.0)[inverse],
+                                 1.0 / count[inverse])
+                centroid = np.stack([np.bincount(inverse, weights=share * coords[:, k],
+                                                 minlength=groups) for k in range(3)], axis=1)
+                summed = np.zeros((groups, zero_ch[b].shape[1]), complex)
+                np.add.at(summed, inverse, zero_ch[b])
+                c_points.append(centre + centroid[:, :1] * axis + centroid[:, 1:2] * e1
+                                + centroid[:, 2:3] * e2)
+                c_channels.append(summed[:, :, None])
             if all(len(p) == len(c_points[0]) for p in c_points[1:]):
                 c_ch = np.stack(c_channels)
             else:
                 c_ch = c_channels
             predicted[reach] = self._apply(c_points, c_ch, reference, frame, reach,
                                            zero_frequency=True)[0].real
+        stage("predictor")
         # ---- clocks (shower/api.py:455-477)
         fastest = float(np.min(T.group))
         time_width = float(np.ptp(edges))
@@ -348,7 +381,9 @@ class ShowerTransport:
                        / (C_M_PER_NS / fastest))
         safety = float(cfg.predictor_safety)
         prompt_extra = safety * np.abs(predicted) + np.abs(late_charge) + extra
-        charge01, b1, computed, level1, prompt_el = self._prompt(el, origins, prompt_extra)
+        stage("clock")
+        charge01, b1, computed, level1, prompt_el, bins0 = self._prompt(el, origins, prompt_extra,
+                                                                        stage)
         # ---- exact zero-frequency >=2 where the decision needs it (shower/api.py:488-525)
         charge = np.zeros((n, 3))
         charge[:, :2] = charge01
@@ -385,12 +420,14 @@ class ShowerTransport:
             active = computable
         if np.any(active & (level == 1)):
             raise RuntimeError("an OM was activated by a predicted >=2 charge")
+        stage("ge2_exact_zero")
         # ---- full frequencies for the active OMs, then the readout
         spectrum = np.zeros((len(omega), n), complex)
         work = np.flatnonzero(active & (used > 0))
         if len(work):
             spectrum[:, work] = self._apply(points, channels, reference, frame, work,
                                             zero_frequency=False)
+        stage("ge2_full")
         spectrum[0] = charge[:, 2] - late_charge
         components = np.zeros((n, len(edges) - 1, 3))
         if np.any(active):
@@ -403,17 +440,15 @@ class ShowerTransport:
             ids = np.flatnonzero(active)
             # order-0 bins of the active OMs (PreparedBallistic.bins, prompt.py:896-903);
             # their charge is the binned integral's, as in the reference
-            full = np.zeros(n)
-            full[ids] = origins[ids]
-            out0 = order0(T.order0, [prompt_el], full[None], edges)
-            charge[ids, 0] = out0["charge"][0].cpu().numpy()[ids]
-            components[ids, :, 0] = out0["bins"][0].cpu().numpy()[ids]
+            components[ids, :, 0] = bins0[ids]
             components[ids, :, 1] = b1[ids]
+            stage("order0_bins")
             rel = spectrum[:, ids] * np.exp(-1j * omega[:, None] * origins[None, ids])
             rel_t = torch.tensor(np.ascontiguousarray(rel.T).astype(np.complex64),
                                  device=T.device)
             bins2, _ = T.readout.bins(rel_t, mode=cfg.readout_mode)
             components[ids, :, 2] = bins2.cpu().numpy().astype(float)
+        stage("readout")
         metadata = {
             "route": "lighthit_b200.shower", "ge2_charge_level": level.tolist(),
             "ge2_predictor": {"cell_m": float(cfg.predictor_cell_m), "safety": safety,
@@ -427,7 +462,7 @@ class ShowerTransport:
                             else "earliest element start and fastest group flight"),
             "active_modules": int(active.sum()), "threshold_pe": threshold,
             "ge2_points": [int(v) for v in npts], "source_elements": len(el["beta"]),
-            "elapsed_seconds": perf_counter() - began}
+            "elapsed_seconds": perf_counter() - began, "timings": stage.times}
         return HybridTransportResponse(None, omega.copy(), edges.copy(), spectrum, components,
                                        charge, origins, active, "shower", metadata)
 
@@ -439,7 +474,7 @@ class ShowerTransport:
         q1, bins1 = grouped(T.order1, table, ids, origins)
         return q1.cpu().numpy()[ids], bins1.cpu().numpy()[ids]
 
-    def _prompt(self, el, origins, extra):
+    def _prompt(self, el, origins, extra, stage):
         """Orders 0 and 1 charges (``transport_prompt``, ``prompt.py:500-947``)."""
         T, cfg = self.tables, self.config
         n = T.n_om
@@ -469,12 +504,19 @@ class ShowerTransport:
             raise ValueError(f"{int(too_close.sum())} OMs are closer than min_distance_m="
                              f"{cfg.min_distance_m:g} m to the source")
         work = np.flatnonzero(inside)
+        stage("prompt_selection")
         charge = np.zeros((n, 2))
         level = np.zeros(n, np.int8)
         if not len(work):
-            return charge, np.zeros((n, len(edges) - 1)), inside, level, el
-        q0 = order0(T.order0, [el])["charge"][0].cpu().numpy()
+            empty = np.zeros((n, len(edges) - 1))
+            return charge, empty, inside, level, el, empty
+        # one order-0 pass gives the charge of every OM and the bins (PreparedBallistic.charge
+        # and .bins integrate the same light; the route keeps the binned charge of active OMs)
+        out0 = order0(T.order0, [el], origins[None], edges)
+        q0 = out0["charge"][0].cpu().numpy()
+        bins0 = out0["bins"][0]
         charge[work, 0] = q0[work]
+        stage("order0_charge")
         # order 1: the fused unit of elements emitting in every band
         # (prompt.py:689-707, muon/secondary_first.py:184-204)
         if not np.all(el["beta"][:, None] * T.phase[None, :] > 1):
@@ -491,6 +533,7 @@ class ShowerTransport:
                              origins)[0].cpu().numpy()
             charge[work, 1] = coarse[work]
             level[work] = 1
+            stage("order1_screen")
             fine_work = work[(charge[work, 0] + extra[work] + cfg.screen_margin
                               * np.maximum(coarse[work], 0.0)) >= threshold]
         b1 = np.zeros((n, len(edges) - 1))
@@ -513,4 +556,5 @@ class ShowerTransport:
                         charge[more, 1] = q1.cpu().numpy()[more]
                         b1[more] = bins1.cpu().numpy()[more]
                         level[more] = 2
-        return charge, b1, level == 2, level, el
+        stage("order1_fine")
+        return charge, b1, level == 2, level, el, bins0.cpu().numpy()
