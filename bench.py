@@ -190,6 +190,86 @@ def reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+N_SHOWER = 48
+
+
+def shower_stream_section(dev, steps, workers=4):
+    """Config 2: the served shower stream at 384 OMs through the device route.
+
+    ``plain_fp32``: one shower after another on one stream, fp32 readout (the
+    per-event path). ``served``: the serving loop, ``workers`` worker streams,
+    split-BF16 readout. Wall time with the device synchronised on both sides
+    (several streams and host orchestration: the device clock of one stream
+    does not cover the job).
+    """
+    import torch
+    from lighthit_b200.serve_shower import ShowerServer
+    from lighthit_b200.shower import ShowerSettings, ShowerTables, ShowerTransport
+    from lighthit_b200.workloads import gaussian_shower, shower_stream
+    plain = ShowerTransport(ShowerTables.synthetic("c2", device=dev,
+                                                   settings=ShowerSettings(readout_mode="fp32")))
+    centroid = plain.tables.positions.mean(axis=0)
+    draws = shower_stream(N_SHOWER, centroid)
+    showers = [gaussian_shower(d["position_m"], d["direction"],
+                               charged_track_length_m=d["charged_track_length_m"],
+                               elements=d["elements"], seed=d["seed"]) for d in draws]
+    for el in showers[:3]:
+        plain(el)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    reps = max(1, min(steps, 2))
+    stage = {}
+    for _ in range(reps):
+        for el in showers:
+            r = plain(el)
+            for k, v in r.metadata["timings"].items():
+                stage[k] = stage.get(k, 0.0) + v
+    torch.cuda.synchronize(dev)
+    plain_s = (time.perf_counter() - t0) / reps
+    server = ShowerServer(lambda: ShowerTransport(ShowerTables.synthetic("c2", device=dev)),
+                          workers=workers)
+    for el in showers[:workers]:
+        server.submit(el)
+    server.drain(workers)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        for el in showers:
+            server.submit(el)
+        done = server.drain(len(showers))
+        assert all(r.error is None for r in done), [r.error for r in done if r.error][:1]
+    torch.cuda.synchronize(dev)
+    served_s = (time.perf_counter() - t0) / reps
+    served_rate = len(showers) / served_s
+    # latency under Poisson arrivals at half the served rate
+    rng = np.random.default_rng(22)
+    arrivals = np.cumsum(rng.exponential(1.0 / (0.5 * served_rate), size=len(showers)))
+    start = time.perf_counter()
+    for k, el in enumerate(showers):
+        wait = start + arrivals[k] - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        server.submit(el, arrival=start + arrivals[k])
+    lat = np.array([r.latency for r in server.drain(len(showers))]) * 1e3
+    server.close()
+    sizes = [d["elements"] for d in draws]
+    return {"workload": f"config 2: {N_SHOWER} Gaussian showers of the seed-21 stream "
+                        "(500-50000 elements log-uniform, 0.15 m per element, vertices in a "
+                        "200 m x 600 m cylinder, isotropic) on the 384-OM array, tables 2-450 m",
+            "value": served_rate, "unit": "showers/s", "served_workers": workers,
+            "plain_fp32": {"value": len(showers) / plain_s, "unit": "showers/s",
+                           "launch": "the device route per shower on one stream, fp32 readout"},
+            "served_over_plain": served_rate * plain_s / len(showers),
+            "latency": {"p50_ms": float(np.percentile(lat, 50)),
+                        "p99_ms": float(np.percentile(lat, 99)),
+                        "offered_showers_per_s": 0.5 * served_rate, "requests": len(lat)},
+            "elements_per_shower": {"min": int(min(sizes)), "median": int(np.median(sizes)),
+                                    "max": int(max(sizes))},
+            "plain_stage_ms_per_shower": {k: 1e3 * v / (reps * len(showers))
+                                          for k, v in sorted(stage.items(), key=lambda x: -x[1])},
+            "timing": "wall clock, device synchronised before and after"}
+
+
 def _events(torch, n):
     return [torch.cuda.Event(enable_timing=True) for _ in range(n)]
 
@@ -348,6 +428,10 @@ def ours(args, rank, world, local_rank):
         srv.completed.clear()  # the client takes each result as it completes
     lat_ms = np.array(latencies) * 1e3
 
+    showers = None
+    if not args.no_showers:
+        showers = shower_stream_section(dev, args.steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         sample = 128
@@ -386,6 +470,7 @@ def ours(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h, "wall_s": wall, "steps": e2e_steps,
                     "path": "FlashServer (serving loop): pinned staging, graph replay, D2H of "
                             "every response field"},
+            "shower_stream": showers,
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
         }
@@ -399,6 +484,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-showers", action="store_true", help="skip the shower-stream section")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
