@@ -214,8 +214,7 @@ typedef struct {
 typedef struct {
   int32_t n_events;
   const int64_t* element_offset; /* [n_events + 1] event e owns elements [off[e], off[e+1]) */
-  const int64_t* chunk_offset;   /* [n_events + 1] from lh_order0_chunks                  */
-  int64_t n_chunks;              /* host: chunk_offset[n_events]                          */
+  int64_t n_elements;            /* host: element_offset[n_events]; n_elements * n_om < 2^31 */
   const double* start;           /* [n_el][3] m                                           */
   const double* direction;       /* [n_el][3] unit                                        */
   const double* length;          /* [n_el] m                                              */
@@ -230,11 +229,12 @@ typedef struct {
   double* charge;                /* [n_events][n_om] pe (overwritten)                     */
   double* bins;                  /* [n_events][n_om][n_edges-1] pe (overwritten) or NULL  */
   int32_t* status;               /* [1] LH_STATUS_* flags (or-ed in)                      */
+  void* workspace;               /* lh_order0_workspace_bytes bytes of device memory      */
+  size_t workspace_bytes;
 } lh_order0_batch;
 
-/* Chunks of the element lists (host helper): fills chunk_offset_host[n_events+1]
- * and returns the total. */
-size_t lh_order0_chunks(const int64_t* element_counts, int32_t n_events, int64_t* chunk_offset_host);
+/* Device scratch for one call: candidate-pair lists (4 bytes per (OM, element)). */
+size_t lh_order0_workspace_bytes(const lh_order0_optics* optics, const lh_order0_batch* batch);
 
 int lh_order0(const lh_order0_optics* optics, const lh_order0_batch* batch, void* stream);
 

@@ -71,11 +71,11 @@ class Order0Optics(C.Structure):
 
 
 class Order0Batch(C.Structure):
-    _fields_ = [("n_events", C.c_int32), ("element_offset", P), ("chunk_offset", P),
-                ("n_chunks", C.c_int64), ("start", P), ("direction", P), ("length", P),
+    _fields_ = [("n_events", C.c_int32), ("element_offset", P), ("n_elements", C.c_int64),
+                ("start", P), ("direction", P), ("length", P),
                 ("c0", P), ("c2", P), ("beta", P), ("t0", P), ("t1", P), ("origins", P),
                 ("n_edges", C.c_int32), ("edges", P), ("charge", P), ("bins", P),
-                ("status", P)]
+                ("status", P), ("workspace", P), ("workspace_bytes", C.c_size_t)]
 
 
 class Order1Config(C.Structure):
@@ -148,7 +148,7 @@ SIGNATURES = {
                                              C.POINTER(FlashBatch), P]),
     "lh_ge2_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem)]),
     "lh_ge2_apply": (C.c_int, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem), P, C.c_size_t, P]),
-    "lh_order0_chunks": (C.c_size_t, [P, C.c_int32, P]),
+    "lh_order0_workspace_bytes": (C.c_size_t, [C.POINTER(Order0Optics), C.POINTER(Order0Batch)]),
     "lh_order0": (C.c_int, [C.POINTER(Order0Optics), C.POINTER(Order0Batch), P]),
     "lh_order1_workspace_bytes": (C.c_size_t, [C.POINTER(Order1Config), C.c_int64, C.c_int32]),
     "lh_order1_pencils": (C.c_int, [C.POINTER(Order1Config), C.POINTER(Order1Elements),

@@ -25,11 +25,15 @@
 //       + (E0 - along sin(th) 2 sin^2(phi/2))^2,
 // E0 = along sin(th) - rho cos(th) formed in float64.
 //
-// Launch: one CTA per (OM, chunk of 32 elements of one event). Warp 0 tests
-// the chunk's elements (candidates) and forms each pair's frame; the CTA then
+// Launch: a candidate pass (one thread per (OM, element), warp-aggregated
+// counts per (event, OM)), a scan into per-(event, OM) pair segments and a
+// list of 32-pair chunks, a second candidate pass listing the pairs, then a
+// persistent grid over the chunks: warp 0 forms each pair's frame, the CTA
 // lists the (pair, panel, piece) work, spreads (piece x wavelength node) over
 // its threads, accumulates bins in shared memory and the charge by a block
-// reduction, and adds both to the outputs once.
+// reduction, and adds both to the outputs once per chunk.
+#include <algorithm>
+
 #include "lh_common.cuh"
 
 namespace lh {
@@ -189,6 +193,163 @@ LH_DEVICE float o0_acceptance(const float* alpha, int n_alpha, float x, float al
   return result;
 }
 
+
+// interval_candidates (_ballistic_interval_numba.py:449-519) with the sphere
+// always in reach and the axis included: does element i light OM om at all?
+LH_DEVICE bool o0_is_candidate(const lh_order0_optics& O, const lh_order0_batch& B, int om,
+                               int64_t i, double pmin, double pmax, uint32_t& flags) {
+  const double radius = O.om_radius[om];
+  const double beta = B.beta[i], len = B.length[i];
+  const double ux = B.direction[3 * i], uy = B.direction[3 * i + 1], uz = B.direction[3 * i + 2];
+  const double wx = O.om_pos[3 * om] - B.start[3 * i], wy = O.om_pos[3 * om + 1] - B.start[3 * i + 1],
+               wz = O.om_pos[3 * om + 2] - B.start[3 * i + 2];
+  const double z = wx * ux + wy * uy + wz * uz;
+  const bool sphere = radius > 0.0;
+  if (B.c0[i] == 0.0 || beta * pmax <= 1.0 || (z <= 0.0 && (!sphere || z <= -radius))) return false;
+  const double cx = wy * uz - wz * uy, cy = wz * ux - wx * uz, cz = wx * uy - wy * ux;
+  const double rho_c = sqrt(cx * cx + cy * cy + cz * cz);
+  const double rad = sphere ? radius : 0.0;
+  if (z <= 0.0 && rad == 0.0) return false;
+  if (rho_c == 0.0) {
+    if (rad == 0.0) {
+      if (0.0 < z && z < len) flags |= LH_STATUS_ON_TRACK;
+      return false;
+    }
+    return true;
+  }
+  if (rad == 0.0) return false;  // a point receiver has no first-entry window: no light here
+  if (!o0_cone_reaches(z, rho_c, len, beta, rad, pmin, pmax)) return false;
+  double a, b, c, d;
+  return o0_support(z, rho_c, len, beta, rad, a, b, c, d) && !(a > pmax || b <= pmin);
+}
+
+LH_DEVICE void o0_phase_range(const lh_order0_optics& O, double& pmin, double& pmax) {
+  pmin = O.phase[0];
+  pmax = O.phase[0];
+  for (int k = 1; k < O.n_panel_edges; ++k) {
+    pmin = fmin(pmin, O.phase[k]);
+    pmax = fmax(pmax, O.phase[k]);
+  }
+}
+
+LH_DEVICE int o0_event_of(const lh_order0_batch& B, int64_t i) {
+  int lo = 0, hi = B.n_events;  // last event with element_offset[ev] <= i
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (B.element_offset[mid] <= i) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+struct O0Work {
+  int32_t* counts;    // [n_events * n_om] candidate pairs
+  int32_t* offsets;   // [n_events * n_om] first pair of each (event, OM)
+  int32_t* cursor;    // [n_events * n_om]
+  int32_t* pairs;     // [pair capacity] global element index
+  int2* chunks;       // [chunk capacity] (event * n_om + om, chunk)
+  int32_t* n_chunks;  // [1]
+  int64_t pair_capacity, chunk_capacity;
+};
+
+// Candidate pairs counted (fill = false) or listed (fill = true) per (event, OM):
+// one thread per (OM, element); a warp's elements are consecutive, so the
+// lanes of one (event, OM) add their count once (warp-aggregated atomics).
+template <bool fill>
+__global__ void order0_candidates_kernel(const lh_order0_optics O, const lh_order0_batch B,
+                                         O0Work W) {
+  double pmin, pmax;
+  o0_phase_range(O, pmin, pmax);
+  const int64_t n_el = B.n_elements;
+  const int64_t total = n_el * O.n_om;
+  uint32_t flags = 0;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < total;
+       base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t item = base + threadIdx.x;
+    bool keep = false;
+    int key = -1;
+    int64_t i = 0;
+    if (item < total) {
+      const int om = (int)(item / n_el);
+      i = item - (int64_t)om * n_el;
+      keep = o0_is_candidate(O, B, om, i, pmin, pmax, flags);
+      key = o0_event_of(B, i) * O.n_om + om;
+    }
+    const unsigned active = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const unsigned peers = __match_any_sync(active, key);
+      const int leader = __ffs(peers) - 1;
+      const int lane = threadIdx.x & 31;
+      const int rank = __popc(peers & ((1u << lane) - 1u));
+      int first = 0;
+      if (lane == leader) first = atomicAdd(fill ? W.cursor + key : W.counts + key, __popc(peers));
+      first = __shfl_sync(peers, first, leader);
+      if (fill && first + rank < W.pair_capacity) W.pairs[first + rank] = (int32_t)i;
+    }
+  }
+  if (!fill && flags) atomicOr(reinterpret_cast<unsigned*>(B.status), flags);
+}
+
+// Single CTA: pair offsets per (event, OM) and the list of 32-pair chunks.
+__global__ void __launch_bounds__(1024) order0_scan_kernel(int32_t n_keys, O0Work W) {
+  __shared__ int32_t warp_sum[32], warp_chunks[32];
+  __shared__ int32_t carry, carry_chunks;
+  if (threadIdx.x == 0) {
+    carry = 0;
+    carry_chunks = 0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base = 0; base < n_keys; base += blockDim.x) {
+    const int key = base + threadIdx.x;
+    const int32_t c = key < n_keys ? W.counts[key] : 0;
+    const int32_t ch = (c + kO0Chunk - 1) / kO0Chunk;
+    int32_t v = c, h = ch;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int32_t a = __shfl_up_sync(0xffffffffu, v, off);
+      const int32_t b = __shfl_up_sync(0xffffffffu, h, off);
+      if (lane >= off) {
+        v += a;
+        h += b;
+      }
+    }
+    if (lane == 31) {
+      warp_sum[warp] = v;
+      warp_chunks[warp] = h;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      int32_t sv = lane < (int)(blockDim.x >> 5) ? warp_sum[lane] : 0;
+      int32_t sh = lane < (int)(blockDim.x >> 5) ? warp_chunks[lane] : 0;
+      for (int off = 1; off < 32; off <<= 1) {
+        const int32_t a = __shfl_up_sync(0xffffffffu, sv, off);
+        const int32_t b = __shfl_up_sync(0xffffffffu, sh, off);
+        if (lane >= off) {
+          sv += a;
+          sh += b;
+        }
+      }
+      warp_sum[lane] = sv;
+      warp_chunks[lane] = sh;
+    }
+    __syncthreads();
+    const int32_t before = (warp ? warp_sum[warp - 1] : 0) + v - c + carry;
+    const int32_t before_ch = (warp ? warp_chunks[warp - 1] : 0) + h - ch + carry_chunks;
+    if (key < n_keys) {
+      W.offsets[key] = before;
+      W.cursor[key] = before;
+      for (int j = 0; j < ch; ++j)
+        if (before_ch + j < W.chunk_capacity) W.chunks[before_ch + j] = make_int2(key, j);
+    }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) {
+      carry = before + c;
+      carry_chunks = before_ch + ch;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *W.n_chunks = carry_chunks;
+}
+
 struct O0Shared {
   double gx[kO0MaxOrder], gw[kO0MaxOrder];
   float alpha[kO0MaxAlpha];
@@ -199,7 +360,7 @@ struct O0Shared {
 };
 
 __global__ void __launch_bounds__(kO0Threads)
-order0_kernel(const lh_order0_optics O, const lh_order0_batch B) {
+order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W) {
   extern __shared__ __align__(16) unsigned char o0_smem[];
   O0Shared& S = *reinterpret_cast<O0Shared*>(o0_smem);
   const int n_panels = O.n_panel_edges - 1;
@@ -208,70 +369,41 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B) {
   double* sbins = reinterpret_cast<double*>(o0_smem + sizeof(O0Shared));
   uint32_t* combos = reinterpret_cast<uint32_t*>(sbins + (want_bins ? nb : 0));
   const int tid = threadIdx.x;
-
-  // chunk -> event
-  const int64_t chunk = blockIdx.x;
-  int lo = 0, hi = B.n_events;  // last event with chunk_offset[ev] <= chunk
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (B.chunk_offset[mid] <= chunk) lo = mid; else hi = mid;
-  }
-  const int ev = lo;
-  const int om = blockIdx.y;
-  const int64_t el_begin = B.element_offset[ev] + (chunk - B.chunk_offset[ev]) * kO0Chunk;
-  const int64_t el_end = min(B.element_offset[ev + 1], el_begin + kO0Chunk);
-  if (el_begin >= el_end) return;
-
   const int order = O.order;
   for (int k = tid; k < order; k += blockDim.x) {
     S.gx[k] = O.gauss_x[k];
     S.gw[k] = O.gauss_w[k];
   }
   for (int k = tid; k < O.n_alpha; k += blockDim.x) S.alpha[k] = (float)O.alpha[k];
+  double pmin, pmax;
+  o0_phase_range(O, pmin, pmax);
+  const int total_chunks = min(*W.n_chunks, (int)W.chunk_capacity);
+  for (int chunk = blockIdx.x; chunk < total_chunks; chunk += gridDim.x) {
+  __syncthreads();
+  const int2 entry = W.chunks[chunk];
+  const int ev = entry.x / O.n_om;
+  const int om = entry.x - ev * O.n_om;
+  const int p_begin = W.offsets[entry.x] + entry.y * kO0Chunk;
+  const int p_end = min(W.offsets[entry.x] + W.counts[entry.x], p_begin + kO0Chunk);
   if (want_bins)
     for (int k = tid; k < nb; k += blockDim.x) sbins[k] = 0.0;
   if (tid == 0) S.n_combos = 0;
-
-  double pmin = O.phase[0], pmax = O.phase[0];
-  for (int k = 1; k < O.n_panel_edges; ++k) {
-    pmin = fmin(pmin, O.phase[k]);
-    pmax = fmax(pmax, O.phase[k]);
-  }
   const double ox = O.om_pos[3 * om], oy = O.om_pos[3 * om + 1], oz = O.om_pos[3 * om + 2];
   const double radius = O.om_radius[om];
   uint32_t flags = 0;
 
-  // ---- phase 0: candidates of the chunk (warp 0) and their frames
+  // ---- phase 0: the chunk's candidate pairs (warp 0) and their frames
   if (tid < 32) {
-    const int64_t i = el_begin + tid;
+    const int pi = p_begin + tid;
     bool keep = false;
     O0Pair P{};
-    if (i < el_end) {
+    if (pi < p_end && pi < W.pair_capacity) {
+      const int64_t i = W.pairs[pi];
       const double beta = B.beta[i], len = B.length[i];
       const double ux = B.direction[3 * i], uy = B.direction[3 * i + 1], uz = B.direction[3 * i + 2];
       const double wx = ox - B.start[3 * i], wy = oy - B.start[3 * i + 1], wz = oz - B.start[3 * i + 2];
       const double z = wx * ux + wy * uy + wz * uz;
-      const bool sphere = radius > 0.0;
-      // interval_candidates with the sphere always in reach and the axis included
-      if (B.c0[i] != 0.0 && beta * pmax > 1.0 && !(z <= 0.0 && (!sphere || z <= -radius))) {
-        const double cx = wy * uz - wz * uy, cy = wz * ux - wx * uz, cz = wx * uy - wy * ux;
-        const double rho_c = sqrt(cx * cx + cy * cy + cz * cz);
-        const double rad = sphere ? radius : 0.0;
-        if (!(z <= 0.0 && rad == 0.0)) {
-          if (rho_c == 0.0) {
-            if (rad == 0.0) {
-              if (0.0 < z && z < len) flags |= LH_STATUS_ON_TRACK;
-            } else {
-              keep = true;
-            }
-          } else if (rad == 0.0) {
-            keep = false;  // a point receiver has no first-entry window: no light on this path
-          } else if (o0_cone_reaches(z, rho_c, len, beta, rad, pmin, pmax)) {
-            double a, b, c, d;
-            keep = o0_support(z, rho_c, len, beta, rad, a, b, c, d) && !(a > pmax || b <= pmin);
-          }
-        }
-      }
+      keep = true;
       if (keep) {
         // _surface_ballistic_rays.py:52-80: frame and support of the pair
         const double tx = wx - z * ux, ty = wy - z * uy, tz = wz - z * uz;
@@ -305,7 +437,7 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B) {
             P.side = e2x * lx + e2y * ly + e2z * lz;
             P.nmin = nmin; P.nmax = nmax; P.cut0 = cut0; P.cut1 = cut1;
             P.tau = (B.t1[i] - B.t0[i]) / len;
-            P.el = (int)(i - el_begin);
+            P.el = (int)i;
           }
         }
       }
@@ -318,7 +450,7 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B) {
   const int n_pairs = S.n_pairs;
   if (n_pairs == 0) {
     if (flags) atomicOr(reinterpret_cast<unsigned*>(B.status), flags);
-    return;
+    continue;
   }
 
   // ---- phase 1: (pair, panel, piece) work list
@@ -358,7 +490,6 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B) {
   const double origin = B.origins[(int64_t)ev * O.n_om + om];
   const double* edges = B.edges;
   const int n_edges = B.n_edges;
-  const int64_t el0 = el_begin;
   float alpha_abs = 0.0f;
   for (int k = 0; k < O.n_alpha; ++k) alpha_abs += fabsf(S.alpha[k]);
   alpha_abs = fmaxf(alpha_abs, 1.0f);
@@ -372,7 +503,7 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B) {
     const uint32_t code = combos[ci];
     const int p = code & 0xff, panel = (code >> 8) & 0xffff, piece = code >> 24;
     const O0Pair& P = S.pair[p];
-    const int64_t i = el0 + P.el;
+    const int64_t i = P.el;
     const double left = O.panel_edges[panel], width = O.panel_edges[panel + 1] - left;
     const double n0 = O.phase[panel], dn = O.phase[panel + 1] - n0;
     double cuts[4];
@@ -545,6 +676,7 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B) {
       if (sbins[k] != 0.0) atomicAdd(&out[k], sbins[k]);
   }
   if (flags) atomicOr(reinterpret_cast<unsigned*>(B.status), flags);
+  }  // chunks
 }
 
 size_t order0_shared_bytes(const lh_order0_optics& O, const lh_order0_batch& B) {
@@ -555,18 +687,52 @@ size_t order0_shared_bytes(const lh_order0_optics& O, const lh_order0_batch& B) 
   return bytes;
 }
 
+static size_t o0_align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Workspace: per (event, OM) counts, offsets, cursors; the pair list (at most
+// every (OM, element) combination) and the chunk list.
+static O0Work o0_layout(const lh_order0_optics& O, const lh_order0_batch& B, unsigned char* base,
+                        size_t* bytes) {
+  O0Work W{};
+  const int64_t keys = (int64_t)B.n_events * O.n_om;
+  W.pair_capacity = B.n_elements * O.n_om;
+  W.chunk_capacity = W.pair_capacity / kO0Chunk + keys;
+  size_t off = 0;
+  auto take = [&](size_t n) {
+    unsigned char* p = base ? base + off : nullptr;
+    off += o0_align(n);
+    return p;
+  };
+  W.counts = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * keys));
+  W.offsets = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * keys));
+  W.cursor = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * keys));
+  W.pairs = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * W.pair_capacity));
+  W.chunks = reinterpret_cast<int2*>(take(sizeof(int2) * W.chunk_capacity));
+  W.n_chunks = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 4));
+  if (bytes) *bytes = off;
+  return W;
+}
+
 int order0_launch(const lh_order0_optics& O, const lh_order0_batch& B, cudaStream_t s) {
   const size_t smem = order0_shared_bytes(O, B);
   if (smem > 200 * 1024) return LH_EUNSUPPORTED;
+  size_t need = 0;
+  O0Work W = o0_layout(O, B, static_cast<unsigned char*>(B.workspace), &need);
+  if (!B.workspace || B.workspace_bytes < need) return LH_ENOMEM;
   if (cudaFuncSetAttribute(order0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return LH_ECUDA;
-  cudaMemsetAsync(B.charge, 0, sizeof(double) * (size_t)B.n_events * O.n_om, s);
-  if (B.bins)
-    cudaMemsetAsync(B.bins, 0, sizeof(double) * (size_t)B.n_events * O.n_om * (B.n_edges - 1), s);
-  if (B.n_chunks == 0) return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
-  dim3 grid((unsigned)B.n_chunks, (unsigned)O.n_om);
-  order0_kernel<<<grid, kO0Threads, smem, s>>>(O, B);
+  const int64_t keys = (int64_t)B.n_events * O.n_om;
+  cudaMemsetAsync(B.charge, 0, sizeof(double) * (size_t)keys, s);
+  if (B.bins) cudaMemsetAsync(B.bins, 0, sizeof(double) * (size_t)keys * (B.n_edges - 1), s);
+  if (B.n_elements == 0) return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+  cudaMemsetAsync(W.counts, 0, sizeof(int32_t) * keys, s);
+  const int64_t items = B.n_elements * O.n_om;
+  const int blocks = (int)std::min<int64_t>((items + 255) / 256, 148 * 16);
+  order0_candidates_kernel<false><<<blocks, 256, 0, s>>>(O, B, W);
+  order0_scan_kernel<<<1, 1024, 0, s>>>((int32_t)keys, W);
+  order0_candidates_kernel<true><<<blocks, 256, 0, s>>>(O, B, W);
+  order0_kernel<<<148 * 8, kO0Threads, smem, s>>>(O, B, W);
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }
 
@@ -580,28 +746,25 @@ bool order0_valid(const lh_order0_optics* O, const lh_order0_batch* B) {
     return false;
   if (O->eff_cols != 4 && O->eff_cols != 6) return false;
   if (O->order < 1 || O->order > kO0MaxOrder || !O->gauss_x || !O->gauss_w) return false;
-  if (B->n_events < 1 || !B->element_offset || !B->chunk_offset || B->n_chunks < 0 ||
-      B->n_chunks > 0x7fffffff)
-    return false;
+  if (B->n_events < 1 || !B->element_offset || B->n_elements < 0) return false;
+  // pair indices, counts and offsets are 32-bit
+  if (B->n_elements * (int64_t)O->n_om >= (1ll << 31)) return false;
+  if ((int64_t)B->n_events * O->n_om >= (1ll << 31)) return false;
   if (B->n_edges < 2 || !B->edges || !B->origins || !B->charge || !B->status) return false;
-  if (B->n_chunks && (!B->start || !B->direction || !B->length || !B->c0 || !B->c2 || !B->beta ||
-                      !B->t0 || !B->t1))
+  if (B->n_elements && (!B->start || !B->direction || !B->length || !B->c0 || !B->c2 ||
+                        !B->beta || !B->t0 || !B->t1))
     return false;
   return true;
 }
 
 }  // namespace lh
 
-extern "C" size_t lh_order0_chunks(const int64_t* element_counts, int32_t n_events,
-                                   int64_t* chunk_offset_host) {
-  if (!element_counts || n_events < 1) return 0;
-  int64_t total = 0;
-  for (int e = 0; e < n_events; ++e) {
-    if (chunk_offset_host) chunk_offset_host[e] = total;
-    total += (element_counts[e] + lh::kO0Chunk - 1) / lh::kO0Chunk;
-  }
-  if (chunk_offset_host) chunk_offset_host[n_events] = total;
-  return (size_t)total;
+extern "C" size_t lh_order0_workspace_bytes(const lh_order0_optics* optics,
+                                            const lh_order0_batch* batch) {
+  if (!lh::order0_valid(optics, batch)) return 0;
+  size_t need = 0;
+  lh::o0_layout(*optics, *batch, nullptr, &need);
+  return need;
 }
 
 extern "C" int lh_order0(const lh_order0_optics* optics, const lh_order0_batch* batch,

@@ -75,6 +75,14 @@ class Order0Optics:
             t["efficiency"].data_ptr(), self.order, t["gauss_x"].data_ptr(),
             t["gauss_w"].data_ptr())
 
+    def workspace(self, nbytes):
+        """Device scratch of at least ``nbytes`` (kept and grown across calls)."""
+        import torch
+        if getattr(self, "_workspace", None) is None or self._workspace.numel() < nbytes:
+            self._workspace = torch.empty(max(int(nbytes), 1), dtype=torch.uint8,
+                                          device=self.device)
+        return self._workspace
+
     @classmethod
     def from_arrays(cls, d, **kw):
         """From a dict holding the optics fields and the detector arrays."""
@@ -104,9 +112,7 @@ class ElementBatch:
         self.counts = counts
         offsets = np.zeros(len(events) + 1, np.int64)
         offsets[1:] = np.cumsum(counts)
-        chunks = np.zeros(len(events) + 1, np.int64)
-        chunks[1:] = np.cumsum((counts + 31) // 32)
-        self.n_chunks = int(chunks[-1])
+        self.n_elements = int(offsets[-1])
         cols = {}
         for name in ELEMENT_FIELDS:
             parts = [np.asarray(_field(e, name), float) for e in events]
@@ -114,7 +120,6 @@ class ElementBatch:
         self._t = {k: torch.tensor(np.ascontiguousarray(v), dtype=torch.float64, device=device)
                    for k, v in cols.items()}
         self._t["offsets"] = torch.tensor(offsets, dtype=torch.int64, device=device)
-        self._t["chunks"] = torch.tensor(chunks, dtype=torch.int64, device=device)
 
     def pointers(self):
         t = self._t
@@ -153,14 +158,20 @@ def order0(optics: Order0Optics, events, origins=None, edges=None, *, stream=Non
             if want_bins else None)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
     t = batch._t
-    b = _lib.Order0Batch(E, t["offsets"].data_ptr(), t["chunks"].data_ptr(), batch.n_chunks,
-                         *batch.pointers(), origins_t.data_ptr(), len(edges_np),
-                         edges_t.data_ptr(), charge.data_ptr(),
-                         bins.data_ptr() if bins is not None else None, status.data_ptr())
+    b = _lib.Order0Batch(E, t["offsets"].data_ptr(), batch.n_elements, *batch.pointers(),
+                         origins_t.data_ptr(), len(edges_np), edges_t.data_ptr(),
+                         charge.data_ptr(), bins.data_ptr() if bins is not None else None,
+                         status.data_ptr(), None, 0)
+    lib = _lib.load()
+    need = int(lib.lh_order0_workspace_bytes(optics.struct, b))
+    if need == 0:
+        raise ValueError("order-0 problem rejected by the device library")
+    workspace = optics.workspace(need)
+    b.workspace, b.workspace_bytes = workspace.data_ptr(), workspace.numel()
     s = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
-    _lib.check(_lib.load().lh_order0(optics.struct, b, s), "lh_order0")
+    _lib.check(lib.lh_order0(optics.struct, b, s), "lh_order0")
     result = dict(charge=charge, bins=bins, status=status,
-                  _keep=(batch, origins_t, edges_t))
+                  _keep=(batch, origins_t, edges_t, workspace))
     if check:
         raise_status(int(status.item()))
     return result
