@@ -558,3 +558,31 @@ class ShowerTransport:
                         level[more] = 2
         stage("order1_fine")
         return charge, b1, level == 2, level, el, bins0.cpu().numpy()
+
+
+def main(argv=None):
+    """Run the first showers of the seeded config-2 stream: ``python -m lighthit_b200.shower``."""
+    import argparse
+    import json
+    import torch
+    from .workloads import gaussian_shower, shower_stream
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--tables", default="c2", choices=["c0", "c2"])
+    ap.add_argument("--showers", type=int, default=8)
+    ap.add_argument("--profile", action="store_true", help="per-stage device-synchronised times")
+    args = ap.parse_args(argv)
+    route = ShowerTransport(ShowerTables.synthetic(args.tables), profile=args.profile)
+    draws = shower_stream(args.showers, route.tables.positions.mean(axis=0))
+    for d in draws:
+        el = gaussian_shower(d["position_m"], d["direction"],
+                             charged_track_length_m=d["charged_track_length_m"],
+                             elements=d["elements"], seed=d["seed"])
+        r = route(el)
+        torch.cuda.synchronize()
+        print(json.dumps({"elements": d["elements"], "active": int(r.active.sum()),
+                          "charge_pe": float(r.charge_pe.sum()),
+                          "ms": 1e3 * r.metadata["elapsed_seconds"]}), flush=True)
+
+
+if __name__ == "__main__":
+    main()
