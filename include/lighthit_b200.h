@@ -322,9 +322,11 @@ int lh_order1_pencils(const lh_order1_config* config, const lh_order1_elements* 
                       void* workspace, size_t workspace_bytes, int32_t* status, void* stream);
 
 /* Stage B: charge[n_om] and bins[n_om][n_edges-1] of the OMs in work[n_work]
- * (others zero), clocks origins[n_om]. */
+ * (others zero), clocks origins[n_om]. n_pencils bounds the table rows used;
+ * n_pencils_device (optional, device) holds the stage-A count, read on the device. */
 int lh_order1_grouped(const lh_order1_config* config, const lh_order1_pencil_table* pencils,
-                      int32_t n_pencils, const int32_t* work, int32_t n_work,
+                      int32_t n_pencils, const int32_t* n_pencils_device,
+                      const int32_t* work, int32_t n_work,
                       const double* origins, double* charge, double* bins, void* workspace,
                       size_t workspace_bytes, int32_t* status, void* stream);
 

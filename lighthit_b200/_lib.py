@@ -154,7 +154,7 @@ SIGNATURES = {
     "lh_order1_pencils": (C.c_int, [C.POINTER(Order1Config), C.POINTER(Order1Elements),
                                     C.POINTER(Order1PencilTable), P, P, C.c_size_t, P, P]),
     "lh_order1_grouped": (C.c_int, [C.POINTER(Order1Config), C.POINTER(Order1PencilTable),
-                                    C.c_int32, P, C.c_int32, P, P, P, P, C.c_size_t, P, P]),
+                                    C.c_int32, P, P, C.c_int32, P, P, P, P, C.c_size_t, P, P]),
     "lh_om_geometry": (C.c_int, [C.POINTER(OmGeometry), P]),
     "lh_source_workspace_bytes": (C.c_size_t, [C.POINTER(SourceProblem)]),
     "lh_source_compile": (C.c_int, [C.POINTER(SourceProblem), C.POINTER(SourceOutput), P,

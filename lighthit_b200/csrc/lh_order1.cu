@@ -273,7 +273,8 @@ struct O1GroupShared {
 // One thread per (work OM, pencil): _grouped_pencils_order1_block's pencil
 // loop (_prompt_numba.py:1827-1921) with the generic moment layout.
 __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
-                                int32_t n_pencils, const int32_t* work, int32_t n_work,
+                                int32_t n_pencils_bound, const int32_t* n_pencils_device,
+                                const int32_t* work, int32_t n_work,
                                 const double* origins, long long* gkeys, double* grows,
                                 int32_t* gcount, int32_t* status) {
   __shared__ O1GroupShared S;
@@ -292,6 +293,9 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
   const double log_theta_ratio = log(1.0 + C.theta_ratio);
   const int theta_bins = C.theta_bins;
   const int64_t cap = C.group_capacity;
+  // the pencil count is read on the device when given (no host round trip)
+  const int32_t n_pencils =
+      n_pencils_device ? min(*n_pencils_device, n_pencils_bound) : n_pencils_bound;
   const int64_t total = (int64_t)n_work * n_pencils;
   for (int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; item < total;
        item += (int64_t)gridDim.x * blockDim.x) {
@@ -1040,7 +1044,8 @@ extern "C" int lh_order1_pencils(const lh_order1_config* C, const lh_order1_elem
 }
 
 extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_pencil_table* P,
-                                 int32_t n_pencils, const int32_t* work, int32_t n_work,
+                                 int32_t n_pencils, const int32_t* n_pencils_device,
+                                 const int32_t* work, int32_t n_work,
                                  const double* origins, double* charge, double* bins,
                                  void* workspace, size_t workspace_bytes, int32_t* status,
                                  void* stream) {
@@ -1062,7 +1067,8 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
   cudaMemsetAsync(W.batch_total, 0, sizeof(int32_t) * 4, s);
   cudaMemsetAsync(W.accum, 0, sizeof(double) * (size_t)n_work * C->n_bands * (3 + 4 * nb + 1), s);
   lh::o1_group_kernel<<<lh::grid_for((int64_t)n_work * n_pencils, 256), 256, 0, s>>>(
-      *C, *P, n_pencils, work, n_work, origins, W.gkeys, W.grows, W.gcount, status);
+      *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows, W.gcount,
+      status);
   const size_t sort_smem = sizeof(unsigned long long) * lh::kO1GroupSort;
   if (cudaFuncSetAttribute(lh::o1_batches_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sort_smem) != cudaSuccess)

@@ -254,7 +254,9 @@ def grouped(tables: Order1Tables, table: "PencilTable", work, origins, *, n_penc
     dev = tables.device
     n = tables.n_om
     work = np.asarray(work, np.int32)
-    n_p = min(int(table.count.item()) if n_pencils is None else int(n_pencils), table.capacity)
+    # the count stays on the device unless the caller passes it
+    n_p = table.capacity if n_pencils is None else min(int(n_pencils), table.capacity)
+    count_ptr = table.count.data_ptr() if n_pencils is None else None
     if len(work) and (work.min() < 0 or work.max() >= n):
         raise ValueError("work lists OMs outside the detector")
     if np.shape(origins) != (n,):
@@ -268,7 +270,7 @@ def grouped(tables: Order1Tables, table: "PencilTable", work, origins, *, n_penc
     ws = tables.workspace(0, len(work))
     st = status if status is not None else torch.zeros(1, dtype=torch.int32, device=dev)
     sp = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
-    _lib.check(_lib.load().lh_order1_grouped(tables.struct, table.struct, n_p,
+    _lib.check(_lib.load().lh_order1_grouped(tables.struct, table.struct, n_p, count_ptr,
                                              work_t.data_ptr(), len(work), origins_t.data_ptr(),
                                              charge.data_ptr(),
                                              bins.data_ptr() if bins is not None else None,

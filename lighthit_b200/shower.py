@@ -37,7 +37,7 @@ import numpy as np
 
 from . import _lib
 from .ge2 import AxialSources, Ge2Table
-from .order0 import Order0Optics, order0
+from .order0 import Order0Optics, order0, raise_status as raise_order0_status
 from .order1 import Order1Tables, PromptSettings, acceptance_monomials, grouped, pencils
 from .readout import DeviceReadout
 from .source import ShowerBasisSettings, SourceCompiler, axis_frame
@@ -164,6 +164,29 @@ class ShowerTables:
             raise ValueError("known synthetic tables: c0, c2")
         return cls(TABLES / f"route_{name}.npz", TABLES / folded[name], **kw)
 
+    def om_geometry_batch(self, prompt_elements, elements, group_index):
+        """Per shower: distances to the prompt elements and earliest arrivals (device)."""
+        import torch
+        dev = self.device
+        n = self.n_om
+        out = []
+        for events in (prompt_elements, elements):
+            offsets, cat = _concat_elements(events)
+            t = {k: torch.tensor(np.ascontiguousarray(v), dtype=torch.float64, device=dev)
+                 for k, v in cat.items()}
+            off = torch.tensor(offsets, dtype=torch.int64, device=dev)
+            res = torch.empty((len(events), n), dtype=torch.float64, device=dev)
+            want_distance = events is prompt_elements
+            g = _lib.OmGeometry(n, self._pos.data_ptr(), len(events), off.data_ptr(),
+                                t["start_m"].data_ptr(), t["direction"].data_ptr(),
+                                t["length_m"].data_ptr(), t["start_ns"].data_ptr(),
+                                float(group_index), res.data_ptr() if want_distance else None,
+                                None if want_distance else res.data_ptr())
+            sp = _lib.stream_ptr(torch.cuda.current_stream(dev))
+            _lib.check(_lib.load().lh_om_geometry(C.byref(g), sp), "lh_om_geometry")
+            out.append((res, t, off))
+        return out[0][0].cpu().numpy(), out[1][0].cpu().numpy()
+
     def attenuation(self, distance):
         radius, log_factor = self._attenuation
         return np.exp(np.interp(distance, radius, log_factor))
@@ -187,6 +210,14 @@ class ShowerTables:
         _lib.check(_lib.load().lh_om_geometry(C.byref(g), sp), "lh_om_geometry")
         return (dist.cpu().numpy() if dist is not None else None,
                 early.cpu().numpy() if early is not None else None)
+
+
+def _concat_elements(events):
+    offsets = np.zeros(len(events) + 1, np.int64)
+    offsets[1:] = np.cumsum([len(e["length_m"]) for e in events])
+    cat = {k: np.concatenate([np.asarray(e[k], float) for e in events])
+           for k in ("start_m", "direction", "length_m", "start_ns")}
+    return offsets, cat
 
 
 def elements_of(source):
@@ -225,9 +256,41 @@ class _Stages:
         self.last = now
 
 
+@dataclass
+class _Event:
+    """Per-shower state carried between the stages of a batch."""
+    el: dict
+    extra: np.ndarray
+    origins: np.ndarray | None = None
+    frame: tuple = None
+    reference: float = 0.0
+    points: list = None
+    channels: object = None
+    zero_ch: list = None
+    npts: np.ndarray = None
+    used: np.ndarray = None
+    tail: np.ndarray = None
+    reach: np.ndarray = None
+    predicted: np.ndarray = None
+    local_origin: bool = False
+    prompt_el: dict = None
+    inside: np.ndarray = None
+    work: np.ndarray = None
+    charge: np.ndarray = None
+    level1: np.ndarray = None
+    bins1: np.ndarray = None
+    fine: np.ndarray = None
+    cone_cos: np.ndarray = None
+    table: object = None
+    pending: dict = field(default_factory=dict)
+
+
 class ShowerTransport:
     """``ShowerTransport(kernel, data)(source, ...)`` on the device route.
 
+    ``batch(sources)`` runs many showers stage by stage: every stage launches
+    its kernels for all showers back to back on the current stream and the
+    host reads the device once per stage, not once per shower.
     ``profile=True`` synchronises the device between stages so that
     ``metadata['timings']`` attributes the GPU time to each stage.
     """
@@ -238,254 +301,383 @@ class ShowerTransport:
         self.config = config or tables.settings
         self.profile = profile
 
-    def _apply(self, points, channels, reference, frame, oms, *, zero_frequency):
-        """``apply_folded`` (``shower/ge2.py:99-119``) for the OMs ``oms``: (frequency, OM)."""
+    # -- order >=2 helpers ----------------------------------------------------
+    def _apply_device(self, points, channels, reference, frame, oms, *, zero_frequency):
+        """``apply_folded`` (``shower/ge2.py:99-119``) for the OMs ``oms``: device (OM, W)."""
+        import torch
         T = self.tables
-        W = 1 if zero_frequency else len(T.omega)
-        if not len(oms):
-            return np.zeros((W, 0), complex)
         centre, axis, first, second = frame
         area = T.areas[oms]
         same = all(len(p) == len(points[0]) and np.array_equal(p, points[0]) for p in points[1:])
         if same:
             src = AxialSources(points[0], channels, np.full(len(points), reference),
                                (centre, first, second, axis), T.source_degree, T.azimuthal_degree)
-            return T.ge2.apply(src, T.positions[oms], T.looks[oms], area, T.radial,
-                               zero_frequency=zero_frequency)
-        total = 0
+            return T.ge2.apply_device(src, T.positions[oms], T.looks[oms], area, T.radial,
+                                      zero_frequency=zero_frequency)
+        total = None
         for b in range(len(points)):
             src = AxialSources(points[b], channels[b][None], np.array([reference]),
                                (centre, first, second, axis), T.source_degree, T.azimuthal_degree)
-            total = total + T.ge2.band(b).apply(src, T.positions[oms], T.looks[oms], area,
-                                                T.radial, zero_frequency=zero_frequency)
+            part = T.ge2.band(b).apply_device(src, T.positions[oms], T.looks[oms], area,
+                                              T.radial, zero_frequency=zero_frequency)
+            total = part if total is None else total + part
         return total
 
     def __call__(self, source, *, time_origin_ns=None, selection_extra_charge=None,
                  receivers=None):
-        import torch
         if receivers is not None:
             raise NotImplementedError("receiver subsets: build ShowerTables for those OMs")
+        return self.batch([source], time_origin_ns=None if time_origin_ns is None
+                          else [time_origin_ns],
+                          selection_extra_charge=None if selection_extra_charge is None
+                          else [selection_extra_charge])[0]
+
+    def batch(self, sources, *, time_origin_ns=None, selection_extra_charge=None):
+        """Responses of several showers (``transport_shower`` per source)."""
+        import torch
         began = perf_counter()
         stage = _Stages(self.profile)
         T, cfg = self.tables, self.config
         n = T.n_om
         omega, edges, threshold = T.omega, T.edges, T.threshold
         low, high = T.radial
-        el = elements_of(source)
-        max_phase = float(np.max(T.phase))
-        valid = el["beta"] * max_phase > 1
-        if not np.any(valid):
-            raise ValueError("source is below Cherenkov threshold over the wavelength range")
-        if not np.all(valid):
-            el = _subset(el, valid)
-        extra = (np.zeros(n) if selection_extra_charge is None
-                 else np.maximum(np.asarray(selection_extra_charge, float), 0.0))
-        if extra.shape != (n,) or not np.isfinite(extra).all():
-            raise ValueError("selection_extra_charge must hold one finite value per OM")
-        # delay groups (shower/ge2.py:122-147): the device route handles prompt steps
-        first = int(np.argmin(el["start_ns"]))
-        distance0 = np.linalg.norm(el["start_m"] - el["start_m"][first], axis=1)
-        delay = el["start_ns"] - el["start_ns"][first] - distance0 / C_M_PER_NS
-        if np.any(delay > cfg.prompt_delay_ns):
-            raise NotImplementedError("delayed light groups (steps more than prompt_delay_ns "
-                                      "behind the light front) are not on the device route")
-        stage("setup")
-        # ---- order >=2 source on the node bands (shower/api.py:373-402)
-        frame = axis_frame(el["start_m"], el["direction"], el["length_m"], el["coefficient0"])
-        pts_d, ch_d, npts_d, reference, frame = T.source.compile(el, frame)
-        npts = npts_d.cpu().numpy()
-        centre, axis, e1, e2 = (np.asarray(v, float) for v in frame)
-        pts_host = pts_d.cpu().numpy()
+        dev = T.device
+        safety = float(cfg.predictor_safety)
         nb_bands = len(T.fold_bands)
-        points = []
-        for b in range(nb_bands):
-            p = pts_host[b, :npts[b]]
-            points.append(centre + p[:, :1] * axis + p[:, 1:2] * e1 + p[:, 2:3] * e2)
-        if np.all(npts == npts[0]):
-            channels = ch_d[:, :int(npts[0])]
-        else:
-            channels = [ch_d[b, :int(npts[b])] for b in range(nb_bands)]
-        zero_ch = [ch_d[b, :int(npts[b]), :, 0].cpu().numpy() for b in range(nb_bands)]
+        max_phase = float(np.max(T.phase))
+        fastest = float(np.min(T.group))
+        events = []
+        # ---- per shower: elements, delay groups, frame (host)
+        for k, source in enumerate(sources):
+            el = elements_of(source)
+            valid = el["beta"] * max_phase > 1
+            if not np.any(valid):
+                raise ValueError("source is below Cherenkov threshold over the wavelength range")
+            if not np.all(valid):
+                el = _subset(el, valid)
+            given = None if selection_extra_charge is None else selection_extra_charge[k]
+            extra = np.zeros(n) if given is None else np.maximum(np.asarray(given, float), 0.0)
+            if extra.shape != (n,) or not np.isfinite(extra).all():
+                raise ValueError("selection_extra_charge must hold one finite value per OM")
+            first = int(np.argmin(el["start_ns"]))
+            distance0 = np.linalg.norm(el["start_m"] - el["start_m"][first], axis=1)
+            delay = el["start_ns"] - el["start_ns"][first] - distance0 / C_M_PER_NS
+            if np.any(delay > cfg.prompt_delay_ns):
+                raise NotImplementedError("delayed light groups (steps more than prompt_delay_ns "
+                                          "behind the light front) are not on the device route")
+            ev = _Event(el, extra)
+            ev.frame = axis_frame(el["start_m"], el["direction"], el["length_m"],
+                                  el["coefficient0"])
+            events.append(ev)
+        stage("setup")
+        # ---- order >=2 sources on the node bands (device, all showers)
+        src_status = torch.zeros(1, dtype=torch.int32, device=dev)
+        compiled = [T.source.compile(ev.el, ev.frame, status=src_status) for ev in events]
+        npts_all = torch.stack([c[2] for c in compiled]).cpu().numpy()
+        if int(src_status.item()) & _lib.LH_STATUS_OVERFLOW:
+            raise ValueError("element nodes fall outside the source lattice")
+        host_pts = [c[0].cpu().numpy() for c in compiled]
+        for ev, c, pts, npts in zip(events, compiled, host_pts, npts_all):
+            _, ch_d, _, ev.reference, ev.frame = c
+            ev.npts = npts
+            centre, axis, e1, e2 = (np.asarray(v, float) for v in ev.frame)
+            ev.points = [centre + p[:npts[b], :1] * axis + p[:npts[b], 1:2] * e1
+                         + p[:npts[b], 2:3] * e2 for b, p in enumerate(pts)]
+            ev.channels = (ch_d[:, :int(npts[0])] if np.all(npts == npts[0])
+                           else [ch_d[b, :int(npts[b])] for b in range(nb_bands)])
+            ev.zero_ch = [ch_d[b, :int(npts[b]), :, 0] for b in range(nb_bands)]
+        zero_host = torch.cat([z for ev in events for z in ev.zero_ch]).cpu().numpy()
+        pos = 0
+        for ev in events:
+            parts = []
+            for b in range(nb_bands):
+                parts.append(zero_host[pos:pos + int(ev.npts[b])])
+                pos += int(ev.npts[b])
+            ev.zero_ch = parts
         stage("source_compile")
         # ---- radial windows (shower/api.py:322-340, shower_basis.py:408-439)
-        used = np.zeros(n, np.int64)
-        near = np.zeros(n, bool)
-        tail = np.zeros(n)
         weight_ratio = float(np.sum(T.fold_scale) / np.sum(T.fold_scale[T.fold_bands]))
-        radius = None
-        for b, band in enumerate(T.fold_bands):
-            photons = np.sqrt(4 * np.pi) * np.abs(zero_ch[b][:, 0]) / T.efficiency[band]
-            if radius is None or not np.array_equal(points[b], points[b - 1]):
-                radius = np.sqrt(((points[b][None] - T.positions[:, None]) ** 2).sum(axis=2))
-                n_near = np.count_nonzero(radius < low, axis=1)
-                om, pt = np.nonzero(radius > high)
-                n_far = np.bincount(om, minlength=n)
-                far_factor = T.attenuation(radius[om, pt]) / (4 * np.pi * radius[om, pt] ** 2)
-            used = np.maximum(used, len(points[b]) - n_near - n_far)
-            near |= n_near > 0
-            tail += weight_ratio * (10 * T.areas * T.peak_acceptance * T.efficiency[band]
-                                    * np.bincount(om, weights=photons[pt] * far_factor,
-                                                  minlength=n))
-        if np.any(near):
-            raise NotImplementedError("basis points inside the table's inner radius need the "
-                                      "near-field clamp (near_field.py), not on the device route")
-        reach = np.flatnonzero(used > 0)
+        for ev in events:
+            used = np.zeros(n, np.int64)
+            near = np.zeros(n, bool)
+            tail = np.zeros(n)
+            radius = None
+            for b, band in enumerate(T.fold_bands):
+                photons = np.sqrt(4 * np.pi) * np.abs(ev.zero_ch[b][:, 0]) / T.efficiency[band]
+                if radius is None or not np.array_equal(ev.points[b], ev.points[b - 1]):
+                    radius = np.sqrt(((ev.points[b][None] - T.positions[:, None]) ** 2).sum(axis=2))
+                    n_near = np.count_nonzero(radius < low, axis=1)
+                    om, pt = np.nonzero(radius > high)
+                    n_far = np.bincount(om, minlength=n)
+                    far_factor = T.attenuation(radius[om, pt]) / (4 * np.pi * radius[om, pt] ** 2)
+                used = np.maximum(used, len(ev.points[b]) - n_near - n_far)
+                near |= n_near > 0
+                tail += weight_ratio * (10 * T.areas * T.peak_acceptance * T.efficiency[band]
+                                        * np.bincount(om, weights=photons[pt] * far_factor,
+                                                      minlength=n))
+            if np.any(near):
+                raise NotImplementedError("basis points inside the table's inner radius need the "
+                                          "near-field clamp (near_field.py), not on the device "
+                                          "route")
+            ev.used, ev.tail, ev.reach = used, tail, np.flatnonzero(used > 0)
         stage("radial_window")
-        # ---- predictor (shower/ge2.py:70-96) and its zero-frequency charge
-        predicted = np.zeros(n)
-        late_charge = np.zeros(n)
-        if len(reach):
+        # ---- predictor (shower/ge2.py:70-96) and its zero-frequency charge (device)
+        for ev in events:
+            ev.predicted = np.zeros(n)
+            if not len(ev.reach):
+                continue
+            centre, axis, e1, e2 = (np.asarray(v, float) for v in ev.frame)
             c_points, c_channels = [], []
             for b in range(nb_bands):
-                rel = points[b] - centre
+                rel = ev.points[b] - centre
                 coords = np.column_stack((rel @ axis, rel @ e1, rel @ e2))
                 keys = np.floor(coords / float(cfg.predictor_cell_m)).astype(np.int64)
-                _, inverse = np.unique(keys, axis=0, return_inverse=True)
-                inverse = np.asarray(inverse).ravel()
+                keys -= keys.min(axis=0)
+                span = keys.max(axis=0) + 1
+                flat = (keys[:, 0] * span[1] + keys[:, 1]) * span[2] + keys[:, 2]
+                _, inverse = np.unique(flat, return_inverse=True)
                 groups = int(inverse.max()) + 1
-                wgt = np.abs(zero_ch[b][:, 0])
+                wgt = np.abs(ev.zero_ch[b][:, 0])
                 total = np.bincount(inverse, weights=wgt, minlength=groups)
                 count = np.bincount(inverse, minlength=groups)
-                share = np.where(total[inverse] > 0, wgt / np.where(total > 0, total, 1.0)[inverse],
+                share = np.where(total[inverse] > 0,
+                                 wgt / np.where(total > 0, total, 1.0)[inverse],
                                  1.0 / count[inverse])
                 centroid = np.stack([np.bincount(inverse, weights=share * coords[:, k],
                                                  minlength=groups) for k in range(3)], axis=1)
-                summed = np.zeros((groups, zero_ch[b].shape[1]), complex)
-                np.add.at(summed, inverse, zero_ch[b])
+                summed = np.zeros((groups, ev.zero_ch[b].shape[1]), complex)
+                np.add.at(summed, inverse, ev.zero_ch[b])
                 c_points.append(centre + centroid[:, :1] * axis + centroid[:, 1:2] * e1
                                 + centroid[:, 2:3] * e2)
                 c_channels.append(summed[:, :, None])
-            if all(len(p) == len(c_points[0]) for p in c_points[1:]):
-                c_ch = np.stack(c_channels)
-            else:
-                c_ch = c_channels
-            predicted[reach] = self._apply(c_points, c_ch, reference, frame, reach,
-                                           zero_frequency=True)[0].real
-        stage("predictor")
-        # ---- clocks (shower/api.py:455-477)
-        fastest = float(np.min(T.group))
+            c_ch = (np.stack(c_channels) if all(len(p) == len(c_points[0]) for p in c_points[1:])
+                    else c_channels)
+            ev.pending["predicted"] = self._apply_device(c_points, c_ch, ev.reference, ev.frame,
+                                                         ev.reach, zero_frequency=True)
+        # ---- clocks (shower/api.py:455-477) and module selection distances (device)
         time_width = float(np.ptp(edges))
-        span = float(np.max(el["end_ns"]) - np.min(el["start_ns"]))
-        mid = el["start_m"] + 0.5 * el["length_m"][:, None] * el["direction"]
-        extent = float(np.linalg.norm(np.ptp(mid, axis=0)))
-        local_origin = extent > high or span > 0.5 * time_width
-        if time_origin_ns is not None:
-            origins = np.asarray(time_origin_ns, float)
-            if origins.shape != (n,) or not np.isfinite(origins).all():
-                raise ValueError("time_origin_ns must hold one finite origin per OM")
-        elif local_origin:
-            origins = T.om_geometry(el, fastest, want_distance=False, want_earliest=True)[1]
-        else:
-            origins = (float(el["start_ns"][first])
-                       + np.linalg.norm(T.positions - el["start_m"][first], axis=1)
-                       / (C_M_PER_NS / fastest))
-        safety = float(cfg.predictor_safety)
-        prompt_extra = safety * np.abs(predicted) + np.abs(late_charge) + extra
-        stage("clock")
-        charge01, b1, computed, level1, prompt_el, bins0 = self._prompt(el, origins, prompt_extra,
-                                                                        stage)
-        # ---- exact zero-frequency >=2 where the decision needs it (shower/api.py:488-525)
-        charge = np.zeros((n, 3))
-        charge[:, :2] = charge01
-        prompt_charge = charge[:, :2].sum(axis=1)
-        computable = (used > 0) | (prompt_charge > 0)
-        candidate = (used > 0) & (prompt_charge + safety * np.abs(predicted) + late_charge + extra
-                                  >= threshold)
-        if threshold == 0:
-            candidate = used > 0
-        zero_only = ([c[:, :, :1] for c in channels] if isinstance(channels, list)
-                     else channels[:, :, :, :1])
-
-        def exact(mask):
-            ids = np.flatnonzero(mask)
-            values = np.zeros(n)
-            if len(ids):
-                values[ids] = self._apply(points, zero_only, reference, frame, ids,
-                                          zero_frequency=True)[0].real
-            return values
-
-        level = np.where(used > 0, 1, 0).astype(np.int8)
-        exact_charge = exact(candidate)
-        ratio = np.abs(exact_charge[candidate]) / np.maximum(np.abs(predicted[candidate]), 1e-300)
-        fallback = bool(np.any(np.abs(exact_charge[candidate])
-                               > safety * np.abs(predicted[candidate])))
-        if fallback:
-            candidate = used > 0
-            exact_charge = exact(candidate)
-        charge[:, 2] = predicted + late_charge
-        charge[candidate, 2] = exact_charge[candidate] + late_charge[candidate]
-        level[candidate] = 2
-        active = computable & (charge.sum(axis=1) + extra >= threshold)
-        if threshold == 0:
-            active = computable
-        if np.any(active & (level == 1)):
-            raise RuntimeError("an OM was activated by a predicted >=2 charge")
-        stage("ge2_exact_zero")
-        # ---- full frequencies for the active OMs, then the readout
-        spectrum = np.zeros((len(omega), n), complex)
-        work = np.flatnonzero(active & (used > 0))
-        if len(work):
-            spectrum[:, work] = self._apply(points, channels, reference, frame, work,
-                                            zero_frequency=False)
-        stage("ge2_full")
-        spectrum[0] = charge[:, 2] - late_charge
-        components = np.zeros((n, len(edges) - 1, 3))
-        if np.any(active):
-            missing = np.flatnonzero(active & ~computed)
-            if len(missing):
-                # the reference recomputes the prompt without its screen (shower/api.py:592-599)
-                q1m, b1m = self._fine_order1(prompt_el, origins, missing)
-                charge[missing, 1] = q1m
-                b1[missing] = b1m
-            ids = np.flatnonzero(active)
-            # order-0 bins of the active OMs (PreparedBallistic.bins, prompt.py:896-903);
-            # their charge is the binned integral's, as in the reference
-            components[ids, :, 0] = bins0[ids]
-            components[ids, :, 1] = b1[ids]
-            stage("order0_bins")
-            rel = spectrum[:, ids] * np.exp(-1j * omega[:, None] * origins[None, ids])
-            rel_t = torch.tensor(np.ascontiguousarray(rel.T).astype(np.complex64),
-                                 device=T.device)
-            bins2, _ = T.readout.bins(rel_t, mode=cfg.readout_mode)
-            components[ids, :, 2] = bins2.cpu().numpy().astype(float)
-        stage("readout")
-        metadata = {
-            "route": "lighthit_b200.shower", "ge2_charge_level": level.tolist(),
-            "ge2_predictor": {"cell_m": float(cfg.predictor_cell_m), "safety": safety,
-                              "candidates": int(candidate.sum()), "reachable": int(len(reach)),
-                              "fallback_to_exact": fallback,
-                              "exact_over_prediction_max": float(ratio.max(initial=0.0))},
-            "prompt_order1_level": level1.tolist(), "radial_window_m": [low, high],
-            "radial_tail_estimate_max_pe": float(tail.max(initial=0.0)),
-            "time_origin": ("supplied event clock" if time_origin_ns is not None else
-                            "earliest local segment and fastest group flight" if local_origin
-                            else "earliest element start and fastest group flight"),
-            "active_modules": int(active.sum()), "threshold_pe": threshold,
-            "ge2_points": [int(v) for v in npts], "source_elements": len(el["beta"]),
-            "elapsed_seconds": perf_counter() - began, "timings": stage.times}
-        return HybridTransportResponse(None, omega.copy(), edges.copy(), spectrum, components,
-                                       charge, origins, active, "shower", metadata)
-
-    def _fine_order1(self, el, origins, ids):
-        """Full-resolution order 1 (charge, bins) of the OMs ``ids``."""
-        T = self.tables
+        for k, ev in enumerate(events):
+            el = ev.el
+            span = float(np.max(el["end_ns"]) - np.min(el["start_ns"]))
+            mid = el["start_m"] + 0.5 * el["length_m"][:, None] * el["direction"]
+            extent = float(np.linalg.norm(np.ptp(mid, axis=0)))
+            ev.local_origin = extent > high or span > 0.5 * time_width
+            given = None if time_origin_ns is None else time_origin_ns[k]
+            if given is not None:
+                ev.origins = np.asarray(given, float)
+                if ev.origins.shape != (n,) or not np.isfinite(ev.origins).all():
+                    raise ValueError("time_origin_ns must hold one finite origin per OM")
+            elif not ev.local_origin:
+                first = int(np.argmin(el["start_ns"]))
+                ev.origins = (float(el["start_ns"][first])
+                              + np.linalg.norm(T.positions - el["start_m"][first], axis=1)
+                              / (C_M_PER_NS / fastest))
+            pel = el
+            pvalid = el["beta"] * T.threshold_phase > 1
+            if not np.any(pvalid):
+                raise ValueError("source is below Cherenkov threshold over the wavelength range")
+            if not np.all(pvalid):
+                pel = _subset(el, pvalid)
+            ev.prompt_el = pel
+        dist, early = T.om_geometry_batch([ev.prompt_el for ev in events],
+                                          [ev.el for ev in events], fastest)
+        for k, ev in enumerate(events):
+            if ev.origins is None:
+                ev.origins = early[k]
+            if "predicted" in ev.pending:
+                ev.predicted[ev.reach] = ev.pending.pop("predicted").cpu().numpy()[:, 0].real
+        stage("predictor_clock")
+        # ---- prompt orders 0 and 1 (transport_prompt, prompt.py:500-947)
+        for k, ev in enumerate(events):
+            self._prompt_selection(ev, dist[k], safety)
+        prompt_events = [ev for ev in events if len(ev.work)]
+        if prompt_events:
+            origins = np.stack([ev.origins for ev in prompt_events])
+            out0 = order0(T.order0, [ev.prompt_el for ev in prompt_events], origins, edges,
+                          check=False)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
         cone = float(np.sum(T.prompt["s0w"] * T.phase) / np.sum(T.prompt["s0w"]))
-        table = pencils(T.order1, el, 1.0 / (el["beta"] * cone))
-        q1, bins1 = grouped(T.order1, table, ids, origins)
-        return q1.cpu().numpy()[ids], bins1.cpu().numpy()[ids]
+        for ev in prompt_events:
+            if not np.all(ev.prompt_el["beta"][:, None] * T.phase[None, :] > 1):
+                raise NotImplementedError("elements above threshold in only some bands need the "
+                                          "per-band order-1 units")
+            ev.cone_cos = 1.0 / (ev.prompt_el["beta"] * cone)
+            if cfg.screen and threshold > 0:
+                coarse = pencils(T.order1_screen, ev.prompt_el, ev.cone_cos, status=status)
+                ev.pending["coarse"] = grouped(T.order1_screen, coarse, ev.work, ev.origins,
+                                               status=status)[0]
+        if prompt_events:
+            raise_order0_status(int(out0["status"].item()))
+            q0_all = out0["charge"].cpu().numpy()
+            bins0_all = out0["bins"]
+            for k, ev in enumerate(prompt_events):
+                ev.charge[ev.work, 0] = q0_all[k][ev.work]
+                ev.pending["bins0"] = bins0_all[k]
+        stage("order0_screen")
+        for ev in prompt_events:
+            ev.fine = ev.work
+            if "coarse" in ev.pending:
+                coarse = ev.pending.pop("coarse").cpu().numpy()
+                ev.charge[ev.work, 1] = coarse[ev.work]
+                ev.level1[ev.work] = 1
+                ev.pending["coarse_host"] = coarse
+                ev.fine = ev.work[(ev.charge[ev.work, 0] + ev.extra_prompt[ev.work]
+                                   + cfg.screen_margin * np.maximum(coarse[ev.work], 0.0))
+                                  >= threshold]
+            if len(ev.fine):
+                ev.table = pencils(T.order1, ev.prompt_el, ev.cone_cos, status=status)
+                ev.pending["fine"] = grouped(T.order1, ev.table, ev.fine, ev.origins,
+                                             status=status)
+        for ev in prompt_events:
+            if "fine" not in ev.pending:
+                continue
+            q1, b1 = ev.pending.pop("fine")
+            q1, b1 = q1.cpu().numpy(), b1.cpu().numpy()
+            ev.charge[ev.fine, 1] = q1[ev.fine]
+            ev.bins1[ev.fine] = b1[ev.fine]
+            ev.level1[ev.fine] = 2
+            coarse = ev.pending.pop("coarse_host", None)
+            if coarse is not None:  # widening (prompt.py:776-805)
+                worst = float(np.min(coarse[ev.fine] / np.maximum(q1[ev.fine], 1e-300)))
+                if worst * cfg.screen_margin < 1.0:
+                    wider = 1.5 / max(worst, 1e-3)
+                    more = ev.work[(ev.level1[ev.work] == 1)
+                                   & (ev.charge[ev.work, 0] + ev.extra_prompt[ev.work] + wider
+                                      * np.maximum(coarse[ev.work], 0.0) >= threshold)]
+                    if len(more):
+                        q1m, b1m = grouped(T.order1, ev.table, more, ev.origins, status=status)
+                        ev.charge[more, 1] = q1m.cpu().numpy()[more]
+                        ev.bins1[more] = b1m.cpu().numpy()[more]
+                        ev.level1[more] = 2
+        if int(status.item()) & _lib.LH_STATUS_OVERFLOW:
+            raise MemoryError("order-1 tables overflowed their device capacity")
+        stage("order1")
+        # ---- exact zero-frequency >=2 where the decision needs it (shower/api.py:488-525)
+        for ev in events:
+            ev.pending["ge2"] = {}
+            prompt_charge = ev.charge.sum(axis=1)
+            ev.computable = (ev.used > 0) | (prompt_charge > 0)
+            cand = (ev.used > 0) & (prompt_charge + safety * np.abs(ev.predicted) + ev.extra
+                                    >= threshold)
+            if threshold == 0:
+                cand = ev.used > 0
+            ev.candidate = cand
+            ids = np.flatnonzero(cand)
+            if len(ids):
+                ev.pending["exact"] = (ids, self._apply_device(
+                    ev.points, self._zero_only(ev.channels), ev.reference, ev.frame, ids,
+                    zero_frequency=True))
+        for ev in events:
+            exact = np.zeros(n)
+            if "exact" in ev.pending:
+                ids, values = ev.pending.pop("exact")
+                exact[ids] = values.cpu().numpy()[:, 0].real
+            cand = ev.candidate
+            ratio = np.abs(exact[cand]) / np.maximum(np.abs(ev.predicted[cand]), 1e-300)
+            fallback = bool(np.any(np.abs(exact[cand]) > safety * np.abs(ev.predicted[cand])))
+            if fallback:  # the prediction failed its own margin: every reachable OM exact
+                cand = ev.used > 0
+                ids = np.flatnonzero(cand)
+                exact = np.zeros(n)
+                if len(ids):
+                    exact[ids] = self._apply_device(ev.points, self._zero_only(ev.channels),
+                                                    ev.reference, ev.frame, ids,
+                                                    zero_frequency=True).cpu().numpy()[:, 0].real
+            ev.fallback, ev.ratio, ev.candidate = fallback, ratio, cand
+            charge2 = ev.predicted.copy()
+            charge2[cand] = exact[cand]
+            ev.charge = np.column_stack((ev.charge, charge2))
+            level = np.where(ev.used > 0, 1, 0).astype(np.int8)
+            level[cand] = 2
+            ev.level2 = level
+            active = ev.computable & (ev.charge.sum(axis=1) + ev.extra >= threshold)
+            if threshold == 0:
+                active = ev.computable
+            if np.any(active & (level == 1)):
+                raise RuntimeError("an OM was activated by a predicted >=2 charge")
+            ev.active = active
+        stage("ge2_exact_zero")
+        # ---- full frequencies for the active OMs, the prompt bins they lack, the readout
+        rows, row_ev = [], []
+        for k, ev in enumerate(events):
+            ev.spectrum = np.zeros((len(omega), n), complex)
+            ids = np.flatnonzero(ev.active)
+            missing = np.flatnonzero(ev.active & (ev.level1 < 2))
+            if len(missing):  # the reference reruns the prompt without its screen
+                table = ev.table if ev.table is not None else pencils(
+                    T.order1, ev.prompt_el, 1.0 / (ev.prompt_el["beta"] * cone), status=status)
+                q1m, b1m = grouped(T.order1, table, missing, ev.origins, status=status)
+                ev.charge[missing, 1] = q1m.cpu().numpy()[missing]
+                ev.bins1[missing] = b1m.cpu().numpy()[missing]
+            work = np.flatnonzero(ev.active & (ev.used > 0))
+            if len(work):
+                spec = self._apply_device(ev.points, ev.channels, ev.reference, ev.frame, work,
+                                          zero_frequency=False)
+                ev.pending["spec"] = (work, spec)
+                phase = torch.tensor(np.exp(-1j * np.outer(ev.origins[work], omega)),
+                                     dtype=torch.complex128, device=dev)
+                rel = spec * phase
+                # the stored zero frequency is the exact >=2 charge (shower/api.py:584)
+                rel[:, 0] = torch.tensor(ev.charge[work, 2], dtype=torch.complex128, device=dev)
+                rel = rel.to(torch.complex64)
+                rows.append(rel)
+                row_ev.append((k, work))
+        if rows:
+            bins2, _ = T.readout.bins(torch.cat(rows), mode=cfg.readout_mode)
+            bins2 = bins2.cpu().numpy().astype(float)
+        responses = []
+        row = 0
+        row_map = {k: work for k, work in row_ev}
+        for k, ev in enumerate(events):
+            if "spec" in ev.pending:
+                work, spec = ev.pending.pop("spec")
+                ev.spectrum[:, work] = spec.cpu().numpy().T
+            ev.spectrum[0] = ev.charge[:, 2]
+            components = np.zeros((n, len(edges) - 1, 3))
+            ids = np.flatnonzero(ev.active)
+            if len(ids):
+                if not np.all(ev.inside[ids]):
+                    raise ValueError("prompt did not compute every active OM")
+                components[ids, :, 0] = ev.pending["bins0"].cpu().numpy()[ids]
+                components[ids, :, 1] = ev.bins1[ids]
+                if k in row_map:
+                    work = row_map[k]
+                    components[work, :, 2] = bins2[row:row + len(work)]
+                    row += len(work)
+            metadata = {
+                "route": "lighthit_b200.shower", "ge2_charge_level": ev.level2.tolist(),
+                "ge2_predictor": {"cell_m": float(cfg.predictor_cell_m), "safety": safety,
+                                  "candidates": int(ev.candidate.sum()),
+                                  "reachable": int(len(ev.reach)),
+                                  "fallback_to_exact": ev.fallback,
+                                  "exact_over_prediction_max": float(ev.ratio.max(initial=0.0))},
+                "prompt_order1_level": ev.level1.tolist(), "radial_window_m": [low, high],
+                "radial_tail_estimate_max_pe": float(ev.tail.max(initial=0.0)),
+                "time_origin": ("supplied event clock" if time_origin_ns is not None else
+                                "earliest local segment and fastest group flight"
+                                if ev.local_origin
+                                else "earliest element start and fastest group flight"),
+                "active_modules": int(ev.active.sum()), "threshold_pe": threshold,
+                "ge2_points": [int(v) for v in ev.npts], "source_elements": len(ev.el["beta"]),
+                "elapsed_seconds": (perf_counter() - began) / len(events),
+                "batch_size": len(events), "timings": stage.times}
+            responses.append(HybridTransportResponse(None, omega.copy(), edges.copy(),
+                                                     ev.spectrum, components, ev.charge,
+                                                     ev.origins, ev.active, "shower", metadata))
+        stage("ge2_full_readout")
+        return responses
 
-    def _prompt(self, el, origins, extra, stage):
-        """Orders 0 and 1 charges (``transport_prompt``, ``prompt.py:500-947``)."""
+    @staticmethod
+    def _zero_only(channels):
+        return ([c[:, :, :1] for c in channels] if isinstance(channels, list)
+                else channels[:, :, :, :1])
+
+    def _prompt_selection(self, ev, distance, safety):
+        """Module selection of ``transport_prompt`` (``prompt.py:603-631``)."""
         T, cfg = self.tables, self.config
         n = T.n_om
-        edges, threshold = T.edges, T.threshold
-        valid = el["beta"] * T.threshold_phase > 1
-        if not np.any(valid):
-            raise ValueError("source is below Cherenkov threshold over the wavelength range")
-        if not np.all(valid):
-            el = _subset(el, valid)
-        fastest = float(np.min(T.group))
-        distance, _ = T.om_geometry(el, fastest)
+        threshold = T.threshold
+        el = ev.prompt_el
         max_distance = T.radial[1]
         inside = distance <= max_distance
         s0 = 1.0 / T.wavelengths ** 2
@@ -503,61 +695,13 @@ class ShowerTransport:
         if np.any(too_close):
             raise ValueError(f"{int(too_close.sum())} OMs are closer than min_distance_m="
                              f"{cfg.min_distance_m:g} m to the source")
-        work = np.flatnonzero(inside)
-        stage("prompt_selection")
-        charge = np.zeros((n, 2))
-        level = np.zeros(n, np.int8)
-        if not len(work):
-            empty = np.zeros((n, len(edges) - 1))
-            return charge, empty, inside, level, el, empty
-        # one order-0 pass gives the charge of every OM and the bins (PreparedBallistic.charge
-        # and .bins integrate the same light; the route keeps the binned charge of active OMs)
-        out0 = order0(T.order0, [el], origins[None], edges)
-        q0 = out0["charge"][0].cpu().numpy()
-        bins0 = out0["bins"][0]
-        charge[work, 0] = q0[work]
-        stage("order0_charge")
-        # order 1: the fused unit of elements emitting in every band
-        # (prompt.py:689-707, muon/secondary_first.py:184-204)
-        if not np.all(el["beta"][:, None] * T.phase[None, :] > 1):
-            raise NotImplementedError("elements above threshold in only some bands need the "
-                                      "per-band order-1 units")
-        cone = float(np.sum(T.prompt["s0w"] * T.phase) / np.sum(T.prompt["s0w"]))
-        cone_cos = 1.0 / (el["beta"] * cone)
-        # coarse charge screen and the reference's decision rule (prompt.py:720-812):
-        # full resolution where q0 + extra + margin * q1_coarse reaches threshold
-        fine_work = work
-        coarse = None
-        if cfg.screen and threshold > 0:
-            coarse = grouped(T.order1_screen, pencils(T.order1_screen, el, cone_cos), work,
-                             origins)[0].cpu().numpy()
-            charge[work, 1] = coarse[work]
-            level[work] = 1
-            stage("order1_screen")
-            fine_work = work[(charge[work, 0] + extra[work] + cfg.screen_margin
-                              * np.maximum(coarse[work], 0.0)) >= threshold]
-        b1 = np.zeros((n, len(edges) - 1))
-        if len(fine_work):
-            table = pencils(T.order1, el, cone_cos)
-            q1, bins1 = grouped(T.order1, table, fine_work, origins)
-            q1, bins1 = q1.cpu().numpy(), bins1.cpu().numpy()
-            charge[fine_work, 1] = q1[fine_work]
-            b1[fine_work] = bins1[fine_work]
-            level[fine_work] = 2
-            if coarse is not None:
-                worst = float(np.min(coarse[fine_work] / np.maximum(q1[fine_work], 1e-300)))
-                if worst * cfg.screen_margin < 1.0:
-                    wider = 1.5 / max(worst, 1e-3)
-                    more = work[(level[work] == 1) & (charge[work, 0] + extra[work] + wider
-                                                      * np.maximum(coarse[work], 0.0)
-                                                      >= threshold)]
-                    if len(more):
-                        q1, bins1 = grouped(T.order1, table, more, origins)
-                        charge[more, 1] = q1.cpu().numpy()[more]
-                        b1[more] = bins1.cpu().numpy()[more]
-                        level[more] = 2
-        stage("order1_fine")
-        return charge, b1, level == 2, level, el, bins0.cpu().numpy()
+        ev.inside = inside
+        ev.work = np.flatnonzero(inside)
+        ev.charge = np.zeros((n, 2))
+        ev.level1 = np.zeros(n, np.int8)
+        ev.bins1 = np.zeros((n, len(T.edges) - 1))
+        ev.extra_prompt = safety * np.abs(ev.predicted) + ev.extra
+        ev.pending["bins0"] = None
 
 
 def main(argv=None):

@@ -131,7 +131,7 @@ class SourceCompiler:
         p.omega = self._omega.data_ptr()
         return p
 
-    def compile(self, elements, frame=None, *, stream=None, check=True):
+    def compile(self, elements, frame=None, *, stream=None, check=True, status=None):
         """Points and channels of every node band (device), the emission reference.
 
         ``elements``: reference ``SpectralLightElements`` or a dict with its
@@ -189,12 +189,14 @@ class SourceCompiler:
             raise ValueError("source compile problem rejected by the device library")
         if self._workspace is None or self._workspace.numel() < need:
             self._workspace = torch.empty(need, dtype=torch.uint8, device=dev)
-        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        own_status = status is None
+        if own_status:
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
         sp = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
         _lib.check(lib.lh_source_compile(C.byref(p), C.byref(out), self._workspace.data_ptr(),
                                          self._workspace.numel(), status.data_ptr(), sp),
                    "lh_source_compile")
         self._keep = arrays
-        if check and int(status.item()) & _lib.LH_STATUS_OVERFLOW:
+        if own_status and check and int(status.item()) & _lib.LH_STATUS_OVERFLOW:
             raise ValueError("element nodes fall outside the source lattice")
         return points, channels, n_points, reference, frame
