@@ -193,12 +193,13 @@ def reference_arm(args, rank):
 N_SHOWER = 48
 
 
-def shower_stream_section(dev, steps, workers=4):
+def shower_stream_section(dev, steps, workers=2, max_batch=12):
     """Config 2: the served shower stream at 384 OMs through the device route.
 
     ``plain_fp32``: one shower after another on one stream, fp32 readout (the
-    per-event path). ``served``: the serving loop, ``workers`` worker streams,
-    split-BF16 readout. Wall time with the device synchronised on both sides
+    per-event path). ``served``: the serving loop (continuous batching of up to
+    ``max_batch`` queued showers per stage-major batch, ``workers`` worker
+    streams), split-BF16 readout. Wall time with the device synchronised on both sides
     (several streams and host orchestration: the device clock of one stream
     does not cover the job).
     """
@@ -227,7 +228,7 @@ def shower_stream_section(dev, steps, workers=4):
     torch.cuda.synchronize(dev)
     plain_s = (time.perf_counter() - t0) / reps
     server = ShowerServer(lambda: ShowerTransport(ShowerTables.synthetic("c2", device=dev)),
-                          workers=workers)
+                          workers=workers, max_batch=max_batch)
     for el in showers[:workers]:
         server.submit(el)
     server.drain(workers)
@@ -257,6 +258,7 @@ def shower_stream_section(dev, steps, workers=4):
                         "(500-50000 elements log-uniform, 0.15 m per element, vertices in a "
                         "200 m x 600 m cylinder, isotropic) on the 384-OM array, tables 2-450 m",
             "value": served_rate, "unit": "showers/s", "served_workers": workers,
+            "max_batch": max_batch,
             "plain_fp32": {"value": len(showers) / plain_s, "unit": "showers/s",
                            "launch": "the device route per shower on one stream, fp32 readout"},
             "served_over_plain": served_rate * plain_s / len(showers),

@@ -195,5 +195,20 @@ def ptr(tensor):
     return C.c_void_p(tensor.data_ptr())
 
 
+def upload(array, dtype, device):
+    """Host array -> device tensor without waiting for the device: staged through
+    pinned memory and copied asynchronously on the current stream (a pageable copy
+    would first drain every kernel queued on the stream)."""
+    import numpy as np
+    import torch
+    np_dtype = {torch.float64: np.float64, torch.int32: np.int32, torch.int64: np.int64,
+                torch.complex128: np.complex128, torch.complex64: np.complex64,
+                torch.float32: np.float32}[dtype]
+    host = torch.from_numpy(np.ascontiguousarray(array, dtype=np_dtype))
+    if torch.device(device).type != "cuda":
+        return host.to(device)
+    return host.pin_memory().to(device, non_blocking=True)
+
+
 def stream_ptr(stream):
     return C.c_void_p(stream.cuda_stream) if stream is not None else None

@@ -193,8 +193,8 @@ class Ge2Table:
             raise ValueError("source channels do not match the folded kernels")
         shift = ref - reference
         if np.any(shift != 0):  # align every band to the earliest emission reference
-            ph = torch.exp(1j * torch.tensor(self.omega[:ch.shape[3]], device=dev)[None, :]
-                           * torch.tensor(shift, device=dev)[:, None]).to(torch.complex64)
+            ph = _lib.upload(np.exp(1j * np.outer(shift, self.omega[:ch.shape[3]])),
+                             torch.complex64, dev)
             ch = ch * ph[:, None, None, :]
         ch = torch.view_as_real(ch.contiguous()).contiguous()
         scale = np.asarray(out_scale, float)
@@ -202,7 +202,7 @@ class Ge2Table:
             scale = np.repeat(scale[None, :], self.n_bands, axis=0)
 
         def f64(x):
-            return torch.tensor(np.ascontiguousarray(x, float), dtype=torch.float64, device=dev)
+            return _lib.upload(x, torch.float64, dev)
 
         d_pts, d_rec, d_lk, d_scale = f64(pts), f64(rec), f64(lk), f64(scale)
         result = torch.empty((n_om, W), dtype=torch.complex128, device=dev)

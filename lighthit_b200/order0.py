@@ -103,7 +103,13 @@ class Order0Optics:
 
 
 class ElementBatch:
-    """Elements of several events, concatenated on the device."""
+    """Elements of several events, concatenated on the device in one upload.
+
+    ``event(k)`` gives device views of event ``k``'s arrays (no copy), so the
+    other stages of a route read the same upload.
+    """
+
+    WIDTH = {"start_m": 3, "direction": 3}
 
     def __init__(self, events, device):
         import torch
@@ -112,18 +118,29 @@ class ElementBatch:
         self.counts = counts
         offsets = np.zeros(len(events) + 1, np.int64)
         offsets[1:] = np.cumsum(counts)
-        self.n_elements = int(offsets[-1])
-        cols = {}
-        for name in ELEMENT_FIELDS:
-            parts = [np.asarray(_field(e, name), float) for e in events]
-            cols[name] = np.concatenate(parts) if parts else np.zeros(0)
-        self._t = {k: torch.tensor(np.ascontiguousarray(v), dtype=torch.float64, device=device)
-                   for k, v in cols.items()}
-        self._t["offsets"] = torch.tensor(offsets, dtype=torch.int64, device=device)
+        self.offsets = offsets
+        self.n_elements = n = int(offsets[-1])
+        parts = [np.concatenate([np.asarray(_field(e, name), float).ravel() for e in events])
+                 if events else np.zeros(0) for name in ELEMENT_FIELDS]
+        flat = _lib.upload(np.concatenate(parts + [offsets.astype(float)]), torch.float64, device)
+        self._t = {}
+        pos = 0
+        for name, part in zip(ELEMENT_FIELDS, parts):
+            w = self.WIDTH.get(name, 1)
+            view = flat[pos:pos + n * w]
+            self._t[name] = view.view(n, w) if w > 1 else view
+            pos += n * w
+        self._t["offsets"] = flat[pos:].to(torch.int64)
+        self._flat = flat
 
     def pointers(self):
         t = self._t
         return [t[k].data_ptr() for k in ELEMENT_FIELDS]
+
+    def event(self, k):
+        """Device views of event ``k``'s element arrays (reference field names)."""
+        a, b = int(self.offsets[k]), int(self.offsets[k + 1])
+        return {name: self._t[name][a:b] for name in ELEMENT_FIELDS}
 
 
 def order0(optics: Order0Optics, events, origins=None, edges=None, *, stream=None,
@@ -149,10 +166,11 @@ def order0(optics: Order0Optics, events, origins=None, edges=None, *, stream=Non
             raise ValueError("bins need per-OM time origins")
         origins_t = torch.zeros((E, n), dtype=torch.float64, device=dev)
     else:
-        origins_t = torch.as_tensor(np.broadcast_to(np.asarray(origins, float), (E, n)).copy()
-                                    if not isinstance(origins, torch.Tensor) else origins,
-                                    dtype=torch.float64, device=dev).contiguous()
-    edges_t = torch.tensor(edges_np, dtype=torch.float64, device=dev)
+        origins_t = (origins.to(dev, torch.float64).contiguous()
+                     if isinstance(origins, torch.Tensor) else
+                     _lib.upload(np.broadcast_to(np.asarray(origins, float), (E, n)),
+                                 torch.float64, dev))
+    edges_t = _lib.upload(edges_np, torch.float64, dev)
     charge = torch.empty((E, n), dtype=torch.float64, device=dev)
     bins = (torch.empty((E, n, len(edges_np) - 1), dtype=torch.float64, device=dev)
             if want_bins else None)

@@ -153,6 +153,18 @@ class Order1Tables:
         self.compute_bins = bool(compute_bins)
         self._workspace = None
 
+    def pencil_table(self, capacity):
+        """A pencil table over this object's pooled buffer (grown when needed). Tables
+        from the pool are valid until the next stage-A call on the same stream."""
+        import torch
+        need = int(capacity) * PencilTable.ROW
+        if getattr(self, "_pencil_pool", None) is None or self._pencil_pool.numel() < need:
+            self._pencil_pool = torch.empty(max(need, 1 << 22), dtype=torch.float64,
+                                            device=self.device)
+        table = PencilTable(capacity, self.device, self._pencil_pool[:need])
+        table.pooled = True
+        return table
+
     def workspace(self, n_subseg, n_work):
         import torch
         need = int(_lib.load().lh_order1_workspace_bytes(self.struct, int(n_subseg), int(n_work)))
@@ -164,16 +176,25 @@ class Order1Tables:
 
 
 class PencilTable:
-    """Device pencil table (stage A output)."""
+    """Device pencil table (stage A output), one float64 buffer cut into its fields."""
 
     FIELDS = (("position", 3), ("direction", 3), ("w0", 1), ("w2", 1), ("time", 1),
               ("major", 3), ("var_major", 1), ("var_minor", 1), ("pos_cov", 6))
+    ROW = sum(c for _, c in FIELDS)
 
-    def __init__(self, capacity, device):
+    def __init__(self, capacity, device, buffer=None):
         import torch
         self.capacity = int(capacity)
-        self.t = {k: torch.empty((self.capacity, c) if c > 1 else (self.capacity,),
-                                 dtype=torch.float64, device=device) for k, c in self.FIELDS}
+        if buffer is None:
+            buffer = torch.empty(self.capacity * self.ROW, dtype=torch.float64, device=device)
+        self.pooled = buffer is not None and buffer.numel() != self.capacity * self.ROW
+        self.t = {}
+        pos = 0
+        for k, c in self.FIELDS:
+            view = buffer[pos:pos + self.capacity * c]
+            self.t[k] = view.view(self.capacity, c) if c > 1 else view
+            pos += self.capacity * c
+        self._buffer = buffer
         self.count = torch.zeros(1, dtype=torch.int32, device=device)
         self.struct = _lib.Order1PencilTable(self.capacity,
                                              *[self.t[k].data_ptr() for k, _ in self.FIELDS])
@@ -197,8 +218,13 @@ def _element(source, name):
     return source[name] if isinstance(source, dict) else getattr(source, name)
 
 
-def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=None):
-    """Stage A: ``compress`` of the elements with frozen cone cosines."""
+def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=None,
+            device_elements=None, capacity_full=False):
+    """Stage A: ``compress`` of the elements with frozen cone cosines.
+
+    ``device_elements``: the same elements already on the device (dict of
+    tensors with the reference field names), read instead of uploading.
+    """
     import torch
     dev = tables.device
     s = tables.settings
@@ -222,19 +248,30 @@ def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=Non
         raise ValueError("cell grid too large for 64-bit pencil keys; increase cell_m")
 
     def f64(x):
-        return torch.tensor(np.ascontiguousarray(x, float), dtype=torch.float64, device=dev)
+        return _lib.upload(x, torch.float64, dev)
 
-    keep = dict(off=torch.tensor(offsets, dtype=torch.int64, device=dev), start=f64(start),
-                direction=f64(direction), length=f64(length),
-                c0=f64(_element(elements, "coefficient0")),
-                c2=f64(_element(elements, "coefficient2")), cone=f64(cone_cos),
-                t0=f64(_element(elements, "start_ns")), t1=f64(_element(elements, "end_ns")))
+    d = device_elements
+    if d is None:
+        keep = dict(start=f64(start), direction=f64(direction), length=f64(length),
+                    c0=f64(_element(elements, "coefficient0")),
+                    c2=f64(_element(elements, "coefficient2")),
+                    t0=f64(_element(elements, "start_ns")), t1=f64(_element(elements, "end_ns")))
+    else:
+        keep = dict(start=d["start_m"], direction=d["direction"], length=d["length_m"],
+                    c0=d["coefficient0"], c2=d["coefficient2"], t0=d["start_ns"],
+                    t1=d["end_ns"])
+    keep["cone"] = (cone_cos if isinstance(cone_cos, torch.Tensor) else f64(cone_cos)).contiguous()
+    keep["off"] = _lib.upload(offsets, torch.int64, dev)
     el = _lib.Order1Elements(n_el, n_sub, keep["off"].data_ptr(), keep["start"].data_ptr(),
                              keep["direction"].data_ptr(), keep["length"].data_ptr(),
                              keep["c0"].data_ptr(), keep["c2"].data_ptr(), keep["cone"].data_ptr(),
                              keep["t0"].data_ptr(), keep["t1"].data_ptr(),
                              (C_DOUBLE3)(*low), (C_INT64_3)(*dims))
-    table = PencilTable(max(n_sub * s.ring_nodes, 1), dev)
+    nodes = max(n_sub * s.ring_nodes, 1)
+    # Pencils are distinct (cell, pixel) keys: far fewer than ring nodes when many
+    # elements share cells. A table that overflows is redone at the full bound.
+    capacity = nodes if capacity_full else min(nodes, max(1 << 17, nodes // 4))
+    table = PencilTable(capacity, dev) if capacity_full else tables.pencil_table(capacity)
     ws = tables.workspace(n_sub, 0)
     st = status if status is not None else torch.zeros(1, dtype=torch.int32, device=dev)
     sp = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
@@ -242,8 +279,13 @@ def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=Non
                                              table.count.data_ptr(), ws.data_ptr(), ws.numel(),
                                              st.data_ptr(), sp), "lh_order1_pencils")
     table._keep = keep
+    table.nodes = nodes
     if status is None:
-        _raise(int(st.item()))
+        flags = int(st.item())
+        if flags & _lib.LH_STATUS_OVERFLOW and capacity < nodes:
+            return pencils(tables, elements, cone_cos, stream=stream,
+                           device_elements=device_elements, capacity_full=True)
+        _raise(flags)
     return table
 
 
@@ -261,9 +303,9 @@ def grouped(tables: Order1Tables, table: "PencilTable", work, origins, *, n_penc
         raise ValueError("work lists OMs outside the detector")
     if np.shape(origins) != (n,):
         raise ValueError("time origins must hold one value per OM")
-    work_t = torch.tensor(work, dtype=torch.int32, device=dev)
-    origins_t = torch.as_tensor(np.asarray(origins, float) if not isinstance(origins, torch.Tensor)
-                                else origins, dtype=torch.float64, device=dev).contiguous()
+    work_t = _lib.upload(work, torch.int32, dev)
+    origins_t = (origins.to(dev, torch.float64).contiguous() if isinstance(origins, torch.Tensor)
+                 else _lib.upload(origins, torch.float64, dev))
     charge = torch.empty(n, dtype=torch.float64, device=dev)
     bins = (torch.empty((n, len(tables.edges) - 1), dtype=torch.float64, device=dev)
             if tables.compute_bins else None)

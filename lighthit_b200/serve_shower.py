@@ -1,12 +1,14 @@
-"""Serving loop for showers: requests overlapped on the device by worker streams.
+"""Serving loop for showers: continuous batching over worker streams.
 
 Each worker owns a ``ShowerTransport`` on its own device tables and
-workspaces and its own CUDA stream; requests (one shower each) are taken from
-a shared queue as workers free up, so the kernels of several showers run on
-the device at once while the host orchestrates the next one. Admission is by
-HBM budget: a request waits until its estimated device footprint fits beside
-the requests in flight. Every result is the same as the shower alone (the
-route is deterministic per request and shares no mutable state).
+workspaces and its own CUDA stream. A free worker takes every queued request
+(up to ``max_batch``) as one batch and runs the route stage by stage for the
+whole batch (``ShowerTransport.batch``), so requests that arrive while others
+are on the device join the next batch, the kernels of several batches overlap
+on the device, and the host orchestrates one batch while the device runs
+another. Admission is by HBM budget: a batch is cut where the estimated device
+footprint of the requests in flight would exceed it. Every result equals the
+shower run alone (the stages are per shower; only launches are shared).
 """
 from __future__ import annotations
 
@@ -47,9 +49,11 @@ class ShowerRequest:
 class ShowerServer:
     """``workers`` threads, each with its own route, stream and workspaces."""
 
-    def __init__(self, make_route, *, workers=4, hbm_budget_bytes=32 << 30, n_om=384):
+    def __init__(self, make_route, *, workers=4, max_batch=16, hbm_budget_bytes=32 << 30,
+                 n_om=384):
         import torch
         self.n_om = n_om
+        self.max_batch = int(max_batch)
         self.budget = int(hbm_budget_bytes)
         self.in_flight = 0
         self.lock = threading.Condition()
@@ -71,27 +75,55 @@ class ShowerServer:
         self.queue.put(req)
         return req
 
+    def _take(self):
+        """Block for one request, then take what else is queued (up to ``max_batch``)."""
+        first = self.queue.get()
+        if first is None:
+            return None
+        batch = [first]
+        while len(batch) < self.max_batch:
+            try:
+                nxt = self.queue.get_nowait()
+            except queue.Empty:
+                break
+            if nxt is None:
+                self.queue.put(None)
+                break
+            batch.append(nxt)
+        return batch
+
     def _work(self, k):
         import torch
         route, stream = self.routes[k], self.streams[k]
         while True:
-            req = self.queue.get()
-            if req is None:
+            batch = self._take()
+            if batch is None:
                 return
+            footprint = sum(r.footprint for r in batch)
             with self.lock:  # admission by HBM budget
-                while self.in_flight and self.in_flight + req.footprint > self.budget:
+                while self.in_flight and self.in_flight + footprint > self.budget:
                     self.lock.wait()
-                self.in_flight += req.footprint
+                self.in_flight += footprint
             try:
                 with torch.cuda.stream(stream):
-                    req.result = route(req.source)
+                    results = route.batch([r.source for r in batch])
                     stream.synchronize()
-            except BaseException as exc:  # noqa: BLE001 - handed back to the client
-                req.error = exc
-            req.done_at = time.perf_counter()
+                for r, res in zip(batch, results):
+                    r.result = res
+            except BaseException:  # noqa: BLE001 - rerun alone to attach the error to its request
+                for r in batch:
+                    try:
+                        with torch.cuda.stream(stream):
+                            r.result = route(r.source)
+                            stream.synchronize()
+                    except BaseException as exc:  # noqa: BLE001 - handed back to the client
+                        r.error = exc
+            done = time.perf_counter()
             with self.lock:
-                self.in_flight -= req.footprint
-                self.completed.append(req)
+                self.in_flight -= footprint
+                for r in batch:
+                    r.done_at = done
+                    self.completed.append(r)
                 self.lock.notify_all()
 
     def drain(self, count):

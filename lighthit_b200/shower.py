@@ -37,7 +37,7 @@ import numpy as np
 
 from . import _lib
 from .ge2 import AxialSources, Ge2Table
-from .order0 import Order0Optics, order0, raise_status as raise_order0_status
+from .order0 import ElementBatch, Order0Optics, order0, raise_status as raise_order0_status
 from .order1 import Order1Tables, PromptSettings, acceptance_monomials, grouped, pencils
 from .readout import DeviceReadout
 from .source import ShowerBasisSettings, SourceCompiler, axis_frame
@@ -164,28 +164,24 @@ class ShowerTables:
             raise ValueError("known synthetic tables: c0, c2")
         return cls(TABLES / f"route_{name}.npz", TABLES / folded[name], **kw)
 
-    def om_geometry_batch(self, prompt_elements, elements, group_index):
+    def om_geometry_batch(self, prompt_store, store, group_index):
         """Per shower: distances to the prompt elements and earliest arrivals (device)."""
         import torch
         dev = self.device
         n = self.n_om
         out = []
-        for events in (prompt_elements, elements):
-            offsets, cat = _concat_elements(events)
-            t = {k: torch.tensor(np.ascontiguousarray(v), dtype=torch.float64, device=dev)
-                 for k, v in cat.items()}
-            off = torch.tensor(offsets, dtype=torch.int64, device=dev)
-            res = torch.empty((len(events), n), dtype=torch.float64, device=dev)
-            want_distance = events is prompt_elements
-            g = _lib.OmGeometry(n, self._pos.data_ptr(), len(events), off.data_ptr(),
+        for batch, want_distance in ((prompt_store, True), (store, False)):
+            t = batch._t
+            res = torch.empty((batch.n_events, n), dtype=torch.float64, device=dev)
+            g = _lib.OmGeometry(n, self._pos.data_ptr(), batch.n_events, t["offsets"].data_ptr(),
                                 t["start_m"].data_ptr(), t["direction"].data_ptr(),
                                 t["length_m"].data_ptr(), t["start_ns"].data_ptr(),
                                 float(group_index), res.data_ptr() if want_distance else None,
                                 None if want_distance else res.data_ptr())
             sp = _lib.stream_ptr(torch.cuda.current_stream(dev))
             _lib.check(_lib.load().lh_om_geometry(C.byref(g), sp), "lh_om_geometry")
-            out.append((res, t, off))
-        return out[0][0].cpu().numpy(), out[1][0].cpu().numpy()
+            out.append(res)
+        return out[0].cpu().numpy(), out[1].cpu().numpy()
 
     def attenuation(self, distance):
         radius, log_factor = self._attenuation
@@ -369,10 +365,13 @@ class ShowerTransport:
             ev.frame = axis_frame(el["start_m"], el["direction"], el["length_m"],
                                   el["coefficient0"])
             events.append(ev)
+        store = ElementBatch([ev.el for ev in events], dev)  # one upload for every stage
         stage("setup")
         # ---- order >=2 sources on the node bands (device, all showers)
         src_status = torch.zeros(1, dtype=torch.int32, device=dev)
-        compiled = [T.source.compile(ev.el, ev.frame, status=src_status) for ev in events]
+        compiled = [T.source.compile(ev.el, ev.frame, status=src_status,
+                                     device_elements=store.event(k))
+                    for k, ev in enumerate(events)]
         npts_all = torch.stack([c[2] for c in compiled]).cpu().numpy()
         if int(src_status.item()) & _lib.LH_STATUS_OVERFLOW:
             raise ValueError("element nodes fall outside the source lattice")
@@ -479,8 +478,9 @@ class ShowerTransport:
             if not np.all(pvalid):
                 pel = _subset(el, pvalid)
             ev.prompt_el = pel
-        dist, early = T.om_geometry_batch([ev.prompt_el for ev in events],
-                                          [ev.el for ev in events], fastest)
+        same = all(ev.prompt_el is ev.el for ev in events)
+        prompt_store = store if same else ElementBatch([ev.prompt_el for ev in events], dev)
+        dist, early = T.om_geometry_batch(prompt_store, store, fastest)
         for k, ev in enumerate(events):
             if ev.origins is None:
                 ev.origins = early[k]
@@ -493,19 +493,24 @@ class ShowerTransport:
         prompt_events = [ev for ev in events if len(ev.work)]
         if prompt_events:
             origins = np.stack([ev.origins for ev in prompt_events])
-            out0 = order0(T.order0, [ev.prompt_el for ev in prompt_events], origins, edges,
-                          check=False)
+            batch0 = (prompt_store if len(prompt_events) == len(events) else
+                      ElementBatch([ev.prompt_el for ev in prompt_events], dev))
+            out0 = order0(T.order0, batch0, origins, edges, check=False)
+        for k, ev in enumerate(events):
+            ev.device_el = prompt_store.event(k)
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         cone = float(np.sum(T.prompt["s0w"] * T.phase) / np.sum(T.prompt["s0w"]))
         for ev in prompt_events:
             if not np.all(ev.prompt_el["beta"][:, None] * T.phase[None, :] > 1):
                 raise NotImplementedError("elements above threshold in only some bands need the "
                                           "per-band order-1 units")
-            ev.cone_cos = 1.0 / (ev.prompt_el["beta"] * cone)
+            ev.cone_cos = 1.0 / (ev.device_el["beta"] * cone)
             if cfg.screen and threshold > 0:
-                coarse = pencils(T.order1_screen, ev.prompt_el, ev.cone_cos, status=status)
+                ev.status = torch.zeros(1, dtype=torch.int32, device=dev)
+                coarse = pencils(T.order1_screen, ev.prompt_el, ev.cone_cos, status=ev.status,
+                                 device_elements=ev.device_el)
                 ev.pending["coarse"] = grouped(T.order1_screen, coarse, ev.work, ev.origins,
-                                               status=status)[0]
+                                               status=ev.status)[0]
         if prompt_events:
             raise_order0_status(int(out0["status"].item()))
             q0_all = out0["charge"].cpu().numpy()
@@ -513,6 +518,7 @@ class ShowerTransport:
             for k, ev in enumerate(prompt_events):
                 ev.charge[ev.work, 0] = q0_all[k][ev.work]
                 ev.pending["bins0"] = bins0_all[k]
+        self._redo_overflow(prompt_events, "coarse", T.order1_screen)
         stage("order0_screen")
         for ev in prompt_events:
             ev.fine = ev.work
@@ -525,9 +531,12 @@ class ShowerTransport:
                                    + cfg.screen_margin * np.maximum(coarse[ev.work], 0.0))
                                   >= threshold]
             if len(ev.fine):
-                ev.table = pencils(T.order1, ev.prompt_el, ev.cone_cos, status=status)
+                ev.status = torch.zeros(1, dtype=torch.int32, device=dev)
+                ev.table = pencils(T.order1, ev.prompt_el, ev.cone_cos, status=ev.status,
+                                   device_elements=ev.device_el)
                 ev.pending["fine"] = grouped(T.order1, ev.table, ev.fine, ev.origins,
-                                             status=status)
+                                             status=ev.status)
+        self._redo_overflow(prompt_events, "fine", T.order1)
         for ev in prompt_events:
             if "fine" not in ev.pending:
                 continue
@@ -545,7 +554,9 @@ class ShowerTransport:
                                    & (ev.charge[ev.work, 0] + ev.extra_prompt[ev.work] + wider
                                       * np.maximum(coarse[ev.work], 0.0) >= threshold)]
                     if len(more):
-                        q1m, b1m = grouped(T.order1, ev.table, more, ev.origins, status=status)
+                        table = pencils(T.order1, ev.prompt_el, ev.cone_cos, status=status,
+                                        device_elements=ev.device_el, capacity_full=True)
+                        q1m, b1m = grouped(T.order1, table, more, ev.origins, status=status)
                         ev.charge[more, 1] = q1m.cpu().numpy()[more]
                         ev.bins1[more] = b1m.cpu().numpy()[more]
                         ev.level1[more] = 2
@@ -604,8 +615,8 @@ class ShowerTransport:
             ids = np.flatnonzero(ev.active)
             missing = np.flatnonzero(ev.active & (ev.level1 < 2))
             if len(missing):  # the reference reruns the prompt without its screen
-                table = ev.table if ev.table is not None else pencils(
-                    T.order1, ev.prompt_el, 1.0 / (ev.prompt_el["beta"] * cone), status=status)
+                table = pencils(T.order1, ev.prompt_el, 1.0 / (ev.prompt_el["beta"] * cone),
+                                status=status, capacity_full=True)
                 q1m, b1m = grouped(T.order1, table, missing, ev.origins, status=status)
                 ev.charge[missing, 1] = q1m.cpu().numpy()[missing]
                 ev.bins1[missing] = b1m.cpu().numpy()[missing]
@@ -614,11 +625,11 @@ class ShowerTransport:
                 spec = self._apply_device(ev.points, ev.channels, ev.reference, ev.frame, work,
                                           zero_frequency=False)
                 ev.pending["spec"] = (work, spec)
-                phase = torch.tensor(np.exp(-1j * np.outer(ev.origins[work], omega)),
-                                     dtype=torch.complex128, device=dev)
+                phase = _lib.upload(np.exp(-1j * np.outer(ev.origins[work], omega)),
+                                    torch.complex128, dev)
                 rel = spec * phase
                 # the stored zero frequency is the exact >=2 charge (shower/api.py:584)
-                rel[:, 0] = torch.tensor(ev.charge[work, 2], dtype=torch.complex128, device=dev)
+                rel[:, 0] = _lib.upload(ev.charge[work, 2], torch.complex128, dev)
                 rel = rel.to(torch.complex64)
                 rows.append(rel)
                 row_ev.append((k, work))
@@ -666,6 +677,24 @@ class ShowerTransport:
                                                      ev.origins, ev.active, "shower", metadata))
         stage("ge2_full_readout")
         return responses
+
+    def _redo_overflow(self, events, key, tables):
+        """Events whose bounded pencil table overflowed: stage A and B again at full size."""
+        import torch
+        pend = [ev for ev in events if key in ev.pending]
+        if not pend:
+            return
+        flags = torch.cat([ev.status for ev in pend]).cpu().numpy()
+        for ev, f in zip(pend, flags):
+            if not f & _lib.LH_STATUS_OVERFLOW:
+                continue
+            table = pencils(tables, ev.prompt_el, ev.cone_cos, device_elements=ev.device_el,
+                            capacity_full=True)
+            work = ev.work if key == "coarse" else ev.fine
+            res = grouped(tables, table, work, ev.origins)
+            ev.pending[key] = res[0] if key == "coarse" else res
+            if key == "fine":
+                ev.table = table
 
     @staticmethod
     def _zero_only(channels):

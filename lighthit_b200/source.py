@@ -131,7 +131,8 @@ class SourceCompiler:
         p.omega = self._omega.data_ptr()
         return p
 
-    def compile(self, elements, frame=None, *, stream=None, check=True, status=None):
+    def compile(self, elements, frame=None, *, stream=None, check=True, status=None,
+                device_elements=None):
         """Points and channels of every node band (device), the emission reference.
 
         ``elements``: reference ``SpectralLightElements`` or a dict with its
@@ -170,9 +171,15 @@ class SourceCompiler:
             raise NotImplementedError("chord nodes reach below the slice lattice origin")
         n_slices = int(zb.max()) + 3
         dev = self.device
-        arrays = {k: torch.tensor(np.ascontiguousarray(v), dtype=torch.float64, device=dev)
-                  for k, v in dict(start=start, direction=direction, length=length, c0=c0, c2=c2,
-                                   beta=beta, t0=t0, t1=t1).items()}
+        if device_elements is None:
+            arrays = {k: _lib.upload(v, torch.float64, dev)
+                      for k, v in dict(start=start, direction=direction, length=length, c0=c0,
+                                       c2=c2, beta=beta, t0=t0, t1=t1).items()}
+        else:
+            d = device_elements
+            arrays = dict(start=d["start_m"], direction=d["direction"], length=d["length_m"],
+                          c0=d["coefficient0"], c2=d["coefficient2"], beta=d["beta"],
+                          t0=d["start_ns"], t1=d["end_ns"])
         p = self.problem(arrays, frame, len(length), order, fractions, weights, reference,
                          z_origin, n_slices, kmax)
         nb = len(self.wavelengths)
