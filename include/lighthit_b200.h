@@ -173,6 +173,17 @@ size_t lh_ge2_workspace_bytes(const lh_ge2_table* t, const lh_ge2_problem* p);
 int lh_ge2_apply(const lh_ge2_table* t, const lh_ge2_problem* p, void* workspace,
                  size_t workspace_bytes, void* stream);
 
+/* Many problems (the events of a batch) on one table in one set of launches:
+ * the same per-problem results as n calls of lh_ge2_apply (n <= 65535; a
+ * problem without points yields zeros). `host_slots` is caller host memory of
+ * lh_ge2_batch_slot_bytes(n) bytes staging the per-problem table copied to the
+ * workspace: pageable memory may be reused when the call returns, pinned memory
+ * only after the stream has passed the call. */
+size_t lh_ge2_batch_workspace_bytes(const lh_ge2_table* t, const lh_ge2_problem* p, int32_t n);
+size_t lh_ge2_batch_slot_bytes(int32_t n);
+int lh_ge2_apply_batch(const lh_ge2_table* t, const lh_ge2_problem* p, int32_t n,
+                       void* workspace, size_t workspace_bytes, void* host_slots, void* stream);
+
 /* ------------------------------------------------------------------ order 0
  * Replaces PreparedBallistic.charge() / .bins(ids, origins, edges)
  * (_surface_ballistic.py:95-118, the first-entry order 0 of transport_prompt,

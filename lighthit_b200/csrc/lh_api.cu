@@ -162,6 +162,10 @@ int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op,
 namespace lh {
 size_t ge2_workspace(const lh_ge2_table& T, const lh_ge2_problem& P);
 int ge2_launch(const lh_ge2_table& T, const lh_ge2_problem& P, void* ws, cudaStream_t s);
+size_t ge2_slot_size();
+size_t ge2_batch_workspace(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n);
+int ge2_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n, void* ws,
+                     void* host_slots, cudaStream_t s);
 }  // namespace lh
 
 namespace {
@@ -201,4 +205,26 @@ extern "C" int lh_ge2_apply(const lh_ge2_table* t, const lh_ge2_problem* p, void
     return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
   }
   return lh::ge2_launch(*t, *p, workspace, s);
+}
+
+extern "C" size_t lh_ge2_batch_workspace_bytes(const lh_ge2_table* t, const lh_ge2_problem* p,
+                                               int32_t n) {
+  if (!t || !p || n < 1 || n > 65535) return 0;
+  for (int i = 0; i < n; ++i)
+    if (!ge2_valid(t, p + i)) return 0;
+  return lh::ge2_batch_workspace(*t, p, n);
+}
+
+extern "C" size_t lh_ge2_batch_slot_bytes(int32_t n) {
+  return n < 1 ? 0 : (size_t)n * lh::ge2_slot_size();
+}
+
+extern "C" int lh_ge2_apply_batch(const lh_ge2_table* t, const lh_ge2_problem* p, int32_t n,
+                                  void* workspace, size_t workspace_bytes, void* host_slots,
+                                  void* stream) {
+  if (!t || !p || n < 1 || n > 65535 || !host_slots) return LH_EINVAL;
+  for (int i = 0; i < n; ++i)
+    if (!ge2_valid(t, p + i)) return LH_EINVAL;
+  if (!workspace || workspace_bytes < lh::ge2_batch_workspace(*t, p, n)) return LH_ENOMEM;
+  return lh::ge2_batch_launch(*t, p, n, workspace, host_slots, static_cast<cudaStream_t>(stream));
 }

@@ -20,6 +20,8 @@
 // (d, c); ge2_apply_kernel runs the float32 contraction with one thread per
 // (band, frequency); ge2_reduce_kernel sums the point chunks in a fixed order
 // (identical results alone or in a batch) and applies the emission-time phase.
+#include <algorithm>
+
 #include "lh_common.cuh"
 
 namespace lh {
@@ -92,9 +94,8 @@ LH_DEVICE void real_harmonics(double x, double y, double z, int A, double* out) 
 }
 
 // One thread per (OM, point): radius, interval, band scales and F.
-__global__ void ge2_geometry_kernel(lh_ge2_table T, lh_ge2_problem P, int* g_j, float* g_t,
-                                    double* g_r, float* g_scale, float* g_F) {
-  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+LH_DEVICE void ge2_geometry_body(const lh_ge2_table& T, const lh_ge2_problem& P, int64_t idx,
+                                 int* g_j, float* g_t, double* g_r, float* g_scale, float* g_F) {
   const int64_t total = (int64_t)P.n_om * P.n_points;
   if (idx >= total) return;
   const int d = (int)(idx / P.n_points), c = (int)(idx % P.n_points);
@@ -211,11 +212,10 @@ __global__ void ge2_geometry_kernel(lh_ge2_table T, lh_ge2_problem P, int* g_j, 
 }
 
 // Grid (OM, point chunk); thread = (band, frequency). Partial sums per chunk.
-__global__ void ge2_apply_kernel(lh_ge2_table T, lh_ge2_problem P, const int* g_j,
-                                 const float* g_t, const double* g_r, const float* g_scale,
-                                 const float* g_F, double2* partial) {
+LH_DEVICE void ge2_apply_body(const lh_ge2_table& T, const lh_ge2_problem& P, int d, int chunk,
+                              int chunks, const int* g_j, const float* g_t, const double* g_r,
+                              const float* g_scale, const float* g_F, double2* partial) {
   extern __shared__ float s_F[];  // [kGe2Chunk][nch*NP] for the chunk's points
-  const int d = blockIdx.x, chunk = blockIdx.y;
   const int c0 = chunk * kGe2Chunk;
   const int c1 = min(P.n_points, c0 + kGe2Chunk);
   const int NP = T.n_pairs, nch = T.nch, Wn = P.n_omega;
@@ -274,15 +274,14 @@ __global__ void ge2_apply_kernel(lh_ge2_table T, lh_ge2_problem P, const int* g_
       acc_re += s * (pr * cv - pi * sv);
       acc_im += s * (pr * sv + pi * cv);
     }
-    partial[(((int64_t)d * gridDim.y + chunk) * T.n_bands + lam) * Wn + w] =
+    partial[(((int64_t)d * chunks + chunk) * T.n_bands + lam) * Wn + w] =
         make_double2(acc_re, acc_im);
   }
 }
 
 // result[d][w] = e^{i w ref} * sum over chunks and bands, fixed order.
-__global__ void ge2_reduce_kernel(lh_ge2_table T, lh_ge2_problem P, int chunks,
-                                  const double2* partial) {
-  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+LH_DEVICE void ge2_reduce_body(const lh_ge2_table& T, const lh_ge2_problem& P, int64_t idx,
+                               int chunks, const double2* partial) {
   const int Wn = P.n_omega;
   if (idx >= (int64_t)P.n_om * Wn) return;
   const int d = (int)(idx / Wn), w = (int)(idx % Wn);
@@ -297,6 +296,64 @@ __global__ void ge2_reduce_kernel(lh_ge2_table T, lh_ge2_problem P, int chunks,
   const double c = cos(ang), s = sin(ang);
   P.result[2 * idx] = re * c - im * s;
   P.result[2 * idx + 1] = re * s + im * c;
+}
+
+// One problem: grids over its own sizes.
+__global__ void ge2_geometry_kernel(lh_ge2_table T, lh_ge2_problem P, int* g_j, float* g_t,
+                                    double* g_r, float* g_scale, float* g_F) {
+  ge2_geometry_body(T, P, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, g_j, g_t, g_r, g_scale,
+                    g_F);
+}
+
+__global__ void ge2_apply_kernel(lh_ge2_table T, lh_ge2_problem P, const int* g_j,
+                                 const float* g_t, const double* g_r, const float* g_scale,
+                                 const float* g_F, double2* partial) {
+  ge2_apply_body(T, P, blockIdx.x, blockIdx.y, gridDim.y, g_j, g_t, g_r, g_scale, g_F, partial);
+}
+
+__global__ void ge2_reduce_kernel(lh_ge2_table T, lh_ge2_problem P, int chunks,
+                                  const double2* partial) {
+  ge2_reduce_body(T, P, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, chunks, partial);
+}
+
+// Many problems (events) in one launch: blockIdx.z (or .y) selects the problem,
+// whose workspace regions start at its pair / partial offsets.
+struct Ge2Slot {
+  lh_ge2_problem P;
+  int64_t pair_offset;     // sum of n_om * n_points of the earlier problems
+  int64_t partial_offset;  // sum of n_om * chunks * n_bands * n_omega of the earlier problems
+  int32_t chunks;
+};
+
+struct Ge2Arrays {
+  int* g_j;
+  float* g_t;
+  double* g_r;
+  float* g_scale;  // [problem][band][pairs]
+  float* g_F;
+  double2* partial;
+};
+
+__global__ void ge2_geometry_batch_kernel(lh_ge2_table T, const Ge2Slot* slots, Ge2Arrays A) {
+  const Ge2Slot& S = slots[blockIdx.y];
+  const int64_t o = S.pair_offset;
+  ge2_geometry_body(T, S.P, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, A.g_j + o, A.g_t + o,
+                    A.g_r + o, A.g_scale + o * T.n_bands, A.g_F + o * T.nch * T.n_pairs);
+}
+
+__global__ void ge2_apply_batch_kernel(lh_ge2_table T, const Ge2Slot* slots, Ge2Arrays A) {
+  const Ge2Slot& S = slots[blockIdx.z];
+  if ((int)blockIdx.x >= S.P.n_om || (int)blockIdx.y >= S.chunks) return;
+  const int64_t o = S.pair_offset;
+  ge2_apply_body(T, S.P, blockIdx.x, blockIdx.y, S.chunks, A.g_j + o, A.g_t + o, A.g_r + o,
+                 A.g_scale + o * T.n_bands, A.g_F + o * T.nch * T.n_pairs,
+                 A.partial + S.partial_offset);
+}
+
+__global__ void ge2_reduce_batch_kernel(lh_ge2_table T, const Ge2Slot* slots, Ge2Arrays A) {
+  const Ge2Slot& S = slots[blockIdx.y];
+  ge2_reduce_body(T, S.P, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, S.chunks,
+                  A.partial + S.partial_offset);
 }
 
 int ge2_chunks(const lh_ge2_problem& P) { return (P.n_points + kGe2Chunk - 1) / kGe2Chunk; }
@@ -329,6 +386,68 @@ int ge2_launch(const lh_ge2_table& T, const lh_ge2_problem& P, void* ws, cudaStr
                                                             partial);
   const int64_t outs = (int64_t)P.n_om * P.n_omega;
   ge2_reduce_kernel<<<(unsigned)((outs + 255) / 256), 256, 0, s>>>(T, P, chunks, partial);
+  return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+}
+
+size_t ge2_slot_size() { return sizeof(Ge2Slot); }
+
+size_t ge2_batch_workspace(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n) {
+  size_t pairs = 0, partial = 0;
+  for (int i = 0; i < n; ++i) {
+    pairs += (size_t)P[i].n_om * P[i].n_points;
+    partial += (size_t)P[i].n_om * ge2_chunks(P[i]) * T.n_bands * P[i].n_omega;
+  }
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  return up(sizeof(Ge2Slot) * (size_t)n) + up(pairs * 4) + up(pairs * 4) + up(pairs * 8) +
+         up(pairs * T.n_bands * 4) + up(pairs * T.nch * T.n_pairs * 4) +
+         up(partial * sizeof(double2));
+}
+
+// The slot table is staged in `host_slots` (caller memory, pinned when the call
+// should not wait) and copied to the workspace on the stream.
+int ge2_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n, void* ws,
+                     void* host_slots, cudaStream_t s) {
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  Ge2Slot* hs = static_cast<Ge2Slot*>(host_slots);
+  size_t pairs = 0, partial = 0;
+  int max_om = 0, max_chunks = 0;
+  int64_t max_pairs = 0, max_outs = 0;
+  for (int i = 0; i < n; ++i) {
+    hs[i].P = P[i];
+    hs[i].pair_offset = (int64_t)pairs;
+    hs[i].partial_offset = (int64_t)partial;
+    hs[i].chunks = ge2_chunks(P[i]);
+    const int64_t pp = (int64_t)P[i].n_om * P[i].n_points;
+    pairs += pp;
+    partial += (size_t)P[i].n_om * hs[i].chunks * T.n_bands * P[i].n_omega;
+    max_om = std::max(max_om, P[i].n_om);
+    max_chunks = std::max(max_chunks, hs[i].chunks);
+    max_pairs = std::max(max_pairs, pp);
+    max_outs = std::max(max_outs, (int64_t)P[i].n_om * P[i].n_omega);
+  }
+  uint8_t* p = static_cast<uint8_t*>(ws);
+  Ge2Slot* slots = reinterpret_cast<Ge2Slot*>(p); p += up(sizeof(Ge2Slot) * (size_t)n);
+  Ge2Arrays A;
+  A.g_j = reinterpret_cast<int*>(p); p += up(pairs * 4);
+  A.g_t = reinterpret_cast<float*>(p); p += up(pairs * 4);
+  A.g_r = reinterpret_cast<double*>(p); p += up(pairs * 8);
+  A.g_scale = reinterpret_cast<float*>(p); p += up(pairs * T.n_bands * 4);
+  A.g_F = reinterpret_cast<float*>(p); p += up(pairs * T.nch * T.n_pairs * 4);
+  A.partial = reinterpret_cast<double2*>(p);
+  if (cudaMemcpyAsync(slots, hs, sizeof(Ge2Slot) * (size_t)n, cudaMemcpyHostToDevice, s) !=
+      cudaSuccess)
+    return LH_ECUDA;
+  if (max_outs == 0) return LH_OK;
+  if (max_pairs > 0) {  // problems without points reduce nothing: their results are zero
+    ge2_geometry_batch_kernel<<<dim3((unsigned)((max_pairs + 127) / 128), n), 128, 0, s>>>(
+        T, slots, A);
+    const size_t smem = (size_t)kGe2Chunk * T.nch * T.n_pairs * sizeof(float);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(ge2_apply_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+    ge2_apply_batch_kernel<<<dim3(max_om, max_chunks, n), 256, smem, s>>>(T, slots, A);
+  }
+  ge2_reduce_batch_kernel<<<dim3((unsigned)((max_outs + 255) / 256), n), 256, 0, s>>>(T, slots, A);
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }
 

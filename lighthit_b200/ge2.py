@@ -151,13 +151,11 @@ class Ge2Table:
         torch.cuda.synchronize(self.device)
         return res.cpu().numpy().T
 
-    def apply_device(self, sources, positions, looks, out_scale, window=None, *,
-                     zero_frequency=False, stream=None):
+    def _prepare(self, sources, positions, looks, out_scale, window, zero_frequency):
+        """Host geometry in the axis frame and the device channels of one problem."""
         import torch
-        lib = _lib.load()
         dev = self.device
         positions = np.atleast_2d(np.asarray(positions, float))
-        n_om = len(positions)
         W = 1 if zero_frequency else len(self.omega)
         if sources.degree < self.degree:
             raise ValueError("source degree is insufficient")
@@ -200,25 +198,65 @@ class Ge2Table:
         scale = np.asarray(out_scale, float)
         if scale.ndim == 1:
             scale = np.repeat(scale[None, :], self.n_bands, axis=0)
+        if scale.shape != (self.n_bands, len(positions)):
+            raise ValueError("out_scale must hold one value per OM (per band)")
+        return dict(pts=pts, rec=rec, lk=lk, scale=scale, ch=ch, W=W, low=low, high=high,
+                    reference=reference, n_om=len(positions))
 
-        def f64(x):
-            return _lib.upload(x, torch.float64, dev)
+    def _problem(self, q, base, result_ptr):
+        """The C problem of a prepared ``q`` whose f64 blocks start at device ``base``."""
+        offs, at = {}, base
+        for key in ("pts", "rec", "lk", "scale"):
+            offs[key] = at
+            at += 8 * q[key].size
+        return _lib.Ge2Problem(len(q["pts"]), offs["pts"], q["ch"].data_ptr(),
+                               int(q["ch"].shape[3]), q["W"], q["n_om"], offs["rec"],
+                               offs["lk"], offs["scale"], q["low"], q["high"], q["reference"],
+                               result_ptr), at
 
-        d_pts, d_rec, d_lk, d_scale = f64(pts), f64(rec), f64(lk), f64(scale)
-        result = torch.empty((n_om, W), dtype=torch.complex128, device=dev)
-        prob = _lib.Ge2Problem(len(pts), d_pts.data_ptr(), ch.data_ptr(), int(ch.shape[3]), W,
-                               n_om, d_rec.data_ptr(), d_lk.data_ptr(), d_scale.data_ptr(), low,
-                               high, reference, result.data_ptr())
-        need = int(lib.lh_ge2_workspace_bytes(self.struct, prob))
-        if need == 0 and n_om and len(pts):
+    def apply_device(self, sources, positions, looks, out_scale, window=None, *,
+                     zero_frequency=False, stream=None):
+        """One problem: device (OM, frequency) complex128 spectrum."""
+        return self.apply_batch([(sources, positions, looks, out_scale, window)],
+                                zero_frequency=zero_frequency, stream=stream)[0]
+
+    def apply_batch(self, items, *, zero_frequency=False, stream=None):
+        """Several problems (``(sources, positions, looks, out_scale, window)`` each)
+        on this table in one set of launches: a list of device (OM, frequency)
+        complex128 spectra, each equal to the problem applied alone."""
+        import torch
+        lib = _lib.load()
+        dev = self.device
+        if not items:
+            return []
+        prepared = [self._prepare(*it, zero_frequency) for it in items]
+        host = np.concatenate([np.concatenate([q[k].ravel() for k in ("pts", "rec", "lk", "scale")])
+                               for q in prepared])
+        d_geom = _lib.upload(host, torch.float64, dev)
+        sizes = [q["n_om"] * q["W"] for q in prepared]
+        result = torch.empty(max(sum(sizes), 1), dtype=torch.complex128, device=dev)
+        probs = (_lib.Ge2Problem * len(prepared))()
+        at, r_at = d_geom.data_ptr(), 0
+        for i, q in enumerate(prepared):
+            probs[i], at = self._problem(q, at, result.data_ptr() + 16 * r_at)
+            r_at += sizes[i]
+        n = len(prepared)
+        need = int(lib.lh_ge2_batch_workspace_bytes(self.struct, probs, n))
+        if need == 0:
             raise ValueError("order >=2 problem rejected by the device library")
         if self._workspace is None or self._workspace.numel() < need:
-            self._workspace = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+            self._workspace = torch.empty(need, dtype=torch.uint8, device=dev)
+        slots = C.create_string_buffer(int(lib.lh_ge2_batch_slot_bytes(n)))  # pageable staging
         s = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
-        _lib.check(lib.lh_ge2_apply(self.struct, prob, self._workspace.data_ptr(),
-                                    self._workspace.numel(), s), "lh_ge2_apply")
-        self._keep = (d_pts, d_rec, d_lk, d_scale, ch)  # alive until the stream runs
-        return result
+        _lib.check(lib.lh_ge2_apply_batch(self.struct, probs, n, self._workspace.data_ptr(),
+                                          self._workspace.numel(), slots, s),
+                   "lh_ge2_apply_batch")
+        self._keep = (d_geom, [q["ch"] for q in prepared])  # alive until the stream runs
+        out, r_at = [], 0
+        for q, size in zip(prepared, sizes):
+            out.append(result[r_at:r_at + size].view(q["n_om"], q["W"]))
+            r_at += size
+        return out
 
 
 def apply_folded(table: Ge2Table, sources: AxialSources, positions, looks, area, window, *,

@@ -300,24 +300,38 @@ class ShowerTransport:
     # -- order >=2 helpers ----------------------------------------------------
     def _apply_device(self, points, channels, reference, frame, oms, *, zero_frequency):
         """``apply_folded`` (``shower/ge2.py:99-119``) for the OMs ``oms``: device (OM, W)."""
-        import torch
+        return self._apply_many([(points, channels, reference, frame, oms)],
+                                zero_frequency=zero_frequency)[0]
+
+    def _apply_many(self, requests, *, zero_frequency):
+        """``_apply_device`` of several ``(points, channels, reference, frame, oms)``
+        requests (the events of a batch) in one batched launch set per table."""
         T = self.tables
-        centre, axis, first, second = frame
-        area = T.areas[oms]
-        same = all(len(p) == len(points[0]) and np.array_equal(p, points[0]) for p in points[1:])
-        if same:
-            src = AxialSources(points[0], channels, np.full(len(points), reference),
-                               (centre, first, second, axis), T.source_degree, T.azimuthal_degree)
-            return T.ge2.apply_device(src, T.positions[oms], T.looks[oms], area, T.radial,
-                                      zero_frequency=zero_frequency)
-        total = None
-        for b in range(len(points)):
-            src = AxialSources(points[b], channels[b][None], np.array([reference]),
-                               (centre, first, second, axis), T.source_degree, T.azimuthal_degree)
-            part = T.ge2.band(b).apply_device(src, T.positions[oms], T.looks[oms], area,
-                                              T.radial, zero_frequency=zero_frequency)
-            total = part if total is None else total + part
-        return total
+        out = [None] * len(requests)
+        joint, split = [], []
+        for i, (points, channels, reference, frame, oms) in enumerate(requests):
+            centre, axis, first, second = frame
+            basis = (centre, first, second, axis)
+            args = (T.positions[oms], T.looks[oms], T.areas[oms], T.radial)
+            if all(len(p) == len(points[0]) and np.array_equal(p, points[0]) for p in points[1:]):
+                src = AxialSources(points[0], channels, np.full(len(points), reference), basis,
+                                   T.source_degree, T.azimuthal_degree)
+                joint.append((i, (src,) + args))
+            else:  # node bands with their own points: one band-view problem per band
+                for b in range(len(points)):
+                    src = AxialSources(points[b], channels[b][None], np.array([reference]), basis,
+                                       T.source_degree, T.azimuthal_degree)
+                    split.append((i, b, (src,) + args))
+        if joint:
+            for (i, _), res in zip(joint, T.ge2.apply_batch([it for _, it in joint],
+                                                            zero_frequency=zero_frequency)):
+                out[i] = res
+        for b in sorted({b for _, b, _ in split}):
+            part = [(i, it) for i, bb, it in split if bb == b]
+            for (i, _), res in zip(part, T.ge2.band(b).apply_batch(
+                    [it for _, it in part], zero_frequency=zero_frequency)):
+                out[i] = res if out[i] is None else out[i] + res
+        return out
 
     def __call__(self, source, *, time_origin_ns=None, selection_extra_charge=None,
                  receivers=None):
@@ -421,6 +435,7 @@ class ShowerTransport:
             ev.used, ev.tail, ev.reach = used, tail, np.flatnonzero(used > 0)
         stage("radial_window")
         # ---- predictor (shower/ge2.py:70-96) and its zero-frequency charge (device)
+        predict = []
         for ev in events:
             ev.predicted = np.zeros(n)
             if not len(ev.reach):
@@ -451,8 +466,10 @@ class ShowerTransport:
                 c_channels.append(summed[:, :, None])
             c_ch = (np.stack(c_channels) if all(len(p) == len(c_points[0]) for p in c_points[1:])
                     else c_channels)
-            ev.pending["predicted"] = self._apply_device(c_points, c_ch, ev.reference, ev.frame,
-                                                         ev.reach, zero_frequency=True)
+            predict.append((ev, (c_points, c_ch, ev.reference, ev.frame, ev.reach)))
+        for (ev, _), res in zip(predict, self._apply_many([r for _, r in predict],
+                                                          zero_frequency=True)):
+            ev.pending["predicted"] = res
         # ---- clocks (shower/api.py:455-477) and module selection distances (device)
         time_width = float(np.ptp(edges))
         for k, ev in enumerate(events):
@@ -564,6 +581,7 @@ class ShowerTransport:
             raise MemoryError("order-1 tables overflowed their device capacity")
         stage("order1")
         # ---- exact zero-frequency >=2 where the decision needs it (shower/api.py:488-525)
+        exact_req = []
         for ev in events:
             ev.pending["ge2"] = {}
             prompt_charge = ev.charge.sum(axis=1)
@@ -575,9 +593,11 @@ class ShowerTransport:
             ev.candidate = cand
             ids = np.flatnonzero(cand)
             if len(ids):
-                ev.pending["exact"] = (ids, self._apply_device(
-                    ev.points, self._zero_only(ev.channels), ev.reference, ev.frame, ids,
-                    zero_frequency=True))
+                exact_req.append((ev, ids))
+        for (ev, ids), res in zip(exact_req, self._apply_many(
+                [(ev.points, self._zero_only(ev.channels), ev.reference, ev.frame, ids)
+                 for ev, ids in exact_req], zero_frequency=True)):
+            ev.pending["exact"] = (ids, res)
         for ev in events:
             exact = np.zeros(n)
             if "exact" in ev.pending:
@@ -609,7 +629,7 @@ class ShowerTransport:
             ev.active = active
         stage("ge2_exact_zero")
         # ---- full frequencies for the active OMs, the prompt bins they lack, the readout
-        rows, row_ev = [], []
+        row_ev = []
         for k, ev in enumerate(events):
             ev.spectrum = np.zeros((len(omega), n), complex)
             ids = np.flatnonzero(ev.active)
@@ -622,19 +642,24 @@ class ShowerTransport:
                 ev.bins1[missing] = b1m.cpu().numpy()[missing]
             work = np.flatnonzero(ev.active & (ev.used > 0))
             if len(work):
-                spec = self._apply_device(ev.points, ev.channels, ev.reference, ev.frame, work,
-                                          zero_frequency=False)
-                ev.pending["spec"] = (work, spec)
-                phase = _lib.upload(np.exp(-1j * np.outer(ev.origins[work], omega)),
-                                    torch.complex128, dev)
-                rel = spec * phase
-                # the stored zero frequency is the exact >=2 charge (shower/api.py:584)
-                rel[:, 0] = _lib.upload(ev.charge[work, 2], torch.complex128, dev)
-                rel = rel.to(torch.complex64)
-                rows.append(rel)
                 row_ev.append((k, work))
-        if rows:
-            bins2, _ = T.readout.bins(torch.cat(rows), mode=cfg.readout_mode)
+        if row_ev:
+            specs = self._apply_many([(events[k].points, events[k].channels, events[k].reference,
+                                       events[k].frame, work) for k, work in row_ev],
+                                     zero_frequency=False)
+            # relative-time spectra e^{-i w origin} N(w); the stored zero frequency is
+            # the exact >=2 charge (shower/api.py:584)
+            origin = np.concatenate([events[k].origins[work] for k, work in row_ev])
+            zero = np.concatenate([events[k].charge[work, 2] for k, work in row_ev])
+            phase = np.exp(-1j * np.outer(origin, omega))
+            phase[:, 0] = 0.0
+            packed = _lib.upload(np.concatenate([phase, zero[:, None].astype(complex)], axis=1),
+                                 torch.complex128, dev)
+            rel = torch.cat(specs) * packed[:, :-1]
+            rel[:, 0] = packed[:, -1]
+            for (k, work), spec in zip(row_ev, specs):
+                events[k].pending["spec"] = (work, spec)
+            bins2, _ = T.readout.bins(rel.to(torch.complex64), mode=cfg.readout_mode)
             bins2 = bins2.cpu().numpy().astype(float)
         responses = []
         row = 0

@@ -77,3 +77,38 @@ def test_device_apply_all_points_random_channels_vs_oracle():
     out = table.apply(src, g["om_positions_m"][oms], g["om_looks"][oms], g["om_area_m2"][oms],
                       g["radial_window_m"])
     assert np.abs(out - ref).max() <= GE2_TOL * np.abs(ref).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("zero_frequency", [True, False])
+def test_batched_problems_equal_alone(zero_frequency):
+    """Problems of one batched launch (different OM subsets, sources, frames,
+    one without points) equal each problem applied alone, bit for bit: the
+    point chunks are summed in the same fixed order either way."""
+    from lighthit_b200.ge2 import AxialSources, Ge2Table
+    g, t, frame = fixture()
+    table = Ge2Table(t, g["alpha"], source_degree=8, azimuthal_degree=2)
+    rng = np.random.default_rng(17)
+    pts = points(g, frame, "zero")
+    P = len(pts)
+    basis = (frame["centre"], frame["first"], frame["second"], frame["axis"])
+    items = []
+    for k, oms in enumerate([np.arange(48), np.arange(3, 40, 5), np.array([7])]):
+        ch = (rng.normal(size=(3, P, 39, 65)) + 1j * rng.normal(size=(3, P, 39, 65))).astype(
+            np.complex64) * np.abs(g["zero_channels"][:, :, :, :1])
+        shifted = tuple(np.asarray(v) + (0.3 * k * frame["axis"] if i == 0 else 0)
+                        for i, v in enumerate(basis))
+        src = AxialSources(pts + 0.3 * k * frame["axis"], ch, np.array([0.0, 0.1 * k, 0.0]),
+                           shifted, 8, 2)
+        items.append((src, g["om_positions_m"][oms], g["om_looks"][oms], g["om_area_m2"][oms],
+                      g["radial_window_m"]))
+    empty = AxialSources(np.zeros((0, 3)), np.zeros((3, 0, 39, 65), np.complex64),
+                         np.zeros(3), basis, 8, 2)
+    items.append((empty,) + items[1][1:])
+    together = [r.cpu().numpy() for r in table.apply_batch(items, zero_frequency=zero_frequency)]
+    for it, got in zip(items, together):
+        alone = table.apply_device(*it, zero_frequency=zero_frequency).cpu().numpy()
+        assert got.shape == alone.shape
+        assert np.array_equal(got, alone)
+    assert not np.any(together[-1])
+    assert np.any(together[0])

@@ -81,3 +81,30 @@ def test_ge2_spectrum_matches_reference(route_response):
     got = r.spectrum_ge2_pe[:, act]
     scale = np.abs(ref).max(axis=0)
     assert (np.abs(got - ref).max(axis=0) / scale).max() < 1e-3
+
+
+def test_batch_equals_alone():
+    """Showers routed as one batch equal each shower routed alone (shared launches
+    only): the golden shower and two displaced, rescaled copies."""
+    from lighthit_b200.shower import ShowerTables, ShowerTransport
+    el = np.load(GOLDEN / "order0_c0.npz")
+    base = {k: np.array(el[k]) for k in ("start_m", "direction", "length_m", "coefficient0",
+                                         "coefficient2", "beta", "start_ns", "end_ns")}
+    sources = [base]
+    for k, (shift, gain) in enumerate([((4.0, -3.0, 2.0), 0.5), ((-6.0, 2.0, -1.0), 2.0)]):
+        s = dict(base)
+        s["start_m"] = base["start_m"] + np.asarray(shift)
+        s["coefficient0"] = base["coefficient0"] * gain
+        s["coefficient2"] = base["coefficient2"] * gain
+        s["start_ns"] = base["start_ns"] + 5.0 * (k + 1)
+        s["end_ns"] = base["end_ns"] + 5.0 * (k + 1)
+        sources.append(s)
+    route = ShowerTransport(ShowerTables.synthetic("c0"))
+    together = route.batch(sources)
+    for src, got in zip(sources, together):
+        alone = route(src)
+        assert np.array_equal(got.active, alone.active)
+        assert np.array_equal(got.time_origin_ns, alone.time_origin_ns)
+        scale = max(np.abs(alone.charge_pe).max(), 1e-300)
+        assert np.abs(got.components_pe - alone.components_pe).max() <= 1e-12 * scale * 10
+        assert np.abs(got.charge_pe - alone.charge_pe).max() <= 1e-12 * scale
