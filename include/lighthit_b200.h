@@ -412,6 +412,45 @@ typedef struct {
 
 int lh_om_geometry(const lh_om_geometry_problem* geometry, void* stream);
 
+/* ------------------------------------------------------------------ radial window
+ * Replaces the radial-window pass of ShowerTransport (shower/api.py:322-340 with
+ * the far-tail screen of shower_basis.py:408-439): for every (event, node band,
+ * OM) the number of basis points closer than radial_low and farther than
+ * radial_high (float64, bit-identical to the reference's NumPy distances), and the
+ * far-tail sum  sum_far photons_c exp(interp(r, att_radius, att_log)) / (4 pi r^2),
+ * photons_c = photon_scale |channel_c(0, 0)| / efficiency_band.
+ * Basis points are in the axis frame (z, x, y) of their event, as the source
+ * compile writes them; world = ((centre + z axis) + x first) + y second. */
+typedef struct {
+  int32_t n_points[8];          /* basis points of each node band                     */
+  int32_t capacity;             /* points stride between bands                        */
+  const double* points;         /* [band][capacity][3] (z, x, y)                      */
+  const float* channels;        /* complex64 [band][capacity][channel_stride/2]       */
+  int32_t channel_stride;       /* floats per point (2 nch n_omega)                   */
+  double centre[3], axis[3], first[3], second[3];
+} lh_window_event;
+
+typedef struct {
+  int32_t n_om, n_bands;
+  const double* om_pos;         /* [n_om][3]                                          */
+  double radial_low, radial_high;
+  int32_t n_att;
+  const double* att_radius;     /* [n_att] ascending                                  */
+  const double* att_log;        /* [n_att]                                            */
+  double photon_scale;          /* sqrt(4 pi)                                         */
+  double efficiency[8];         /* of each node band                                  */
+  int32_t* n_near;              /* [event][band][n_om]                                */
+  int32_t* n_far;               /* [event][band][n_om]                                */
+  double* far_sum;              /* [event][band][n_om]                                */
+} lh_radial_window_problem;
+
+/* `events` (host memory, n_events <= 65535 / n_bands) is copied on the stream
+ * into the workspace (lh_window_slot_bytes(n_events) bytes of device memory);
+ * pageable `events` may be reused when the call returns. */
+size_t lh_window_slot_bytes(int32_t n_events);
+int lh_radial_window(const lh_radial_window_problem* problem, const lh_window_event* events,
+                     int32_t n_events, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

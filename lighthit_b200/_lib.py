@@ -62,6 +62,19 @@ class Ge2Problem(C.Structure):
                 ("radial_high", C.c_double), ("reference_ns", C.c_double), ("result", P)]
 
 
+class WindowEvent(C.Structure):
+    _fields_ = [("n_points", C.c_int32 * 8), ("capacity", C.c_int32), ("points", P),
+                ("channels", P), ("channel_stride", C.c_int32), ("centre", C.c_double * 3),
+                ("axis", C.c_double * 3), ("first", C.c_double * 3), ("second", C.c_double * 3)]
+
+
+class RadialWindowProblem(C.Structure):
+    _fields_ = [("n_om", C.c_int32), ("n_bands", C.c_int32), ("om_pos", P),
+                ("radial_low", C.c_double), ("radial_high", C.c_double), ("n_att", C.c_int32),
+                ("att_radius", P), ("att_log", P), ("photon_scale", C.c_double),
+                ("efficiency", C.c_double * 8), ("n_near", P), ("n_far", P), ("far_sum", P)]
+
+
 class Order0Optics(C.Structure):
     _fields_ = [("n_om", C.c_int32), ("om_pos", P), ("om_look", P), ("om_area", P),
                 ("om_radius", P), ("n_alpha", C.c_int32), ("alpha", P),
@@ -148,6 +161,9 @@ SIGNATURES = {
                                              C.POINTER(FlashBatch), P]),
     "lh_ge2_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem)]),
     "lh_ge2_apply": (C.c_int, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem), P, C.c_size_t, P]),
+    "lh_window_slot_bytes": (C.c_size_t, [C.c_int32]),
+    "lh_radial_window": (C.c_int, [C.POINTER(RadialWindowProblem), C.POINTER(WindowEvent),
+                                   C.c_int32, P, C.c_size_t, P]),
     "lh_ge2_batch_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem),
                                                   C.c_int32]),
     "lh_ge2_batch_slot_bytes": (C.c_size_t, [C.c_int32]),
@@ -209,10 +225,27 @@ def upload(array, dtype, device):
     np_dtype = {torch.float64: np.float64, torch.int32: np.int32, torch.int64: np.int64,
                 torch.complex128: np.complex128, torch.complex64: np.complex64,
                 torch.float32: np.float32}[dtype]
-    host = torch.from_numpy(np.ascontiguousarray(array, dtype=np_dtype))
     if torch.device(device).type != "cuda":
-        return host.to(device)
-    return host.pin_memory().to(device, non_blocking=True)
+        return torch.from_numpy(np.array(array, dtype=np_dtype, copy=True)).to(device)
+    array = np.asarray(array)
+    host = torch.empty(array.shape, dtype=dtype, pin_memory=True)
+    host.numpy()[...] = array  # one conversion copy straight into pinned memory
+    return host.to(device, non_blocking=True)
+
+
+def upload_parts(parts, dtype, device):
+    """Several host arrays -> one flat device tensor (their raveled concatenation)
+    through one pinned buffer and one asynchronous copy; returns it and the offsets."""
+    import numpy as np
+    import torch
+    sizes = [int(np.size(a)) for a in parts]
+    offsets = np.zeros(len(parts) + 1, np.int64)
+    offsets[1:] = np.cumsum(sizes)
+    host = torch.empty(int(offsets[-1]), dtype=dtype, pin_memory=torch.device(device).type == "cuda")
+    flat = host.numpy()
+    for a, lo, hi in zip(parts, offsets[:-1], offsets[1:]):
+        flat[lo:hi] = np.ravel(a)
+    return host.to(device, non_blocking=True), offsets
 
 
 def stream_ptr(stream):

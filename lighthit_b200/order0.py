@@ -120,12 +120,11 @@ class ElementBatch:
         offsets[1:] = np.cumsum(counts)
         self.offsets = offsets
         self.n_elements = n = int(offsets[-1])
-        parts = [np.concatenate([np.asarray(_field(e, name), float).ravel() for e in events])
-                 if events else np.zeros(0) for name in ELEMENT_FIELDS]
-        flat = _lib.upload(np.concatenate(parts + [offsets.astype(float)]), torch.float64, device)
+        parts = [_field(e, name) for name in ELEMENT_FIELDS for e in events]
+        flat, _ = _lib.upload_parts(parts + [offsets], torch.float64, device)
         self._t = {}
         pos = 0
-        for name, part in zip(ELEMENT_FIELDS, parts):
+        for name in ELEMENT_FIELDS:
             w = self.WIDTH.get(name, 1)
             view = flat[pos:pos + n * w]
             self._t[name] = view.view(n, w) if w > 1 else view

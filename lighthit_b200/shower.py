@@ -154,6 +154,9 @@ class ShowerTables:
         log_factor = (np.log(np.exp(-np.outer(radius, self.absorption - lowest)) @ w / w.sum())
                       - lowest * radius)
         self._attenuation = (radius, log_factor)
+        self._att = (torch.tensor(radius, dtype=torch.float64, device=self.device),
+                     torch.tensor(log_factor, dtype=torch.float64, device=self.device))
+        self._window_ws = None
         self.n_om = n
 
     @classmethod
@@ -182,6 +185,49 @@ class ShowerTables:
             _lib.check(_lib.load().lh_om_geometry(C.byref(g), sp), "lh_om_geometry")
             out.append(res)
         return out[0].cpu().numpy(), out[1].cpu().numpy()
+
+    def radial_window(self, compiled):
+        """Per (event, node band, OM): basis points inside / beyond the radial range
+        and the far-tail photon sum, for compiled sources ``(points, channels,
+        n_points (host), frame)`` (device points and channels): three host arrays."""
+        import torch
+        dev = self.device
+        n, nb, ne = self.n_om, len(self.fold_bands), len(compiled)
+        events = (_lib.WindowEvent * ne)()
+        for e, (points, channels, npts, frame) in enumerate(compiled):
+            E = events[e]
+            for b in range(nb):
+                E.n_points[b] = int(npts[b])
+            E.capacity = int(points.shape[1])
+            E.points, E.channels = points.data_ptr(), channels.data_ptr()
+            E.channel_stride = 2 * int(channels.shape[2]) * int(channels.shape[3])
+            centre, axis, first, second = frame
+            for k in range(3):
+                E.centre[k], E.axis[k] = float(centre[k]), float(axis[k])
+                E.first[k], E.second[k] = float(first[k]), float(second[k])
+        cells = ne * nb * n
+        out = torch.empty(16 * cells, dtype=torch.uint8, device=dev)  # n_near, n_far, far_sum
+        S = _lib.RadialWindowProblem()
+        S.n_om, S.n_bands, S.om_pos = n, nb, self._pos.data_ptr()
+        S.radial_low, S.radial_high = self.radial
+        S.n_att, S.att_radius, S.att_log = len(self._attenuation[0]), self._att[0].data_ptr(), \
+            self._att[1].data_ptr()
+        S.photon_scale = float(np.sqrt(4 * np.pi))
+        for b, band in enumerate(self.fold_bands):
+            S.efficiency[b] = float(self.efficiency[band])
+        S.n_near, S.n_far, S.far_sum = (out.data_ptr(), out.data_ptr() + 4 * cells,
+                                        out.data_ptr() + 8 * cells)
+        lib = _lib.load()
+        need = int(lib.lh_window_slot_bytes(ne))
+        if self._window_ws is None or self._window_ws.numel() < need:
+            self._window_ws = torch.empty(need, dtype=torch.uint8, device=dev)
+        sp = _lib.stream_ptr(torch.cuda.current_stream(dev))
+        _lib.check(lib.lh_radial_window(C.byref(S), events, ne, self._window_ws.data_ptr(),
+                                        self._window_ws.numel(), sp), "lh_radial_window")
+        host = out.cpu().numpy()
+        return (host[:4 * cells].view(np.int32).reshape(ne, nb, n),
+                host[4 * cells:8 * cells].view(np.int32).reshape(ne, nb, n),
+                host[8 * cells:].view(np.float64).reshape(ne, nb, n))
 
     def attenuation(self, distance):
         radius, log_factor = self._attenuation
@@ -410,24 +456,16 @@ class ShowerTransport:
         stage("source_compile")
         # ---- radial windows (shower/api.py:322-340, shower_basis.py:408-439)
         weight_ratio = float(np.sum(T.fold_scale) / np.sum(T.fold_scale[T.fold_bands]))
-        for ev in events:
+        n_near, n_far, far_sum = T.radial_window(
+            [(c[0], c[1], ev.npts, ev.frame) for c, ev in zip(compiled, events)])
+        for k, ev in enumerate(events):
             used = np.zeros(n, np.int64)
-            near = np.zeros(n, bool)
             tail = np.zeros(n)
-            radius = None
             for b, band in enumerate(T.fold_bands):
-                photons = np.sqrt(4 * np.pi) * np.abs(ev.zero_ch[b][:, 0]) / T.efficiency[band]
-                if radius is None or not np.array_equal(ev.points[b], ev.points[b - 1]):
-                    radius = np.sqrt(((ev.points[b][None] - T.positions[:, None]) ** 2).sum(axis=2))
-                    n_near = np.count_nonzero(radius < low, axis=1)
-                    om, pt = np.nonzero(radius > high)
-                    n_far = np.bincount(om, minlength=n)
-                    far_factor = T.attenuation(radius[om, pt]) / (4 * np.pi * radius[om, pt] ** 2)
-                used = np.maximum(used, len(ev.points[b]) - n_near - n_far)
-                near |= n_near > 0
+                used = np.maximum(used, int(ev.npts[b]) - n_near[k, b] - n_far[k, b])
                 tail += weight_ratio * (10 * T.areas * T.peak_acceptance * T.efficiency[band]
-                                        * np.bincount(om, weights=photons[pt] * far_factor,
-                                                      minlength=n))
+                                        * far_sum[k, b])
+            near = np.any(n_near[k] > 0, axis=0)
             if np.any(near):
                 raise NotImplementedError("basis points inside the table's inner radius need the "
                                           "near-field clamp (near_field.py), not on the device "
@@ -459,8 +497,9 @@ class ShowerTransport:
                                  1.0 / count[inverse])
                 centroid = np.stack([np.bincount(inverse, weights=share * coords[:, k],
                                                  minlength=groups) for k in range(3)], axis=1)
-                summed = np.zeros((groups, ev.zero_ch[b].shape[1]), complex)
-                np.add.at(summed, inverse, ev.zero_ch[b])
+                order = np.argsort(inverse, kind="stable")  # group sums in point order
+                starts = np.searchsorted(inverse[order], np.arange(groups))
+                summed = np.add.reduceat(ev.zero_ch[b][order].astype(complex), starts, axis=0)
                 c_points.append(centre + centroid[:, :1] * axis + centroid[:, 1:2] * e1
                                 + centroid[:, 2:3] * e2)
                 c_channels.append(summed[:, :, None])

@@ -96,12 +96,11 @@ class SourceCompiler:
         self._omega = torch.tensor(self.omega, dtype=torch.float64, device=self.device)
         self._workspace = None
 
-    def problem(self, arrays, frame, n_el, order, fractions, weights, reference, z_origin,
-                n_slices, kmax):
+    def _template(self):
+        """The event-independent fields (bands, harmonic layout, basis settings)."""
+        if getattr(self, "_fixed", None) is not None:
+            return self._fixed
         p = _lib.SourceProblem()
-        p.n_el = n_el
-        for name in ("start", "direction", "length", "c0", "c2", "beta", "t0", "t1"):
-            setattr(p, name, arrays[name].data_ptr())
         nb = len(self.wavelengths)
         p.n_bands = nb
         s0 = 1.0 / self.wavelengths ** 2
@@ -109,9 +108,6 @@ class SourceCompiler:
         for k in range(nb):
             p.band_s0[k], p.band_s2[k] = float(s0[k]), float(s2[k])
             p.band_phase[k], p.band_scale[k] = float(self.phase[k]), float(self.scale[k])
-        centre, axis, first, second = frame
-        for k in range(3):
-            p.centre[k], p.first[k], p.second[k], p.axis[k] = centre[k], first[k], second[k], axis[k]
         p.degree, p.max_m, p.nch = self.degree, self.max_m, self.nch
         for k, v in enumerate(self.starts):
             p.starts[k] = int(v)
@@ -119,16 +115,28 @@ class SourceCompiler:
             p.channel_degree[k] = int(v)
         for k, (a, b) in enumerate(zip(self.aa.ravel(), self.bb.ravel())):
             p.aa[k], p.bb[k] = float(a), float(b)
-        p.element_order = order
-        for k in range(order):
-            p.node_fraction[k], p.node_weight[k] = float(fractions[k]), float(weights[k])
         s = self.settings
         p.cell_m, p.stencil_m = s.cell_m, s.stencil_m
         p.stencil_threshold_m, p.time_step_ns = s.stencil_threshold_m, s.time_step_ns
-        p.reference_ns, p.z_origin = reference, z_origin
-        p.n_slices, p.kmax = n_slices, kmax
         p.n_omega = len(self.omega)
         p.omega = self._omega.data_ptr()
+        self._fixed = p
+        return p
+
+    def problem(self, arrays, frame, n_el, order, fractions, weights, reference, z_origin,
+                n_slices, kmax):
+        p = _lib.SourceProblem.from_buffer_copy(self._template())
+        p.n_el = n_el
+        for name in ("start", "direction", "length", "c0", "c2", "beta", "t0", "t1"):
+            setattr(p, name, arrays[name].data_ptr())
+        centre, axis, first, second = frame
+        for k in range(3):
+            p.centre[k], p.first[k], p.second[k], p.axis[k] = centre[k], first[k], second[k], axis[k]
+        p.element_order = order
+        for k in range(order):
+            p.node_fraction[k], p.node_weight[k] = float(fractions[k]), float(weights[k])
+        p.reference_ns, p.z_origin = reference, z_origin
+        p.n_slices, p.kmax = n_slices, kmax
         return p
 
     def compile(self, elements, frame=None, *, stream=None, check=True, status=None,
