@@ -180,7 +180,7 @@ LH_DEVICE float o0_acceptance(const float* alpha, int n_alpha, float x, float al
   float previous = 1.0f, current = x;
   if (n_alpha > 1) result += 3.0f * alpha[1] * current * inv4pi;
   for (int ell = 2; ell < n_alpha; ++ell) {
-    float value = ((2 * ell - 1) * x * current - (ell - 1) * previous) / ell;
+    float value = ((2 * ell - 1) * x * current - (ell - 1) * previous) * (1.0f / ell);
     result += (2 * ell + 1) * alpha[ell] * value * inv4pi;
     previous = current;
     current = value;
@@ -352,6 +352,7 @@ __global__ void __launch_bounds__(1024) order0_scan_kernel(int32_t n_keys, O0Wor
 
 struct O0Shared {
   double gx[kO0MaxOrder], gw[kO0MaxOrder];
+  double sin_psi[kO0MaxOrder], cos_psi[kO0MaxOrder];  // sin/cos(pi/2 gx): s-node map
   float alpha[kO0MaxAlpha];
   O0Pair pair[kO0Chunk];
   double warp_charge[kO0Threads / 32];
@@ -359,7 +360,7 @@ struct O0Shared {
   int n_combos;
 };
 
-__global__ void __launch_bounds__(kO0Threads)
+__global__ void __launch_bounds__(kO0Threads, 3)
 order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W) {
   extern __shared__ __align__(16) unsigned char o0_smem[];
   O0Shared& S = *reinterpret_cast<O0Shared*>(o0_smem);
@@ -373,6 +374,7 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
   for (int k = tid; k < order; k += blockDim.x) {
     S.gx[k] = O.gauss_x[k];
     S.gw[k] = O.gauss_w[k];
+    sincospi(0.5 * O.gauss_x[k], &S.sin_psi[k], &S.cos_psi[k]);
   }
   for (int k = tid; k < O.n_alpha; k += blockDim.x) S.alpha[k] = (float)O.alpha[k];
   double pmin, pmax;
@@ -582,8 +584,7 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
       const double sa = scuts[sp], sb = scuts[sp + 1];
       if (sa >= sb) continue;
       for (int j = 0; j < order; ++j) {
-        double sin_psi, cos_psi;
-        sincospi(0.5 * S.gx[j], &sin_psi, &cos_psi);
+        const double sin_psi = S.sin_psi[j], cos_psi = S.cos_psi[j];
         const double s = (sa + sb) / 2 + (sb - sa) / 2 * sin_psi;
         const double ds = (sb - sa) / 2 * cos_psi * kPi / 2 * S.gw[j];
         const double along = z - s, W2 = rho * rho + along * along, Bq = W2 - radius * radius;
@@ -629,22 +630,26 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
           const float mid = (float)((pa + pb) / 2), hw = (float)((pb - pa) / 2);
           float integral = 0.0f;
           for (int jp = 0; jp < order; ++jp) {
+            // arguments lie in [0, pi]: the hardware approximations (absolute error
+            // near 2^-21) are well inside the float32 integrand's budget
             float s_eta, c_eta;
-            sincosf(mid + hw * (float)S.gx[jp], &s_eta, &c_eta);
+            __sincosf(mid + hw * (float)S.gx[jp], &s_eta, &c_eta);
             const float phi = half_f * s_eta;
             const float dphi = half_f * c_eta * hw * (float)S.gw[jp];
-            float ss, cp;
-            sincosf(phi, &ss, &cp);
-            const float sh = sinf(0.5f * phi);
+            // sin(phi), cos(phi) from the half angle: 2 sin^2(phi/2) = 1 - cos(phi)
+            // without cancellation near phi = 0
+            float sh, chh;
+            __sincosf(0.5f * phi, &sh, &chh);
+            const float ss = 2.0f * sh * chh, cp = 1.0f - 2.0f * sh * sh;
             const float E = E0 - Sa * (2.0f * sh * sh);
             const float D = R2 - (sin2W2 * ss * ss + E * E);
             const float dot = along_cos + rho_sin * cp;
-            const float distance = B_f / (dot + sqrtf(fmaxf(D, 0.0f)));
+            const float distance = __fdividef(B_f, dot + sqrtf(fmaxf(D, 0.0f)));
             const float x1 = cos_f * axial + sin_f * (cp * across + ss * side);
             const float x2 = cos_f * axial + sin_f * (cp * across - ss * side);
             const float accept = o0_acceptance(S.alpha, O.n_alpha, x1, alpha_abs, bad_acceptance) +
                                  o0_acceptance(S.alpha, O.n_alpha, x2, alpha_abs, bad_acceptance);
-            integral += dphi * accept * expf(-absorption_f * distance);
+            integral += dphi * accept * __expf(-absorption_f * distance);
           }
           const double value = scale * ds * (double)integral * (1.0 / (2 * kPi));
           charge += value;

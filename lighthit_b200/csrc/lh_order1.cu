@@ -52,9 +52,10 @@ LH_DEVICE uint64_t o1_mix(uint64_t v) {
 // Insert `key` (>= 0) into an open-addressing table of `capacity` (power of
 // two) slots holding -1 when free. Returns the slot, or -1 when full; `fresh`
 // tells whether this call claimed it.
-LH_DEVICE int64_t o1_insert(long long* keys, int64_t capacity, long long key, bool& fresh) {
+LH_DEVICE int64_t o1_insert(long long* keys, int64_t capacity, long long key, bool& fresh,
+                            bool ordered = false) {
   const uint64_t mask = (uint64_t)capacity - 1;
-  uint64_t slot = o1_mix((uint64_t)key) & mask;
+  uint64_t slot = (ordered ? (uint64_t)key : o1_mix((uint64_t)key)) & mask;
   fresh = false;
   for (int64_t probe = 0; probe < capacity; ++probe) {
     long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(keys + slot),
@@ -105,107 +106,220 @@ LH_DEVICE O1Subseg o1_subseg(const lh_order1_elements& E, int64_t i, int64_t ia,
   return s;
 }
 
-// One thread per (sub-segment, ring node): compress_subsegments
-// (_prompt_numba.py:1122-1232) with the ring rotation evaluated directly.
+// Sum of `v` over the lanes of a warp that share a key (their __match_any_sync
+// mask minus the calling lane is `rest`), valid in the group's lowest lane.
+// Every lane of the warp calls it with the same `rounds` (the largest group
+// size minus one), so the shuffles stay convergent.
+LH_DEVICE double o1_group_sum(double v, unsigned rest, int rounds) {
+  double acc = v;
+  for (int r = 0; r < rounds; ++r) {
+    const int src = rest ? __ffs(rest) - 1 : (int)(threadIdx.x & 31);
+    const double got = __shfl_sync(0xffffffffu, v, src);
+    if (rest) {
+      acc += got;
+      rest &= rest - 1;
+    }
+  }
+  return acc;
+}
+
+constexpr int kO1RingBlock = 16;  // ring nodes per thread
+
+// One thread per (sub-segment, block of kO1RingBlock ring nodes):
+// compress_subsegments (_prompt_numba.py:1122-1232) with the ring rotation
+// evaluated directly. The lanes of a warp hold consecutive sub-segments and
+// take the same ring node together, so nodes that land in the same (cell,
+// pixel) (neighbouring steps of a track or shower) are summed in registers
+// first: one hash insert and one set of moment atomics per distinct key and warp.
 __global__ void o1_ring_kernel(const lh_order1_config C, const lh_order1_elements E,
                                const int64_t* subseg_offset, int64_t n_subseg,
                                long long* keys, int64_t capacity, double* rows,
                                int32_t* status) {
-  const int64_t total = n_subseg * C.ring_nodes;
   const int n_pix = 6 * C.pixel_face * C.pixel_face;
   const double golden = 0.6180339887498949;
   const double two_pi = 2.0 * kPi;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t sub = k / C.ring_nodes;
-    const int q = (int)(k - sub * C.ring_nodes);
-    // element of this sub-segment: last i with subseg_offset[i] <= sub
-    int64_t lo = 0, hi = E.n_el;
-    while (hi - lo > 1) {
-      int64_t mid = (lo + hi) >> 1;
-      if (subseg_offset[mid] <= sub) lo = mid; else hi = mid;
+  const int lane = threadIdx.x & 31;
+  const int64_t n_pad = (n_subseg + 31) & ~(int64_t)31;  // warps never straddle node blocks
+  const int n_blocks = (C.ring_nodes + kO1RingBlock - 1) / kO1RingBlock;
+  const int64_t total = n_pad * n_blocks;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += stride) {
+    const int64_t sub = k % n_pad;
+    const int q_begin = (int)(k / n_pad) * kO1RingBlock;
+    const int q_end = min(q_begin + kO1RingBlock, C.ring_nodes);
+    const bool live = sub < n_subseg;
+    double ux = 0, uy = 0, uz = 1, e1x = 1, e1y = 0, e1z = 0, e2x = 0, e2y = 1, e2z = 0;
+    double cc = 0, cs = 0, arc2 = 0, sub2 = 0, w0 = 0, w2 = 0, offset = 0;
+    O1Subseg P{};
+    long long cell = 0;
+    if (live) {
+      // element of this sub-segment: last i with subseg_offset[i] <= sub
+      int64_t lo = 0, hi = E.n_el;
+      while (hi - lo > 1) {
+        int64_t mid = (lo + hi) >> 1;
+        if (subseg_offset[mid] <= sub) lo = mid; else hi = mid;
+      }
+      const int64_t i = lo;
+      const int64_t ia = sub - subseg_offset[i];
+      const int64_t n_a = subseg_offset[i + 1] - subseg_offset[i];
+      ux = E.direction[3 * i]; uy = E.direction[3 * i + 1]; uz = E.direction[3 * i + 2];
+      double hx, hy, hz;
+      if (fabs(uz) < 0.9) { hx = 0.0; hy = 0.0; hz = 1.0; } else { hx = 1.0; hy = 0.0; hz = 0.0; }
+      e1x = uy * hz - uz * hy; e1y = uz * hx - ux * hz; e1z = ux * hy - uy * hx;
+      const double norm = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+      e1x /= norm; e1y /= norm; e1z /= norm;
+      e2x = uy * e1z - uz * e1y; e2y = uz * e1x - ux * e1z; e2z = ux * e1y - uy * e1x;
+      cc = E.cone_cos[i];
+      cs = sqrt(fmax(1.0 - cc * cc, 0.0));
+      const double share = 1.0 / ((double)n_a * C.ring_nodes);
+      const double arc = two_pi * cs / C.ring_nodes;
+      arc2 = arc * arc / 12.0;
+      const double sl = E.length[i] / n_a;
+      sub2 = sl * sl / 12.0;
+      w0 = E.c0[i] * share;
+      w2 = E.c2[i] * share;
+      const double ig = (double)i * golden;
+      offset = (ig - floor(ig)) * two_pi / C.ring_nodes;
+      P = o1_subseg(E, i, ia, n_a);
+      const long long cx = min(max((long long)floor((P.px - E.grid_origin[0]) / C.cell_m), 0ll), (long long)E.grid_dims[0] - 1);
+      const long long cy = min(max((long long)floor((P.py - E.grid_origin[1]) / C.cell_m), 0ll), (long long)E.grid_dims[1] - 1);
+      const long long cz = min(max((long long)floor((P.pz - E.grid_origin[2]) / C.cell_m), 0ll), (long long)E.grid_dims[2] - 1);
+      cell = (cx * E.grid_dims[1] + cy) * E.grid_dims[2] + cz;
     }
-    const int64_t i = lo;
-    const int64_t ia = sub - subseg_offset[i];
-    const int64_t n_a = subseg_offset[i + 1] - subseg_offset[i];
-    const double ux = E.direction[3 * i], uy = E.direction[3 * i + 1], uz = E.direction[3 * i + 2];
-    double hx, hy, hz;
-    if (fabs(uz) < 0.9) { hx = 0.0; hy = 0.0; hz = 1.0; } else { hx = 1.0; hy = 0.0; hz = 0.0; }
-    double e1x = uy * hz - uz * hy, e1y = uz * hx - ux * hz, e1z = ux * hy - uy * hx;
-    const double norm = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
-    e1x /= norm; e1y /= norm; e1z /= norm;
-    const double e2x = uy * e1z - uz * e1y, e2y = uz * e1x - ux * e1z, e2z = ux * e1y - uy * e1x;
-    const double cc = E.cone_cos[i];
-    const double cs = sqrt(fmax(1.0 - cc * cc, 0.0));
-    const double share = 1.0 / ((double)n_a * C.ring_nodes);
-    const double arc = two_pi * cs / C.ring_nodes;
-    const double arc2 = arc * arc / 12.0;
-    const double sl = E.length[i] / n_a;
-    const double sub2 = sl * sl / 12.0;
-    const double w0 = E.c0[i] * share, w2 = E.c2[i] * share;
-    const double ig = (double)i * golden;
-    const double offset = (ig - floor(ig)) * two_pi / C.ring_nodes;
-    const O1Subseg P = o1_subseg(E, i, ia, n_a);
-    const long long cx = min(max((long long)floor((P.px - E.grid_origin[0]) / C.cell_m), 0ll), (long long)E.grid_dims[0] - 1);
-    const long long cy = min(max((long long)floor((P.py - E.grid_origin[1]) / C.cell_m), 0ll), (long long)E.grid_dims[1] - 1);
-    const long long cz = min(max((long long)floor((P.pz - E.grid_origin[2]) / C.cell_m), 0ll), (long long)E.grid_dims[2] - 1);
-    const long long cell = (cx * E.grid_dims[1] + cy) * E.grid_dims[2] + cz;
-    double sp, cp;
-    sincos(offset + two_pi * q / C.ring_nodes, &sp, &cp);
-    const double sx = cc * ux + cs * (cp * e1x + sp * e2x);
-    const double sy = cc * uy + cs * (cp * e1y + sp * e2y);
-    const double sz = cc * uz + cs * (cp * e1z + sp * e2z);
-    const long long key = cell * n_pix + o1_pixel(sx, sy, sz, C.pixel_face);
-    bool fresh;
-    const int64_t slot = o1_insert(keys, capacity, key, fresh);
-    if (slot < 0) {
-      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
-      continue;
-    }
-    double* row = rows + slot * kO1Moments;
     const double px = P.px, py = P.py, pz = P.pz, t = P.t;
-    const double tx = -sp * e1x + cp * e2x, ty = -sp * e1y + cp * e2y, tz = -sp * e1z + cp * e2z;
-    atomicAdd(row + 0, w0);
-    atomicAdd(row + 1, w2);
-    atomicAdd(row + 2, w0 * px);
-    atomicAdd(row + 3, w0 * py);
-    atomicAdd(row + 4, w0 * pz);
-    atomicAdd(row + 5, w0 * t);
-    atomicAdd(row + 6, w0 * sx);
-    atomicAdd(row + 7, w0 * sy);
-    atomicAdd(row + 8, w0 * sz);
-    atomicAdd(row + 9, w0 * (px * px + py * py + pz * pz + sub2));
-    atomicAdd(row + 10, w0 * t * t);
-    atomicAdd(row + 11, w0 * (sx * sx + arc2 * tx * tx));
-    atomicAdd(row + 12, w0 * (sy * sy + arc2 * ty * ty));
-    atomicAdd(row + 13, w0 * (sz * sz + arc2 * tz * tz));
-    atomicAdd(row + 14, w0 * (sx * sy + arc2 * tx * ty));
-    atomicAdd(row + 15, w0 * (sx * sz + arc2 * tx * tz));
-    atomicAdd(row + 16, w0 * (sy * sz + arc2 * ty * tz));
-    atomicAdd(row + 17, w0 * (px * px + sub2 * ux * ux));
-    atomicAdd(row + 18, w0 * (py * py + sub2 * uy * uy));
-    atomicAdd(row + 19, w0 * (pz * pz + sub2 * uz * uz));
-    atomicAdd(row + 20, w0 * (px * py + sub2 * ux * uy));
-    atomicAdd(row + 21, w0 * (px * pz + sub2 * ux * uz));
-    atomicAdd(row + 22, w0 * (py * pz + sub2 * uy * uz));
+    for (int q = q_begin; q < q_end; ++q) {
+      double sp, cp;
+      sincos(offset + two_pi * q / C.ring_nodes, &sp, &cp);
+      const double sx = cc * ux + cs * (cp * e1x + sp * e2x);
+      const double sy = cc * uy + cs * (cp * e1y + sp * e2y);
+      const double sz = cc * uz + cs * (cp * e1z + sp * e2z);
+      const long long key = live ? cell * n_pix + o1_pixel(sx, sy, sz, C.pixel_face) : -1ll;
+      const unsigned group = __match_any_sync(0xffffffffu, key);
+      const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)__popc(group)) - 1;
+      const bool leader = live && lane == __ffs(group) - 1;
+      const unsigned rest = group & ~(1u << lane);
+      double* row = nullptr;
+      if (leader) {
+        bool fresh;
+        // slots in key order (keys of one cell are contiguous) so that the
+        // compacted pencils come out spatially ordered
+        const int64_t slot = o1_insert(keys, capacity, key, fresh, true);
+        if (slot < 0) atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+        else row = rows + slot * kO1Moments;
+      }
+      const double tx = -sp * e1x + cp * e2x, ty = -sp * e1y + cp * e2y, tz = -sp * e1z + cp * e2z;
+      const double m[kO1Moments] = {
+          w0, w2, w0 * px, w0 * py, w0 * pz, w0 * t, w0 * sx, w0 * sy, w0 * sz,
+          w0 * (px * px + py * py + pz * pz + sub2), w0 * t * t,
+          w0 * (sx * sx + arc2 * tx * tx), w0 * (sy * sy + arc2 * ty * ty),
+          w0 * (sz * sz + arc2 * tz * tz), w0 * (sx * sy + arc2 * tx * ty),
+          w0 * (sx * sz + arc2 * tx * tz), w0 * (sy * sz + arc2 * ty * tz),
+          w0 * (px * px + sub2 * ux * ux), w0 * (py * py + sub2 * uy * uy),
+          w0 * (pz * pz + sub2 * uz * uz), w0 * (px * py + sub2 * ux * uy),
+          w0 * (px * pz + sub2 * ux * uz), w0 * (py * pz + sub2 * uy * uz)};
+#pragma unroll
+      for (int k = 0; k < kO1Moments; ++k) {
+        const double sum = o1_group_sum(m[k], rest, rounds);
+        if (row) atomicAdd(row + k, sum);
+      }
+    }
   }
 }
 
-// One thread per table slot: finish_pencils (_prompt_numba.py:2247-2354) for
-// slots with a positive weight, compacted into the pencil table.
-__global__ void o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
-                                 lh_order1_pencil_table Pn, int32_t* count, int32_t* status) {
-  for (int64_t slot = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; slot < capacity;
-       slot += (int64_t)gridDim.x * blockDim.x) {
-    if (keys[slot] == -1ll) continue;
-    const double* a = rows + slot * kO1Moments;
-    const double w = a[0];
-    if (!(w > 0.0)) continue;
-    const int q = atomicAdd(count, 1);
+constexpr int kO1Tile = 4096;          // ring-table slots per compaction CTA
+constexpr int kO1FinishThreads = 256;  // kO1Tile / kO1FinishThreads consecutive slots each
+
+LH_DEVICE bool o1_slot_used(const long long* keys, const double* rows, int64_t slot) {
+  return keys[slot] != -1ll && rows[slot * kO1Moments] > 0.0;
+}
+
+// Exclusive prefix sum of `v` over the CTA (blockDim a multiple of 32, at most
+// 1024); `total` receives the CTA's sum.
+LH_DEVICE int o1_block_exclusive_scan(int v, int& total) {
+  __shared__ int warp_sums[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+  int inclusive = v;
+  for (int off = 1; off < 32; off <<= 1) {
+    const int up = __shfl_up_sync(0xffffffffu, inclusive, off);
+    if (lane >= off) inclusive += up;
+  }
+  __syncthreads();  // warp_sums may still be read by a previous call
+  if (lane == 31) warp_sums[warp] = inclusive;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < n_warps ? warp_sums[lane] : 0;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int up = __shfl_up_sync(0xffffffffu, w, off);
+      if (lane >= off) w += up;
+    }
+    warp_sums[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  total = warp_sums[n_warps - 1];
+  return inclusive - v + (warp ? warp_sums[warp - 1] : 0);
+}
+
+// Used slots per tile of the ring table.
+__global__ void __launch_bounds__(kO1FinishThreads)
+o1_tile_count_kernel(const long long* keys, const double* rows, int64_t capacity,
+                     int32_t* tile_count) {
+  const int per = kO1Tile / kO1FinishThreads;
+  const int64_t begin = blockIdx.x * (int64_t)kO1Tile + threadIdx.x * per;
+  int mine = 0;
+  for (int j = 0; j < per; ++j)
+    if (begin + j < capacity && o1_slot_used(keys, rows, begin + j)) ++mine;
+  int total;
+  o1_block_exclusive_scan(mine, total);
+  if (threadIdx.x == 0) tile_count[blockIdx.x] = total;
+}
+
+// Exclusive tile offsets (in place) and the pencil count, in one CTA.
+__global__ void __launch_bounds__(1024)
+o1_tile_scan_kernel(int32_t* tile, int64_t n_tiles, int32_t* count) {
+  int carry = 0;
+  for (int64_t base = 0; base < n_tiles; base += blockDim.x) {
+    const int64_t i = base + threadIdx.x;
+    const int v = i < n_tiles ? tile[i] : 0;
+    int total;
+    const int before = o1_block_exclusive_scan(v, total);
+    if (i < n_tiles) tile[i] = carry + before;
+    carry += total;
+  }
+  if (threadIdx.x == 0) *count = carry;
+}
+
+LH_DEVICE void o1_write_pencil(const double* a, lh_order1_pencil_table& Pn, int q);
+
+// finish_pencils (_prompt_numba.py:2247-2354) for slots with a positive weight,
+// compacted into the pencil table in slot order: one CTA per tile, each thread
+// over kO1Tile / kO1FinishThreads consecutive slots, ranks by a CTA scan plus
+// the tile's offset. Slot order follows the keys, so pencils of a cell are
+// neighbours in the table.
+__global__ void __launch_bounds__(kO1FinishThreads)
+o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
+                 lh_order1_pencil_table Pn, const int32_t* tile_offset, int32_t* status) {
+  const int per = kO1Tile / kO1FinishThreads;
+  const int64_t begin = blockIdx.x * (int64_t)kO1Tile + threadIdx.x * per;
+  int mine = 0;
+  for (int j = 0; j < per; ++j)
+    if (begin + j < capacity && o1_slot_used(keys, rows, begin + j)) ++mine;
+  int total;
+  int q = tile_offset[blockIdx.x] + o1_block_exclusive_scan(mine, total);
+  if (!mine) return;
+  for (int j = 0; j < per; ++j) {
+    const int64_t slot = begin + j;
+    if (slot >= capacity || !o1_slot_used(keys, rows, slot)) continue;
     if (q >= Pn.capacity) {
       atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
-      continue;
+      return;
     }
+    o1_write_pencil(rows + slot * kO1Moments, Pn, q++);
+  }
+}
+
+LH_DEVICE void o1_write_pencil(const double* a, lh_order1_pencil_table& Pn, int q) {
+  {
+    const double w = a[0];
     const double mx = a[2] / w, my = a[3] / w, mz = a[4] / w;
     Pn.position[3 * q] = mx; Pn.position[3 * q + 1] = my; Pn.position[3 * q + 2] = mz;
     Pn.time[q] = a[5] / w;
@@ -297,10 +411,15 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
   const int32_t n_pencils =
       n_pencils_device ? min(*n_pencils_device, n_pencils_bound) : n_pencils_bound;
   const int64_t total = (int64_t)n_work * n_pencils;
-  for (int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; item < total;
-       item += (int64_t)gridDim.x * blockDim.x) {
-    const int w = (int)(item / n_pencils);
-    const int p = (int)(item - (int64_t)w * n_pencils);
+  const int lane = threadIdx.x & 31;
+  // whole warps iterate together: lanes past the end compute on pencil 0 of OM
+  // 0 and take no part in any group
+  for (int64_t item0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - lane; item0 < total;
+       item0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t item = item0 + lane;
+    bool live = item < total;
+    const int w = live ? (int)(item / n_pencils) : 0;
+    const int p = live ? (int)(item - (int64_t)w * n_pencils) : 0;
     const int d = work[w];
     const double rx = C.om_pos[3 * d], ry = C.om_pos[3 * d + 1], rz = C.om_pos[3 * d + 2];
     const double nx = C.om_look[3 * d], ny = C.om_look[3 * d + 1], nz = C.om_look[3 * d + 2];
@@ -377,7 +496,7 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
           theta = factor > 1.0 ? asin(fmin(1.0, 1.0 / factor)) : theta;
           averaged = avg;
         } else {
-          if (sine <= 1e-300) continue;
+          if (sine <= 1e-300) live = false;
           const double d2 = u_ * u_ + v_ * v_;
           factor = 1.0 / sine;
           if (d2 > 0.0) {
@@ -393,16 +512,25 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
     if (!(theta >= C.theta_lo)) i_theta = 0;
     else i_theta = min(1 + (int)(log(theta / C.theta_lo) / log_theta_ratio), theta_bins - 1);
     const long long key = base + (backward ? theta_bins : 0) + i_theta;
-    bool fresh;
-    long long* keys = gkeys + (int64_t)w * cap;
-    const int64_t slot = o1_insert(keys, cap, key, fresh);
-    if (slot < 0) {
-      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
-      continue;
+    // lanes with the same (OM, group key) sum their moments in registers; the
+    // group's lowest lane inserts the key and adds the sums
+    const unsigned group = __match_any_sync(0xffffffffu, live ? key : -1ll) &
+                           __match_any_sync(0xffffffffu, live ? w : -1);
+    const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)__popc(group)) - 1;
+    const unsigned rest = group & ~(1u << lane);
+    double* row = nullptr;
+    if (live && lane == __ffs(group) - 1) {
+      bool fresh;
+      long long* keys = gkeys + (int64_t)w * cap;
+      const int64_t slot = o1_insert(keys, cap, key, fresh);
+      if (slot < 0) {
+        atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+      } else {
+        if (fresh && atomicAdd(gcount + w, 1) >= kO1GroupSort)
+          atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+        row = grows + ((int64_t)w * cap + slot) * kO1MaxValues;
+      }
     }
-    if (fresh && atomicAdd(gcount + w, 1) >= kO1GroupSort)
-      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
-    double* row = grows + ((int64_t)w * cap + slot) * kO1MaxValues;
     // _fill_moments_averaged_pair (_prompt_numba.py:1260-1277)
     double cpw[5], spw[5];
     cpw[0] = 1.0;
@@ -420,15 +548,20 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
       const double basis = cpw[S.ipow[m]] * spw[S.jpow[m]];
       const double v0 = weight0 * basis;
       if (m == 0) omega = fabs(v0);
-      atomicAdd(row + m, v0);
-      atomicAdd(row + nm + m, weight2 * basis);
+      const double s0 = o1_group_sum(v0, rest, rounds);
+      const double s2 = o1_group_sum(weight2 * basis, rest, rounds);
+      if (row) {
+        atomicAdd(row + m, s0);
+        atomicAdd(row + nm + m, s2);
+      }
     }
-    atomicAdd(row + 2 * nm, omega);
-    atomicAdd(row + 2 * nm + 1, omega * theta);
-    atomicAdd(row + 2 * nm + 2, omega * r);
-    atomicAdd(row + 2 * nm + 3, omega * t_emit);
-    atomicAdd(row + 2 * nm + 4, omega * tau);
-    atomicAdd(row + 2 * nm + 5, omega * tau * tau);
+    const double tail[6] = {omega, omega * theta, omega * r, omega * t_emit, omega * tau,
+                            omega * tau * tau};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const double sum = o1_group_sum(tail[k], rest, rounds);
+      if (row) atomicAdd(row + 2 * nm + k, sum);
+    }
     (void)n_values;
   }
 }
@@ -930,6 +1063,7 @@ struct O1Workspace {
   long long* pkeys;
   double* prows;
   int32_t* pcount;
+  int32_t* tiles;
   long long* gkeys;
   double* grows;
   int32_t* gcount;
@@ -955,6 +1089,7 @@ static O1Workspace o1_layout(const lh_order1_config& C, int64_t pencil_capacity,
   W.pkeys = reinterpret_cast<long long*>(take(sizeof(long long) * ring_capacity));
   W.prows = reinterpret_cast<double*>(take(sizeof(double) * kO1Moments * ring_capacity));
   W.pcount = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 4));
+  W.tiles = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (ring_capacity / kO1Tile + 1)));
   W.gkeys = reinterpret_cast<long long*>(take(sizeof(long long) * (size_t)n_work * C.group_capacity));
   W.grows = reinterpret_cast<double*>(
       take(sizeof(double) * kO1MaxValues * (size_t)n_work * C.group_capacity));
@@ -1035,11 +1170,16 @@ extern "C" int lh_order1_pencils(const lh_order1_config* C, const lh_order1_elem
   if (E->n_el == 0 || E->n_subseg == 0) return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
   cudaMemsetAsync(W.pkeys, 0xff, sizeof(long long) * ring_cap, s);
   cudaMemsetAsync(W.prows, 0, sizeof(double) * lh::kO1Moments * ring_cap, s);
-  const int64_t nodes = E->n_subseg * C->ring_nodes;
-  lh::o1_ring_kernel<<<lh::grid_for(nodes, 256), 256, 0, s>>>(*C, *E, E->subseg_offset, E->n_subseg,
-                                                               W.pkeys, ring_cap, W.prows, status);
-  lh::o1_finish_kernel<<<lh::grid_for(ring_cap, 256), 256, 0, s>>>(W.pkeys, ring_cap, W.prows, *P,
-                                                                   n_pencils_device, status);
+  const int64_t ring_threads = ((E->n_subseg + 31) / 32) * 32 *
+                               ((C->ring_nodes + lh::kO1RingBlock - 1) / lh::kO1RingBlock);
+  lh::o1_ring_kernel<<<lh::grid_for(ring_threads, 256), 256, 0, s>>>(
+      *C, *E, E->subseg_offset, E->n_subseg, W.pkeys, ring_cap, W.prows, status);
+  const int64_t n_tiles = (ring_cap + lh::kO1Tile - 1) / lh::kO1Tile;
+  lh::o1_tile_count_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(W.pkeys, W.prows,
+                                                                             ring_cap, W.tiles);
+  lh::o1_tile_scan_kernel<<<1, 1024, 0, s>>>(W.tiles, n_tiles, n_pencils_device);
+  lh::o1_finish_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(
+      W.pkeys, ring_cap, W.prows, *P, W.tiles, status);
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }
 

@@ -385,8 +385,11 @@ __global__ void src_layout_kernel(const lh_source_problem P, const int32_t* slic
   }
 }
 
-// One CTA per (slice, band): time-lattice transform and the slice's points
-// (_shower_basis.py:577-611).
+// One CTA per (slice, band, block of kSrcOmegaBlock frequencies): time-lattice
+// transform and the slice's points (_shower_basis.py:577-611). One thread per
+// (channel, frequency) walks the slice's ticks with a rotating phasor.
+constexpr int kSrcOmegaBlock = 8;
+
 __global__ void src_transform_kernel(const lh_source_problem P, const int32_t* slice_lo,
                                      const int32_t* slice_hi, const double* deposit,
                                      const int32_t* slice_point, const int32_t* slice_wide,
@@ -403,8 +406,10 @@ __global__ void src_transform_kernel(const lh_source_problem P, const int32_t* s
   const int wide_count = (O.n_points[b] - occ) / 4;
   const double h = P.stencil_m, h2 = h * h;
   const double scale = P.band_scale[b];
-  for (int i = threadIdx.x; i < nch * W; i += blockDim.x) {
-    const int c = i % nch, w = i / nch;
+  const int w_begin = blockIdx.z * kSrcOmegaBlock;
+  const int w_count = min(kSrcOmegaBlock, W - w_begin);
+  for (int i = threadIdx.x; i < nch * w_count; i += blockDim.x) {
+    const int c = i % nch, w = w_begin + i / nch;
     const double om = P.omega[w];
     double ps, pc, ds, dc;
     sincos(om * lo * P.time_step_ns, &ps, &pc);
@@ -537,8 +542,10 @@ extern "C" int lh_source_compile(const lh_source_problem* P, const lh_source_out
       *P, W.nodes, W.offsets, W.counts, W.order, W.groups, W.n_groups, W.deposit, W.zero);
   lh::src_layout_kernel<<<1, 32, 0, s>>>(*P, W.slice_lo, W.slice_hi, W.zero, W.slice_point,
                                          W.slice_wide, W.centroid, W.n_occ, *O);
-  dim3 grid((unsigned)P->n_slices, (unsigned)NB);
-  lh::src_transform_kernel<<<grid, 256, 0, s>>>(*P, W.slice_lo, W.slice_hi, W.deposit,
+  dim3 grid((unsigned)P->n_slices, (unsigned)NB,
+            (unsigned)((P->n_omega + lh::kSrcOmegaBlock - 1) / lh::kSrcOmegaBlock));
+  const int threads = ((P->nch * lh::kSrcOmegaBlock + 31) / 32) * 32;
+  lh::src_transform_kernel<<<grid, std::min(threads, 1024), 0, s>>>(*P, W.slice_lo, W.slice_hi, W.deposit,
                                                 W.slice_point, W.slice_wide, W.n_occ, *O);
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }

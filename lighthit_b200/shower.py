@@ -29,6 +29,7 @@ construction) carry a different coarse order-1 charge.
 from __future__ import annotations
 
 import ctypes as C
+from contextlib import contextmanager
 from dataclasses import dataclass, field
 from pathlib import Path
 from time import perf_counter
@@ -58,7 +59,12 @@ class ShowerSettings:
     prompt_delay_ns: float = 20.0
     min_distance_m: float = 0.1          # PromptConfig.min_distance_m
     readout_mode: str = "split-bf16"
-    order0_gauss: int = 8
+    # Gauss order of the order-0 ray quadrature (wavelength, along-track and
+    # azimuth nodes per piece). Against the reference's control-variate order 0
+    # on the README shower: order 6 agrees to 6e-8 in charge (order 8: 2.5e-8,
+    # order 5: 4.6e-7), inside the reference's own tolerance 1e-10 + 2e-6 |q|
+    # (_surface_ballistic.py:149-168), at (6/8)^3 of order 8's work.
+    order0_gauss: int = 6
     screen: bool = True                  # PromptConfig.screen
     screen_margin: float = 3.0           # PromptConfig.screen_margin
 
@@ -299,6 +305,14 @@ class _Stages:
 
 
 @dataclass
+class _Lane:
+    stream: object
+    order1: object
+    order1_screen: object
+    source: object
+
+
+@dataclass
 class _Event:
     """Per-shower state carried between the stages of a batch."""
     el: dict
@@ -338,10 +352,48 @@ class ShowerTransport:
     """
 
     def __init__(self, tables: ShowerTables, config: ShowerSettings | None = None, *,
-                 profile=False):
+                 profile=False, lanes=4):
         self.tables = tables
         self.config = config or tables.settings
         self.profile = profile
+        self.n_lanes = max(1, int(lanes))
+        self._lane_list = None
+
+    # -- per-event launches on side streams -------------------------------------
+    def _lanes(self):
+        """Side streams for the per-event launch sequences of a batch (source
+        compile, order-1 stages A and B), each with its own workspaces, so the
+        small grids of several showers share the device."""
+        import copy
+        import torch
+        if self._lane_list is None:
+            T = self.tables
+            lanes = []
+            for _ in range(self.n_lanes):
+                views = {}
+                for name in ("order1", "order1_screen", "source"):
+                    view = copy.copy(getattr(T, name))
+                    view._workspace = None
+                    view._pencil_pool = None
+                    views[name] = view
+                lanes.append(_Lane(torch.cuda.Stream(T.device), **views))
+            self._lane_list = lanes
+        return self._lane_list
+
+    @contextmanager
+    def _fan_out(self):
+        """Lanes that start after the work queued so far on the current stream;
+        on exit the current stream waits for all of them."""
+        import torch
+        main = torch.cuda.current_stream(self.tables.device)
+        lanes = self._lanes()
+        for lane in lanes:
+            lane.stream.wait_stream(main)
+        try:
+            yield lanes
+        finally:
+            for lane in lanes:
+                main.wait_stream(lane.stream)
 
     # -- order >=2 helpers ----------------------------------------------------
     def _apply_device(self, points, channels, reference, frame, oms, *, zero_frequency):
@@ -429,9 +481,13 @@ class ShowerTransport:
         stage("setup")
         # ---- order >=2 sources on the node bands (device, all showers)
         src_status = torch.zeros(1, dtype=torch.int32, device=dev)
-        compiled = [T.source.compile(ev.el, ev.frame, status=src_status,
-                                     device_elements=store.event(k))
-                    for k, ev in enumerate(events)]
+        compiled = []
+        with self._fan_out() as lanes:
+            for k, ev in enumerate(events):
+                lane = lanes[k % len(lanes)]
+                with torch.cuda.stream(lane.stream):
+                    compiled.append(lane.source.compile(ev.el, ev.frame, status=src_status,
+                                                        device_elements=store.event(k)))
         npts_all = torch.stack([c[2] for c in compiled]).cpu().numpy()
         if int(src_status.item()) & _lib.LH_STATUS_OVERFLOW:
             raise ValueError("element nodes fall outside the source lattice")
@@ -547,11 +603,6 @@ class ShowerTransport:
         for k, ev in enumerate(events):
             self._prompt_selection(ev, dist[k], safety)
         prompt_events = [ev for ev in events if len(ev.work)]
-        if prompt_events:
-            origins = np.stack([ev.origins for ev in prompt_events])
-            batch0 = (prompt_store if len(prompt_events) == len(events) else
-                      ElementBatch([ev.prompt_el for ev in prompt_events], dev))
-            out0 = order0(T.order0, batch0, origins, edges, check=False)
         for k, ev in enumerate(events):
             ev.device_el = prompt_store.event(k)
         status = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -561,12 +612,23 @@ class ShowerTransport:
                 raise NotImplementedError("elements above threshold in only some bands need the "
                                           "per-band order-1 units")
             ev.cone_cos = 1.0 / (ev.device_el["beta"] * cone)
+            ev.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        # the coarse order-1 screens run on the lanes while order 0 (one launch for
+        # every shower) runs on this stream
+        with self._fan_out() as lanes:
             if cfg.screen and threshold > 0:
-                ev.status = torch.zeros(1, dtype=torch.int32, device=dev)
-                coarse = pencils(T.order1_screen, ev.prompt_el, ev.cone_cos, status=ev.status,
-                                 device_elements=ev.device_el)
-                ev.pending["coarse"] = grouped(T.order1_screen, coarse, ev.work, ev.origins,
-                                               status=ev.status)[0]
+                for k, ev in enumerate(prompt_events):
+                    lane = lanes[k % len(lanes)]
+                    with torch.cuda.stream(lane.stream):
+                        coarse = pencils(lane.order1_screen, ev.prompt_el, ev.cone_cos,
+                                         status=ev.status, device_elements=ev.device_el)
+                        ev.pending["coarse"] = grouped(lane.order1_screen, coarse, ev.work,
+                                                       ev.origins, status=ev.status)[0]
+            if prompt_events:
+                origins = np.stack([ev.origins for ev in prompt_events])
+                batch0 = (prompt_store if len(prompt_events) == len(events) else
+                          ElementBatch([ev.prompt_el for ev in prompt_events], dev))
+                out0 = order0(T.order0, batch0, origins, edges, check=False)
         if prompt_events:
             raise_order0_status(int(out0["status"].item()))
             q0_all = out0["charge"].cpu().numpy()
@@ -576,6 +638,7 @@ class ShowerTransport:
                 ev.pending["bins0"] = bins0_all[k]
         self._redo_overflow(prompt_events, "coarse", T.order1_screen)
         stage("order0_screen")
+        fine_events = []
         for ev in prompt_events:
             ev.fine = ev.work
             if "coarse" in ev.pending:
@@ -588,10 +651,15 @@ class ShowerTransport:
                                   >= threshold]
             if len(ev.fine):
                 ev.status = torch.zeros(1, dtype=torch.int32, device=dev)
-                ev.table = pencils(T.order1, ev.prompt_el, ev.cone_cos, status=ev.status,
-                                   device_elements=ev.device_el)
-                ev.pending["fine"] = grouped(T.order1, ev.table, ev.fine, ev.origins,
-                                             status=ev.status)
+                fine_events.append(ev)
+        with self._fan_out() as lanes:
+            for k, ev in enumerate(fine_events):
+                lane = lanes[k % len(lanes)]
+                with torch.cuda.stream(lane.stream):
+                    ev.table = pencils(lane.order1, ev.prompt_el, ev.cone_cos, status=ev.status,
+                                       device_elements=ev.device_el)
+                    ev.pending["fine"] = grouped(lane.order1, ev.table, ev.fine, ev.origins,
+                                                 status=ev.status)
         self._redo_overflow(prompt_events, "fine", T.order1)
         for ev in prompt_events:
             if "fine" not in ev.pending:
