@@ -106,24 +106,26 @@ LH_DEVICE O1Subseg o1_subseg(const lh_order1_elements& E, int64_t i, int64_t ia,
   return s;
 }
 
-// Sum of `v` over the lanes of a warp that share a key (their __match_any_sync
-// mask minus the calling lane is `rest`), valid in the group's lowest lane.
-// Every lane of the warp calls it with the same `rounds` (the largest group
-// size minus one), so the shuffles stay convergent.
-LH_DEVICE double o1_group_sum(double v, unsigned rest, int rounds) {
-  double acc = v;
-  for (int r = 0; r < rounds; ++r) {
-    const int src = rest ? __ffs(rest) - 1 : (int)(threadIdx.x & 31);
-    const double got = __shfl_sync(0xffffffffu, v, src);
-    if (rest) {
-      acc += got;
-      rest &= rest - 1;
+// Warp-level sums by key: every lane writes its n values to its row of the
+// warp's staging area (`stage`, 32 rows of n doubles in shared memory); the
+// lowest lane of each group of equal keys (`group`, a __match_any_sync mask)
+// adds its members' rows in lane order and issues one atomic per value to
+// `row`. The loads are independent, so a group of g lanes costs about g x n
+// issue slots in its leader instead of g dependent round trips.
+LH_DEVICE void o1_warp_group_add(double* stage, int n, unsigned group, bool leader, double* row) {
+  __syncwarp();
+  if (leader && row) {
+    for (int k = 0; k < n; ++k) {
+      double sum = 0.0;
+      for (unsigned g = group; g; g &= g - 1) sum += stage[(__ffs(g) - 1) * n + k];
+      atomicAdd(row + k, sum);
     }
   }
-  return acc;
+  __syncwarp();
 }
 
-constexpr int kO1RingBlock = 16;  // ring nodes per thread
+constexpr int kO1RingBlock = 16;    // ring nodes per thread
+constexpr int kO1RingThreads = 256;
 
 // One thread per (sub-segment, block of kO1RingBlock ring nodes):
 // compress_subsegments (_prompt_numba.py:1122-1232) with the ring rotation
@@ -131,7 +133,8 @@ constexpr int kO1RingBlock = 16;  // ring nodes per thread
 // take the same ring node together, so nodes that land in the same (cell,
 // pixel) (neighbouring steps of a track or shower) are summed in registers
 // first: one hash insert and one set of moment atomics per distinct key and warp.
-__global__ void o1_ring_kernel(const lh_order1_config C, const lh_order1_elements E,
+__global__ void __launch_bounds__(kO1RingThreads)
+o1_ring_kernel(const lh_order1_config C, const lh_order1_elements E,
                                const int64_t* subseg_offset, int64_t n_subseg,
                                long long* keys, int64_t capacity, double* rows,
                                int32_t* status) {
@@ -143,6 +146,8 @@ __global__ void o1_ring_kernel(const lh_order1_config C, const lh_order1_element
   const int n_blocks = (C.ring_nodes + kO1RingBlock - 1) / kO1RingBlock;
   const int64_t total = n_pad * n_blocks;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  __shared__ double s_stage[kO1RingThreads / 32][32 * kO1Moments];
+  double* stage = s_stage[threadIdx.x >> 5];
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total; k += stride) {
     const int64_t sub = k % n_pad;
     const int q_begin = (int)(k / n_pad) * kO1RingBlock;
@@ -195,9 +200,7 @@ __global__ void o1_ring_kernel(const lh_order1_config C, const lh_order1_element
       const double sz = cc * uz + cs * (cp * e1z + sp * e2z);
       const long long key = live ? cell * n_pix + o1_pixel(sx, sy, sz, C.pixel_face) : -1ll;
       const unsigned group = __match_any_sync(0xffffffffu, key);
-      const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)__popc(group)) - 1;
       const bool leader = live && lane == __ffs(group) - 1;
-      const unsigned rest = group & ~(1u << lane);
       double* row = nullptr;
       if (leader) {
         bool fresh;
@@ -217,11 +220,10 @@ __global__ void o1_ring_kernel(const lh_order1_config C, const lh_order1_element
           w0 * (px * px + sub2 * ux * ux), w0 * (py * py + sub2 * uy * uy),
           w0 * (pz * pz + sub2 * uz * uz), w0 * (px * py + sub2 * ux * uy),
           w0 * (px * pz + sub2 * ux * uz), w0 * (py * pz + sub2 * uy * uz)};
+      double* mine = stage + lane * kO1Moments;
 #pragma unroll
-      for (int k = 0; k < kO1Moments; ++k) {
-        const double sum = o1_group_sum(m[k], rest, rounds);
-        if (row) atomicAdd(row + k, sum);
-      }
+      for (int k = 0; k < kO1Moments; ++k) mine[k] = m[k];
+      o1_warp_group_add(stage, kO1Moments, group, leader, row);
     }
   }
 }
@@ -412,6 +414,8 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
       n_pencils_device ? min(*n_pencils_device, n_pencils_bound) : n_pencils_bound;
   const int64_t total = (int64_t)n_work * n_pencils;
   const int lane = threadIdx.x & 31;
+  extern __shared__ double o1g_stage[];  // [warp][32][n_values]
+  double* stage = o1g_stage + (threadIdx.x >> 5) * 32 * n_values;
   // whole warps iterate together: lanes past the end compute on pencil 0 of OM
   // 0 and take no part in any group
   for (int64_t item0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - lane; item0 < total;
@@ -516,10 +520,9 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
     // group's lowest lane inserts the key and adds the sums
     const unsigned group = __match_any_sync(0xffffffffu, live ? key : -1ll) &
                            __match_any_sync(0xffffffffu, live ? w : -1);
-    const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)__popc(group)) - 1;
-    const unsigned rest = group & ~(1u << lane);
+    const bool leader = live && lane == __ffs(group) - 1;
     double* row = nullptr;
-    if (live && lane == __ffs(group) - 1) {
+    if (leader) {
       bool fresh;
       long long* keys = gkeys + (int64_t)w * cap;
       const int64_t slot = o1_insert(keys, cap, key, fresh);
@@ -544,25 +547,21 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
     const double weight0 = weight * Pn.w0[p], weight2 = weight * Pn.w2[p];
     const int nm = C.n_mono;
     double omega = 0.0;
+    double* mine = stage + lane * n_values;
     for (int m = 0; m < nm; ++m) {
       const double basis = cpw[S.ipow[m]] * spw[S.jpow[m]];
       const double v0 = weight0 * basis;
       if (m == 0) omega = fabs(v0);
-      const double s0 = o1_group_sum(v0, rest, rounds);
-      const double s2 = o1_group_sum(weight2 * basis, rest, rounds);
-      if (row) {
-        atomicAdd(row + m, s0);
-        atomicAdd(row + nm + m, s2);
-      }
+      mine[m] = v0;
+      mine[nm + m] = weight2 * basis;
     }
-    const double tail[6] = {omega, omega * theta, omega * r, omega * t_emit, omega * tau,
-                            omega * tau * tau};
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      const double sum = o1_group_sum(tail[k], rest, rounds);
-      if (row) atomicAdd(row + 2 * nm + k, sum);
-    }
-    (void)n_values;
+    mine[2 * nm] = omega;
+    mine[2 * nm + 1] = omega * theta;
+    mine[2 * nm + 2] = omega * r;
+    mine[2 * nm + 3] = omega * t_emit;
+    mine[2 * nm + 4] = omega * tau;
+    mine[2 * nm + 5] = omega * tau * tau;
+    o1_warp_group_add(stage, n_values, group, leader, row);
   }
 }
 
@@ -1172,7 +1171,7 @@ extern "C" int lh_order1_pencils(const lh_order1_config* C, const lh_order1_elem
   cudaMemsetAsync(W.prows, 0, sizeof(double) * lh::kO1Moments * ring_cap, s);
   const int64_t ring_threads = ((E->n_subseg + 31) / 32) * 32 *
                                ((C->ring_nodes + lh::kO1RingBlock - 1) / lh::kO1RingBlock);
-  lh::o1_ring_kernel<<<lh::grid_for(ring_threads, 256), 256, 0, s>>>(
+  lh::o1_ring_kernel<<<lh::grid_for(ring_threads, lh::kO1RingThreads), lh::kO1RingThreads, 0, s>>>(
       *C, *E, E->subseg_offset, E->n_subseg, W.pkeys, ring_cap, W.prows, status);
   const int64_t n_tiles = (ring_cap + lh::kO1Tile - 1) / lh::kO1Tile;
   lh::o1_tile_count_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(W.pkeys, W.prows,
@@ -1206,7 +1205,12 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
   cudaMemsetAsync(W.gcount, 0, sizeof(int32_t) * (size_t)n_work, s);
   cudaMemsetAsync(W.batch_total, 0, sizeof(int32_t) * 4, s);
   cudaMemsetAsync(W.accum, 0, sizeof(double) * (size_t)n_work * C->n_bands * (3 + 4 * nb + 1), s);
-  lh::o1_group_kernel<<<lh::grid_for((int64_t)n_work * n_pencils, 256), 256, 0, s>>>(
+  const size_t group_smem = sizeof(double) * 32 * (256 / 32) * (2 * C->n_mono + 6);
+  if (group_smem > 48 * 1024 &&
+      cudaFuncSetAttribute(lh::o1_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)group_smem) != cudaSuccess)
+    return LH_ECUDA;
+  lh::o1_group_kernel<<<lh::grid_for((int64_t)n_work * n_pencils, 256), 256, group_smem, s>>>(
       *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows, W.gcount,
       status);
   const size_t sort_smem = sizeof(unsigned long long) * lh::kO1GroupSort;

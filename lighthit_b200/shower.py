@@ -875,18 +875,31 @@ def main(argv=None):
     ap.add_argument("--tables", default="c2", choices=["c0", "c2"])
     ap.add_argument("--showers", type=int, default=8)
     ap.add_argument("--profile", action="store_true", help="per-stage device-synchronised times")
+    ap.add_argument("--batch", action="store_true",
+                    help="route all showers as one stage-major batch")
     args = ap.parse_args(argv)
     route = ShowerTransport(ShowerTables.synthetic(args.tables), profile=args.profile)
     draws = shower_stream(args.showers, route.tables.positions.mean(axis=0))
-    for d in draws:
-        el = gaussian_shower(d["position_m"], d["direction"],
-                             charged_track_length_m=d["charged_track_length_m"],
-                             elements=d["elements"], seed=d["seed"])
-        r = route(el)
+    showers = [gaussian_shower(d["position_m"], d["direction"],
+                               charged_track_length_m=d["charged_track_length_m"],
+                               elements=d["elements"], seed=d["seed"]) for d in draws]
+    if args.batch:
+        began = perf_counter()
+        responses = route.batch(showers)
         torch.cuda.synchronize()
+        elapsed = perf_counter() - began
+    else:
+        responses = []
+        for el in showers:
+            responses.append(route(el))
+            torch.cuda.synchronize()
+    for d, r in zip(draws, responses):
         print(json.dumps({"elements": d["elements"], "active": int(r.active.sum()),
                           "charge_pe": float(r.charge_pe.sum()),
                           "ms": 1e3 * r.metadata["elapsed_seconds"]}), flush=True)
+    if args.batch:
+        print(json.dumps({"batch_showers": len(showers), "batch_ms": 1e3 * elapsed,
+                          "showers_per_s": len(showers) / elapsed}), flush=True)
 
 
 if __name__ == "__main__":
