@@ -184,7 +184,7 @@ bool ge2_valid(const lh_ge2_table* t, const lh_ge2_problem* p) {
     return false;
   if (p->n_points && (!p->points || !p->channels)) return false;
   if (p->n_om && (!p->receivers || !p->looks || !p->out_scale)) return false;
-  if ((size_t)t->nch * t->n_pairs * 32 * sizeof(float) > 200 * 1024) return false;
+  if ((size_t)t->nch * t->n_pairs * 32 * sizeof(float) + 32 * 128 * 8 > 200 * 1024) return false;
   return true;
 }
 }  // namespace
