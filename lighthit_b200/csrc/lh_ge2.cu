@@ -30,7 +30,6 @@ constexpr int kGe2Degree = 16;   // source/kernel degree bound
 constexpr int kGe2Out = 4;       // acceptance (detector) degree bound
 constexpr int kGe2M = 4;         // azimuthal degree bound
 constexpr int kGe2Chunk = 32;    // points per partial sum
-constexpr int kGe2Sub = 4;       // points sharing one pass over the degrees
 
 LH_DEVICE double par(int n) { return (n & 1) ? -1.0 : 1.0; }
 
@@ -295,69 +294,49 @@ LH_DEVICE void ge2_apply_body(const lh_ge2_table& T, const lh_ge2_problem& P, in
     const int lam = item / Wn, w = item % Wn;
     const double om = T.omega[w];
     float acc_re = 0.f, acc_im = 0.f;
-    // points in sub-blocks of kGe2Sub with the degree loop outside the point
-    // loop: the (band, interval, degree) coefficient slab a thread reads is
-    // reused from L1 by the sub-block's points (neighbouring points of a shower
-    // share their radial interval); per point the sums run in the same order
-    for (int cb = c0; cb < c1; cb += kGe2Sub) {
-      float pr[kGe2Sub], pi[kGe2Sub], tt[kGe2Sub];
-      int jj[kGe2Sub];
-#pragma unroll
-      for (int u = 0; u < kGe2Sub; ++u) {
-        pr[u] = 0.f;
-        pi[u] = 0.f;
-        jj[u] = cb + u < c1 ? g_j[base + cb + u] : -1;
-        tt[u] = jj[u] >= 0 ? g_t[base + cb + u] : 0.f;
-      }
+    for (int c = c0; c < c1; ++c) {
+      const int64_t idx = base + c;
+      const int j = g_j[idx];
+      if (j < 0) continue;
+      const float t = g_t[idx];
+      const float* F = s_F + (c - c0) * fsz;
+      const float2* ch = reinterpret_cast<const float2*>(P.channels) +
+                         (((int64_t)lam * P.n_points + c) * nch) * P.n_omega_channels;
+      float pr = 0.f, pi = 0.f;
       for (int l = 0; l <= T.degree; ++l) {
+        // radial cubic of every pair at (lam, j, l, w)
+        float rr[8], ri[8];
+        const float2* cf = reinterpret_cast<const float2*>(T.coef) +
+                           ((((int64_t)lam * T.n_intervals + j) * (T.degree + 1) + l) * NP * 4) *
+                               T.n_omega + w;
+        for (int p = 0; p < NP; ++p) {
+          const float2 k0 = cf[(p * 4 + 0) * T.n_omega], k1 = cf[(p * 4 + 1) * T.n_omega];
+          const float2 k2 = cf[(p * 4 + 2) * T.n_omega], k3 = cf[(p * 4 + 3) * T.n_omega];
+          rr[p] = fmaf(fmaf(fmaf(k0.x, t, k1.x), t, k2.x), t, k3.x);
+          ri[p] = fmaf(fmaf(fmaf(k0.y, t, k1.y), t, k2.y), t, k3.y);
+        }
         const int keep = l < T.max_m ? l : T.max_m;
-        const int row0 = T.starts[l], rows = 2 * keep + 1;
-#pragma unroll
-        for (int u = 0; u < kGe2Sub; ++u) {
-          if (jj[u] < 0) continue;
-          const int c = cb + u;
-          const float t = tt[u];
-          const float* F = s_F + (c - c0) * fsz;
-          const float2* ch = reinterpret_cast<const float2*>(P.channels) +
-                             (((int64_t)lam * P.n_points + c) * nch) * P.n_omega_channels;
-          // radial cubic of every pair at (lam, j, l, w)
-          float rr[8], ri[8];
-          const float2* cf = reinterpret_cast<const float2*>(T.coef) +
-                             ((((int64_t)lam * T.n_intervals + jj[u]) * (T.degree + 1) + l) * NP * 4) *
-                                 T.n_omega + w;
+        for (int row = T.starts[l]; row < T.starts[l] + 2 * keep + 1; ++row) {
+          float gr = 0.f, gi = 0.f;
           for (int p = 0; p < NP; ++p) {
-            const float2 k0 = cf[(p * 4 + 0) * T.n_omega], k1 = cf[(p * 4 + 1) * T.n_omega];
-            const float2 k2 = cf[(p * 4 + 2) * T.n_omega], k3 = cf[(p * 4 + 3) * T.n_omega];
-            rr[p] = fmaf(fmaf(fmaf(k0.x, t, k1.x), t, k2.x), t, k3.x);
-            ri[p] = fmaf(fmaf(fmaf(k0.y, t, k1.y), t, k2.y), t, k3.y);
+            const float f = F[row * NP + p];
+            gr = fmaf(f, rr[p], gr);
+            gi = fmaf(f, ri[p], gi);
           }
-          for (int row = row0; row < row0 + rows; ++row) {
-            float gr = 0.f, gi = 0.f;
-            for (int p = 0; p < NP; ++p) {
-              const float f = F[row * NP + p];
-              gr = fmaf(f, rr[p], gr);
-              gi = fmaf(f, ri[p], gi);
-            }
-            const float2 x = ch[row * P.n_omega_channels + w];
-            pr[u] += x.x * gr - x.y * gi;
-            pi[u] += x.x * gi + x.y * gr;
-          }
+          const float2 x = ch[row * P.n_omega_channels + w];
+          pr += x.x * gr - x.y * gi;
+          pi += x.x * gi + x.y * gr;
         }
       }
-#pragma unroll
-      for (int u = 0; u < kGe2Sub; ++u) {
-        if (jj[u] < 0) continue;
-        const int64_t idx = base + cb + u;
-        // band scale and flight phase e^{i w r / v}
-        const float sc = g_scale[(int64_t)lam * total + idx];
-        float sv = 0.f, cv = 1.f;
-        if (T.flight) {
-          const double turns = om * g_r[idx] / T.speed[lam] * (1.0 / (2 * kPi));
-          sincospif(2.f * (float)(turns - rint(turns)), &sv, &cv);
-        }
-        acc_re += sc * (pr[u] * cv - pi[u] * sv);
-        acc_im += sc * (pr[u] * sv + pi[u] * cv);
+      // band scale and flight phase e^{i w r / v}
+      const float sc = g_scale[(int64_t)lam * total + idx];
+      float sv = 0.f, cv = 1.f;
+      if (T.flight) {
+        const double turns = om * g_r[idx] / T.speed[lam] * (1.0 / (2 * kPi));
+        sincospif(2.f * (float)(turns - rint(turns)), &sv, &cv);
       }
+      acc_re += sc * (pr * cv - pi * sv);
+      acc_im += sc * (pr * sv + pi * cv);
     }
     partial[(((int64_t)d * chunks + chunk) * T.n_bands + lam) * Wn + w] =
         make_double2(acc_re, acc_im);
@@ -390,7 +369,7 @@ __global__ void ge2_geometry_kernel(lh_ge2_table T, lh_ge2_problem P, int* g_j, 
                     g_F);
 }
 
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
 ge2_apply_kernel(lh_ge2_table T, lh_ge2_problem P, const int* g_j,
                                  const float* g_t, const double* g_r, const float* g_scale,
                                  const float* g_F, double2* partial) {
@@ -427,7 +406,7 @@ __global__ void ge2_geometry_batch_kernel(lh_ge2_table T, const Ge2Slot* slots, 
                     A.g_r + o, A.g_scale + o * T.n_bands, A.g_F + o * T.nch * T.n_pairs);
 }
 
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
 ge2_apply_batch_kernel(lh_ge2_table T, const Ge2Slot* slots, Ge2Arrays A) {
   const Ge2Slot& S = slots[blockIdx.z];
   if ((int)blockIdx.x >= S.P.n_om || (int)blockIdx.y >= S.chunks) return;
@@ -446,10 +425,11 @@ __global__ void ge2_reduce_batch_kernel(lh_ge2_table T, const Ge2Slot* slots, Ge
 int ge2_chunks(const lh_ge2_problem& P) { return (P.n_points + kGe2Chunk - 1) / kGe2Chunk; }
 
 // Shared memory of the apply kernels (256 threads): the chunk's F rows, then
-// the point values of the few-item path (at most 128 (band, frequency) items).
-size_t ge2_apply_smem(const lh_ge2_table& T) {
+// the point values of the few-item path when a problem takes it (at most 128
+// (band, frequency) items).
+size_t ge2_apply_smem(const lh_ge2_table& T, int items) {
   return (size_t)kGe2Chunk * T.nch * T.n_pairs * sizeof(float) +
-         (size_t)kGe2Chunk * 128 * sizeof(float2);
+         (2 * items <= 256 ? (size_t)kGe2Chunk * items * sizeof(float2) : 0);
 }
 
 size_t ge2_workspace(const lh_ge2_table& T, const lh_ge2_problem& P) {
@@ -473,7 +453,7 @@ int ge2_launch(const lh_ge2_table& T, const lh_ge2_problem& P, void* ws, cudaStr
   double2* partial = reinterpret_cast<double2*>(p);
   ge2_geometry_kernel<<<(unsigned)((pairs + 127) / 128), 128, 0, s>>>(T, P, g_j, g_t, g_r, g_scale, g_F);
   const int chunks = ge2_chunks(P);
-  const size_t smem = ge2_apply_smem(T);
+  const size_t smem = ge2_apply_smem(T, T.n_bands * P.n_omega);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(ge2_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   ge2_apply_kernel<<<dim3(P.n_om, chunks), 256, smem, s>>>(T, P, g_j, g_t, g_r, g_scale, g_F,
@@ -535,7 +515,8 @@ int ge2_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n, 
   if (max_pairs > 0) {  // problems without points reduce nothing: their results are zero
     ge2_geometry_batch_kernel<<<dim3((unsigned)((max_pairs + 127) / 128), n), 128, 0, s>>>(
         T, slots, A);
-    const size_t smem = ge2_apply_smem(T);
+    size_t smem = 0;
+    for (int i = 0; i < n; ++i) smem = std::max(smem, ge2_apply_smem(T, T.n_bands * P[i].n_omega));
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(ge2_apply_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
