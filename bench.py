@@ -190,10 +190,10 @@ def reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
-N_SHOWER = 48
+N_SHOWER = 96
 
 
-def shower_stream_section(dev, steps, workers=2, max_batch=12):
+def shower_stream_section(dev, steps, workers=2, max_batch=8):
     """Config 2: the served shower stream at 384 OMs through the device route.
 
     ``plain_fp32``: one shower after another on one stream, fp32 readout (the

@@ -299,23 +299,30 @@ LH_DEVICE void o1_write_pencil(const double* a, lh_order1_pencil_table& Pn, int 
 // neighbours in the table.
 __global__ void __launch_bounds__(kO1FinishThreads)
 o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
-                 lh_order1_pencil_table Pn, const int32_t* tile_offset, int32_t* status) {
+                 lh_order1_pencil_table Pn, const int32_t* tile_offset, const int32_t* count,
+                 int32_t* status) {
   const int per = kO1Tile / kO1FinishThreads;
   const int64_t begin = blockIdx.x * (int64_t)kO1Tile + threadIdx.x * per;
+  const int64_t n = *count;
+  if (n > Pn.capacity) {  // the caller redoes the stage with a larger table
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+    return;
+  }
   int mine = 0;
   for (int j = 0; j < per; ++j)
     if (begin + j < capacity && o1_slot_used(keys, rows, begin + j)) ++mine;
   int total;
-  int q = tile_offset[blockIdx.x] + o1_block_exclusive_scan(mine, total);
+  int64_t q = tile_offset[blockIdx.x] + o1_block_exclusive_scan(mine, total);
   if (!mine) return;
   for (int j = 0; j < per; ++j) {
     const int64_t slot = begin + j;
     if (slot >= capacity || !o1_slot_used(keys, rows, slot)) continue;
-    if (q >= Pn.capacity) {
-      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
-      return;
-    }
-    o1_write_pencil(rows + slot * kO1Moments, Pn, q++);
+    // rank q goes to row (q * 2^31-1) mod n, a fixed permutation (2^31 - 1 is
+    // prime and n < 2^31): stage B's warps then see pencils of many cells, not
+    // a run of one cell's pencils competing for the same group rows
+    o1_write_pencil(rows + slot * kO1Moments, Pn, (int)((q * 2147483647ll) % n));
+    ++q;
   }
 }
 
@@ -1178,7 +1185,7 @@ extern "C" int lh_order1_pencils(const lh_order1_config* C, const lh_order1_elem
                                                                              ring_cap, W.tiles);
   lh::o1_tile_scan_kernel<<<1, 1024, 0, s>>>(W.tiles, n_tiles, n_pencils_device);
   lh::o1_finish_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(
-      W.pkeys, ring_cap, W.prows, *P, W.tiles, status);
+      W.pkeys, ring_cap, W.prows, *P, W.tiles, n_pencils_device, status);
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }
 
