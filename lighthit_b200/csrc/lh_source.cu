@@ -385,15 +385,19 @@ __global__ void src_layout_kernel(const lh_source_problem P, const int32_t* slic
   }
 }
 
-// One CTA per (slice, band, block of kSrcOmegaBlock frequencies): time-lattice
+// One CTA per (slice, band, block of `w_block` frequencies): time-lattice
 // transform and the slice's points (_shower_basis.py:577-611). One thread per
-// (channel, frequency) walks the slice's ticks with a rotating phasor.
+// (channel, frequency) walks the slice's ticks with a rotating phasor; the
+// CTA stages the deposit rows of kSrcStageBytes worth of ticks at a time in
+// shared memory (coalesced, independent loads) before the threads read them.
 constexpr int kSrcOmegaBlock = 8;
+constexpr int kSrcStageBytes = 48 * 1024;
 
 __global__ void src_transform_kernel(const lh_source_problem P, const int32_t* slice_lo,
                                      const int32_t* slice_hi, const double* deposit,
                                      const int32_t* slice_point, const int32_t* slice_wide,
-                                     const int32_t* n_occ, lh_source_output O) {
+                                     const int32_t* n_occ, lh_source_output O, int w_block) {
+  extern __shared__ double s_dep[];  // [tick][moment][channel]
   const int64_t s = blockIdx.x;
   const int b = blockIdx.y;
   const int NB = P.n_bands, nch = P.nch, W = P.n_omega;
@@ -406,20 +410,34 @@ __global__ void src_transform_kernel(const lh_source_problem P, const int32_t* s
   const int wide_count = (O.n_points[b] - occ) / 4;
   const double h = P.stencil_m, h2 = h * h;
   const double scale = P.band_scale[b];
-  const int w_begin = blockIdx.z * kSrcOmegaBlock;
-  const int w_count = min(kSrcOmegaBlock, W - w_begin);
-  for (int i = threadIdx.x; i < nch * w_count; i += blockDim.x) {
-    const int c = i % nch, w = w_begin + i / nch;
-    const double om = P.omega[w];
-    double ps, pc, ds, dc;
+  const int w_begin = blockIdx.z * w_block;
+  const int w_count = min(w_block, W - w_begin);
+  const int nk = wide >= 0 ? 5 : 1;
+  const int row = nk * nch;  // staged doubles per tick
+  const int chunk = max(1, min(64, (int)(kSrcStageBytes / sizeof(double)) / row));
+  const int i = threadIdx.x;
+  const bool mine = i < nch * w_count;
+  const int c = mine ? i % nch : 0, w = w_begin + (mine ? i / nch : 0);
+  const double om = P.omega[w];
+  double ps = 0, pc = 1, ds = 0, dc = 1;
+  if (mine) {
     sincos(om * lo * P.time_step_ns, &ps, &pc);
     sincos(om * P.time_step_ns, &ds, &dc);
-    double re[5] = {0, 0, 0, 0, 0}, im[5] = {0, 0, 0, 0, 0};
-    const int nk = wide >= 0 ? 5 : 1;
-    for (int tick = lo; tick <= hi; ++tick) {
-      const double* row = deposit + (((s * P.kmax + tick) * NB + b) * 5) * nch + c;
+  }
+  double re[5] = {0, 0, 0, 0, 0}, im[5] = {0, 0, 0, 0, 0};
+  for (int t0 = lo; t0 <= hi; t0 += chunk) {
+    const int n_t = min(chunk, hi - t0 + 1);
+    __syncthreads();
+    for (int e = threadIdx.x; e < n_t * row; e += blockDim.x) {
+      const int tt = e / row, r = e - tt * row;
+      s_dep[e] = deposit[(((s * P.kmax + t0 + tt) * NB + b) * 5) * nch + r];
+    }
+    __syncthreads();
+    if (!mine) continue;
+    for (int tt = 0; tt < n_t; ++tt) {
+      const double* rowp = s_dep + tt * row + c;
       for (int k = 0; k < nk; ++k) {
-        const double v = row[k * nch];
+        const double v = rowp[k * nch];
         re[k] += v * pc;
         im[k] += v * ps;
       }
@@ -427,6 +445,8 @@ __global__ void src_transform_kernel(const lh_source_problem P, const int32_t* s
       pc = npc;
       ps = nps;
     }
+  }
+  if (mine) {
     float2* out = reinterpret_cast<float2*>(O.channels);
     auto put = [&](int p, double r, double m) {
       out[(((int64_t)b * O.capacity + p) * nch + c) * W + w] =
@@ -542,10 +562,10 @@ extern "C" int lh_source_compile(const lh_source_problem* P, const lh_source_out
       *P, W.nodes, W.offsets, W.counts, W.order, W.groups, W.n_groups, W.deposit, W.zero);
   lh::src_layout_kernel<<<1, 32, 0, s>>>(*P, W.slice_lo, W.slice_hi, W.zero, W.slice_point,
                                          W.slice_wide, W.centroid, W.n_occ, *O);
-  dim3 grid((unsigned)P->n_slices, (unsigned)NB,
-            (unsigned)((P->n_omega + lh::kSrcOmegaBlock - 1) / lh::kSrcOmegaBlock));
-  const int threads = ((P->nch * lh::kSrcOmegaBlock + 31) / 32) * 32;
-  lh::src_transform_kernel<<<grid, std::min(threads, 1024), 0, s>>>(*P, W.slice_lo, W.slice_hi, W.deposit,
-                                                W.slice_point, W.slice_wide, W.n_occ, *O);
+  const int w_block = std::max(1, std::min(lh::kSrcOmegaBlock, 1024 / P->nch));
+  dim3 grid((unsigned)P->n_slices, (unsigned)NB, (unsigned)((P->n_omega + w_block - 1) / w_block));
+  const int threads = ((P->nch * w_block + 31) / 32) * 32;
+  lh::src_transform_kernel<<<grid, threads, lh::kSrcStageBytes, s>>>(
+      *P, W.slice_lo, W.slice_hi, W.deposit, W.slice_point, W.slice_wide, W.n_occ, *O, w_block);
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }
