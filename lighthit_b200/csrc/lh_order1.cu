@@ -124,7 +124,7 @@ LH_DEVICE void o1_warp_group_add(double* stage, int n, unsigned group, bool lead
   __syncwarp();
 }
 
-constexpr int kO1RingBlock = 16;    // ring nodes per thread
+constexpr int kO1RingBlock = 4;     // ring nodes per thread
 constexpr int kO1RingThreads = 256;
 
 // One thread per (sub-segment, block of kO1RingBlock ring nodes):
