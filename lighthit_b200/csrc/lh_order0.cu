@@ -358,6 +358,7 @@ struct O0Shared {
   double warp_charge[kO0Threads / 32];
   int n_pairs;
   int n_combos;
+  int next_item;  // phase-2 work counter (warps take 32 items at a time)
 };
 
 __global__ void __launch_bounds__(kO0Threads, 3)
@@ -389,7 +390,10 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
   const int p_end = min(W.offsets[entry.x] + W.counts[entry.x], p_begin + kO0Chunk);
   if (want_bins)
     for (int k = tid; k < nb; k += blockDim.x) sbins[k] = 0.0;
-  if (tid == 0) S.n_combos = 0;
+  if (tid == 0) {
+    S.n_combos = 0;
+    S.next_item = 0;
+  }
   const double ox = O.om_pos[3 * om], oy = O.om_pos[3 * om + 1], oz = O.om_pos[3 * om + 2];
   const double radius = O.om_radius[om];
   uint32_t flags = 0;
@@ -500,7 +504,16 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
   double scuts[kO0MaxSCuts];
   double phicuts[kO0MaxPhiCuts];
 
-  for (int item = tid; item < n_combos * order; item += blockDim.x) {
+  // warps take 32 consecutive items at a time from a shared counter, so a warp
+  // that drew cheap pieces goes back for more instead of idling at the barrier
+  const int n_items = n_combos * order;
+  const int lane = tid & 31;
+  for (int item_base = 0;;) {
+    if (lane == 0) item_base = atomicAdd(&S.next_item, 32);
+    item_base = __shfl_sync(0xffffffffu, item_base, 0);
+    if (item_base >= n_items) break;
+    const int item = item_base + lane;
+    if (item >= n_items) continue;
     const int ci = item / order, ilam = item - ci * order;
     const uint32_t code = combos[ci];
     const int p = code & 0xff, panel = (code >> 8) & 0xffff, piece = code >> 24;
