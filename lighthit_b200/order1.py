@@ -218,12 +218,27 @@ def _element(source, name):
     return source[name] if isinstance(source, dict) else getattr(source, name)
 
 
+def element_box(elements):
+    """Per-coordinate minima and maxima of the element starts and ends
+    ``start + length * direction`` (``compress``'s cell grid, ``prompt.py:1317-1402``):
+    ``(low, high)``. Column reductions (an axis-0 reduction of an (N, 3) array is
+    several times slower in NumPy); minima and maxima are exact in any order."""
+    start = np.ascontiguousarray(_element(elements, "start_m"), float)
+    direction = np.ascontiguousarray(_element(elements, "direction"), float)
+    length = np.asarray(_element(elements, "length_m"), float)
+    ends = start + length[:, None] * direction
+    low = np.array([min(start[:, k].min(), ends[:, k].min()) for k in range(3)])
+    high = np.array([max(start[:, k].max(), ends[:, k].max()) for k in range(3)])
+    return low, high
+
+
 def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=None,
-            device_elements=None, capacity_full=False):
+            device_elements=None, capacity_full=False, box=None):
     """Stage A: ``compress`` of the elements with frozen cone cosines.
 
     ``device_elements``: the same elements already on the device (dict of
     tensors with the reference field names), read instead of uploading.
+    ``box``: ``element_box(elements)`` when the caller has it already.
     """
     import torch
     dev = tables.device
@@ -238,9 +253,9 @@ def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=Non
     offsets[1:] = np.cumsum(n_a)
     n_sub = int(offsets[-1])
     if n_el:
-        ends = start + length[:, None] * direction
-        low = np.minimum(start.min(axis=0), ends.min(axis=0)) - s.cell_m
-        high = np.maximum(start.max(axis=0), ends.max(axis=0)) + s.cell_m
+        lo_box, hi_box = element_box(elements) if box is None else box
+        low = lo_box - s.cell_m
+        high = hi_box + s.cell_m
         dims = np.ceil((high - low) / s.cell_m).astype(np.int64) + 1
     else:
         low, dims = np.zeros(3), np.ones(3, np.int64)
@@ -284,7 +299,7 @@ def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=Non
         flags = int(st.item())
         if flags & _lib.LH_STATUS_OVERFLOW and capacity < nodes:
             return pencils(tables, elements, cone_cos, stream=stream,
-                           device_elements=device_elements, capacity_full=True)
+                           device_elements=device_elements, capacity_full=True, box=box)
         _raise(flags)
     return table
 

@@ -39,7 +39,8 @@ import numpy as np
 from . import _lib
 from .ge2 import AxialSources, Ge2Table
 from .order0 import ElementBatch, Order0Optics, order0, raise_status as raise_order0_status
-from .order1 import Order1Tables, PromptSettings, acceptance_monomials, grouped, pencils
+from .order1 import (Order1Tables, PromptSettings, acceptance_monomials, element_box, grouped,
+                     pencils)
 from .readout import DeviceReadout
 from .source import ShowerBasisSettings, SourceCompiler, axis_frame
 
@@ -468,7 +469,8 @@ class ShowerTransport:
             if extra.shape != (n,) or not np.isfinite(extra).all():
                 raise ValueError("selection_extra_charge must hold one finite value per OM")
             first = int(np.argmin(el["start_ns"]))
-            distance0 = np.linalg.norm(el["start_m"] - el["start_m"][first], axis=1)
+            d0 = el["start_m"] - el["start_m"][first]
+            distance0 = np.sqrt(d0[:, 0] * d0[:, 0] + d0[:, 1] * d0[:, 1] + d0[:, 2] * d0[:, 2])
             delay = el["start_ns"] - el["start_ns"][first] - distance0 / C_M_PER_NS
             if np.any(delay > cfg.prompt_delay_ns):
                 raise NotImplementedError("delayed light groups (steps more than prompt_delay_ns "
@@ -491,7 +493,11 @@ class ShowerTransport:
         npts_all = torch.stack([c[2] for c in compiled]).cpu().numpy()
         if int(src_status.item()) & _lib.LH_STATUS_OVERFLOW:
             raise ValueError("element nodes fall outside the source lattice")
-        host_pts = [c[0].cpu().numpy() for c in compiled]
+        flat_pts = torch.cat([c[0].reshape(-1) for c in compiled]).cpu().numpy()
+        host_pts, at = [], 0
+        for c in compiled:
+            host_pts.append(flat_pts[at:at + c[0].numel()].reshape(c[0].shape))
+            at += c[0].numel()
         for ev, c, pts, npts in zip(events, compiled, host_pts, npts_all):
             _, ch_d, _, ev.reference, ev.frame = c
             ev.npts = npts
@@ -570,8 +576,13 @@ class ShowerTransport:
         for k, ev in enumerate(events):
             el = ev.el
             span = float(np.max(el["end_ns"]) - np.min(el["start_ns"]))
-            mid = el["start_m"] + 0.5 * el["length_m"][:, None] * el["direction"]
-            extent = float(np.linalg.norm(np.ptp(mid, axis=0)))
+            # midpoints lie inside the box of starts and ends: the exact extent is
+            # needed only when the box's extent passes the radial limit
+            low_box, high_box = ev.box = element_box(el)
+            extent = float(np.linalg.norm(high_box - low_box))
+            if extent > high:
+                mid = el["start_m"] + 0.5 * el["length_m"][:, None] * el["direction"]
+                extent = float(np.linalg.norm([np.ptp(mid[:, k]) for k in range(3)]))
             ev.local_origin = extent > high or span > 0.5 * time_width
             given = None if time_origin_ns is None else time_origin_ns[k]
             if given is not None:
@@ -590,6 +601,7 @@ class ShowerTransport:
             if not np.all(pvalid):
                 pel = _subset(el, pvalid)
             ev.prompt_el = pel
+            ev.prompt_box = ev.box if pel is el else element_box(pel)
         same = all(ev.prompt_el is ev.el for ev in events)
         prompt_store = store if same else ElementBatch([ev.prompt_el for ev in events], dev)
         dist, early = T.om_geometry_batch(prompt_store, store, fastest)
@@ -608,7 +620,7 @@ class ShowerTransport:
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         cone = float(np.sum(T.prompt["s0w"] * T.phase) / np.sum(T.prompt["s0w"]))
         for ev in prompt_events:
-            if not np.all(ev.prompt_el["beta"][:, None] * T.phase[None, :] > 1):
+            if not np.all(ev.prompt_el["beta"] * float(np.min(T.phase)) > 1):
                 raise NotImplementedError("elements above threshold in only some bands need the "
                                           "per-band order-1 units")
             ev.cone_cos = 1.0 / (ev.device_el["beta"] * cone)
@@ -621,7 +633,8 @@ class ShowerTransport:
                     lane = lanes[k % len(lanes)]
                     with torch.cuda.stream(lane.stream):
                         coarse = pencils(lane.order1_screen, ev.prompt_el, ev.cone_cos,
-                                         status=ev.status, device_elements=ev.device_el)
+                                         status=ev.status, device_elements=ev.device_el,
+                                         box=ev.prompt_box)
                         ev.pending["coarse"] = grouped(lane.order1_screen, coarse, ev.work,
                                                        ev.origins, status=ev.status)[0]
             if prompt_events:
@@ -657,7 +670,7 @@ class ShowerTransport:
                 lane = lanes[k % len(lanes)]
                 with torch.cuda.stream(lane.stream):
                     ev.table = pencils(lane.order1, ev.prompt_el, ev.cone_cos, status=ev.status,
-                                       device_elements=ev.device_el)
+                                       device_elements=ev.device_el, box=ev.prompt_box)
                     ev.pending["fine"] = grouped(lane.order1, ev.table, ev.fine, ev.origins,
                                                  status=ev.status)
         self._redo_overflow(prompt_events, "fine", T.order1)
@@ -679,7 +692,8 @@ class ShowerTransport:
                                       * np.maximum(coarse[ev.work], 0.0) >= threshold)]
                     if len(more):
                         table = pencils(T.order1, ev.prompt_el, ev.cone_cos, status=status,
-                                        device_elements=ev.device_el, capacity_full=True)
+                                        device_elements=ev.device_el, capacity_full=True,
+                                        box=ev.prompt_box)
                         q1m, b1m = grouped(T.order1, table, more, ev.origins, status=status)
                         ev.charge[more, 1] = q1m.cpu().numpy()[more]
                         ev.bins1[more] = b1m.cpu().numpy()[more]
@@ -743,7 +757,7 @@ class ShowerTransport:
             missing = np.flatnonzero(ev.active & (ev.level1 < 2))
             if len(missing):  # the reference reruns the prompt without its screen
                 table = pencils(T.order1, ev.prompt_el, 1.0 / (ev.prompt_el["beta"] * cone),
-                                status=status, capacity_full=True)
+                                status=status, capacity_full=True, box=ev.prompt_box)
                 q1m, b1m = grouped(T.order1, table, missing, ev.origins, status=status)
                 ev.charge[missing, 1] = q1m.cpu().numpy()[missing]
                 ev.bins1[missing] = b1m.cpu().numpy()[missing]
@@ -821,7 +835,7 @@ class ShowerTransport:
             if not f & _lib.LH_STATUS_OVERFLOW:
                 continue
             table = pencils(tables, ev.prompt_el, ev.cone_cos, device_elements=ev.device_el,
-                            capacity_full=True)
+                            capacity_full=True, box=ev.prompt_box)
             work = ev.work if key == "coarse" else ev.fine
             res = grouped(tables, table, work, ev.origins)
             ev.pending[key] = res[0] if key == "coarse" else res
@@ -842,9 +856,10 @@ class ShowerTransport:
         max_distance = T.radial[1]
         inside = distance <= max_distance
         s0 = 1.0 / T.wavelengths ** 2
-        density = (el["coefficient0"][:, None] * s0[None]
-                   + el["coefficient2"][:, None] * (s0 / T.phase ** 2)[None])
-        emitted = float(np.sum(T.weights[None, :] * np.maximum(density, 0.0)))
+        s2 = s0 / T.phase ** 2
+        emitted = float(sum(T.weights[b] * np.maximum(el["coefficient0"] * s0[b]
+                                                      + el["coefficient2"] * s2[b], 0.0).sum()
+                            for b in range(len(s0))))
         far = np.maximum(distance, 1e-9)
         upper = (10 * max(emitted, 0.0) * T.areas * T.peak_acceptance * float(np.max(T.efficiency))
                  * np.exp(-float(np.min(T.absorption)) * far) / (4 * np.pi * far ** 2))

@@ -52,9 +52,10 @@ def axis_frame(start, direction, length, weights):
     start, direction = np.asarray(start, float), np.asarray(direction, float)
     points = start + 0.5 * np.asarray(length, float)[:, None] * direction
     share = np.asarray(weights, float) / np.sum(weights)
-    centre = (share[:, None] * points).sum(axis=0)
+    weighted = share[:, None] * points
+    centre = np.array([weighted[:, k].sum() for k in range(3)])  # column sums (fast)
     offset = points - centre
-    covariance = np.einsum("i,ij,ik->jk", share, offset, offset)
+    covariance = (share[:, None] * offset).T @ offset
     values, vectors = np.linalg.eigh(covariance)
     if np.max(np.abs(values)) <= 1e-24:
         axis = np.sum(share[:, None] * direction, axis=0)
@@ -157,7 +158,8 @@ class SourceCompiler:
         start, direction, length = field("start_m"), field("direction"), field("length_m")
         c0, c2, beta = field("coefficient0"), field("coefficient2"), field("beta")
         t0, t1 = field("start_ns"), field("end_ns")
-        if np.any(beta[:, None] * self.phase[None, :] <= 1):
+        # rounding is monotone: beta n <= 1 for some band iff it holds at the smallest n
+        if np.any(beta * float(np.min(self.phase)) <= 1):
             raise NotImplementedError("device source compile needs every element above the "
                                       "Cherenkov threshold in every node band")
         if frame is None:
@@ -168,10 +170,13 @@ class SourceCompiler:
         x, w = np.polynomial.legendre.leggauss(order)
         fractions, weights = (x + 1) / 2, w / 2
         reference = float(t0.min())
-        z_mid = (start + 0.5 * length[:, None] * direction - centre) @ axis
+        # axial coordinates as start.axis + f length (direction.axis): matrix-vector
+        # products instead of (N, 3) temporaries (the lattice sizes only)
+        z_start = start @ axis - float(centre @ axis)
+        z_step = length * (direction @ axis)
+        z_mid = z_start + 0.5 * z_step
         z_origin = float(z_mid.min()) - 2 * s.cell_m
-        z_nodes = np.concatenate([(start + f * length[:, None] * direction - centre) @ axis
-                                  for f in fractions])
+        z_nodes = np.concatenate([z_start + f * z_step for f in fractions])
         t_nodes = np.concatenate([t0 + f * (t1 - t0) for f in fractions])
         kmax = int(np.floor((float(t_nodes.max()) - reference) / s.time_step_ns)) + 3
         zb = np.floor((z_nodes - z_origin) / s.cell_m)
