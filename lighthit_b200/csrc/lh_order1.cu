@@ -741,6 +741,7 @@ struct O1BatchShared {
   double t[kO1MaxNodes];
   double h[kO1MaxNodes];
   double mom[kO1MaxValues * 128];  // moments of the batch's theta groups (<= 128)
+  double sin_q[128], cos_q[128];   // per group: sin, cos of its mean angle (0, 0: empty)
   double coef[kO1MaxMono];
   int ipow[kO1MaxMono], jpow[kO1MaxMono];
   double red[kO1BatchThreads / 32];
@@ -854,6 +855,16 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
     const double r_b = S.stats[0], t_b = S.stats[1], front_extra = S.stats[2];
     const double sigma = S.stats[3], u_win = S.stats[4], u_end = S.stats[5];
     const int n_in = (int)S.stats[6], n_out = (int)S.stats[7];
+    // the groups' mean angles, once per batch (the profile loop below reads them
+    // for every path node)
+    for (int q = tid; q < count; q += blockDim.x) {
+      const double* row = S.mom + q * kO1MaxValues;
+      const double omega = row[2 * nm];
+      double sin_t = 0.0, cos_t = 0.0;
+      if (omega > 0.0) sincos(fmax(row[2 * nm + 1] / omega, 1e-9), &sin_t, &cos_t);
+      S.sin_q[q] = sin_t;
+      S.cos_q[q] = cos_t;
+    }
     for (int k = tid; k < n; k += blockDim.x) {
       double s;
       if (k == 0) s = r_b;
@@ -870,9 +881,7 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
         const double* row = S.mom + q * kO1MaxValues;
         const double omega = row[2 * nm];
         if (omega <= 0.0) continue;
-        const double theta = fmax(row[2 * nm + 1] / omega, 1e-9);
-        double sin_t, cos_t;
-        sincos(theta, &sin_t, &cos_t);
+        const double sin_t = S.sin_q[q], cos_t = S.cos_q[q];
         const double rs = r_b * sin_t;
         double c, s, path_jacobian;
         if (backward) {
