@@ -91,7 +91,7 @@ typedef struct {
   const double* omega;         /* [n_omega] rad/ns                                 */
   int32_t n_radii;
   const double* log_r;         /* [n_radii] log of table radii                     */
-  const float* coef;           /* float2 [n_radii-1][n_omega][acc_top+1][2][4]    */
+  const float* coef;           /* float2 [n_radii-1][acc_top+1][2][4][n_omega]    */
   double mu_a, mu_t;           /* absorption, extinction 1/m                       */
   double speed;                /* m/ns of the table's band                        */
   double origin_speed;         /* c / min group index (clock)                      */

@@ -151,19 +151,24 @@ LH_DEVICE void flash_item(const lh_flash_problem& p, const lh_flash_batch& b, in
   float2 s1 = make_float2(0.f, 0.f), s2 = make_float2(0.f, 0.f);
   if (s.j >= 0) {
     const int L = p.acc_top + 1;
-    const float4* c = reinterpret_cast<const float4*>(p.coef) +
-                      ((int64_t)s.j * p.n_omega + w) * L * 4;  // 8 float2 = 4 float4 per l
+    const int W = p.n_omega;
+    // [interval][degree][order][power][omega]: the lanes of a warp (consecutive
+    // omega) read consecutive float2, one coalesced segment per coefficient
+    const float2* c = reinterpret_cast<const float2*>(p.coef) + (int64_t)s.j * L * 8 * W + w;
     const float t = s.tt;
     for (int l = 0; l < L; ++l) {
-      const float4 a0 = __ldg(c + 4 * l + 0), a1 = __ldg(c + 4 * l + 1);  // order 1: c0..c3
-      const float4 b0 = __ldg(c + 4 * l + 2), b1 = __ldg(c + 4 * l + 3);  // order 2
-      float vr = fmaf(fmaf(fmaf(a0.x, t, a0.z), t, a1.x), t, a1.z);
-      float vi = fmaf(fmaf(fmaf(a0.y, t, a0.w), t, a1.y), t, a1.w);
+      const float2* cl = c + (int64_t)l * 8 * W;
+      const float2 a0 = __ldg(cl), a1 = __ldg(cl + W), a2 = __ldg(cl + 2 * W),
+                   a3 = __ldg(cl + 3 * W);  // order 1: c0..c3
+      const float2 b0 = __ldg(cl + 4 * W), b1 = __ldg(cl + 5 * W), b2 = __ldg(cl + 6 * W),
+                   b3 = __ldg(cl + 7 * W);  // order 2
+      float vr = fmaf(fmaf(fmaf(a0.x, t, a1.x), t, a2.x), t, a3.x);
+      float vi = fmaf(fmaf(fmaf(a0.y, t, a1.y), t, a2.y), t, a3.y);
       const float wl = s.w[l];
       s1.x = fmaf(wl, vr, s1.x);
       s1.y = fmaf(wl, vi, s1.y);
-      vr = fmaf(fmaf(fmaf(b0.x, t, b0.z), t, b1.x), t, b1.z);
-      vi = fmaf(fmaf(fmaf(b0.y, t, b0.w), t, b1.y), t, b1.w);
+      vr = fmaf(fmaf(fmaf(b0.x, t, b1.x), t, b2.x), t, b3.x);
+      vi = fmaf(fmaf(fmaf(b0.y, t, b1.y), t, b2.y), t, b3.y);
       s2.x = fmaf(wl, vr, s2.x);
       s2.y = fmaf(wl, vi, s2.y);
     }
@@ -397,19 +402,37 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
     const uint32_t lane_addr = tmem + ((uint32_t)(q * 32) << 16);
     float* dst = b.components + ((base + lp) * 3 + order) * (int64_t)n_bins;
     const bool vec = (n_bins & 3) == 0;
+    // The A tile is free once the MMA has completed: each warp transposes its
+    // 32 rows x 16 bins through a 32 x 20-float slice of it, so that four
+    // lanes store one row's 64 bytes and a store instruction covers eight rows
+    // (full 32-byte sectors) instead of 32 rows at a 16-byte stride.
+    float* stage = reinterpret_cast<float*>(smem) + warp * 32 * 20;
+    const bool staged = vec && 2u * a_bytes >= (blockDim.x / 32) * 32u * 20u * sizeof(float);
     for (int c = c_begin; c < c_end; ++c) {
       float v[16];
       tmem_ld16(lane_addr + (uint32_t)(c * 16), v);
-      if (valid) {
-        if (vec && c * 16 + 16 <= n_bins) {
-          float4* d4 = reinterpret_cast<float4*>(dst + c * 16);
+      if (staged && c * 16 + 16 <= n_bins) {
 #pragma unroll
-          for (int i = 0; i < 4; ++i) d4[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-        } else {
+        for (int i = 0; i < 4; ++i)
+          *reinterpret_cast<float4*>(stage + lane * 20 + 4 * i) =
+              make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        __syncwarp();
 #pragma unroll
-          for (int i = 0; i < 16; ++i)
-            if (c * 16 + i < n_bins) dst[c * 16 + i] = v[i];
+        for (int it = 0; it < 4; ++it) {
+          const int r = it * 8 + (lane >> 2), part = lane & 3;
+          const int trow = q * 32 + r;
+          const int tlp = trow >> 1, torder = 1 + (trow & 1);
+          if (sp[tlp].valid) {
+            const float4 x = *reinterpret_cast<const float4*>(stage + r * 20 + 4 * part);
+            *reinterpret_cast<float4*>(b.components + ((base + tlp) * 3 + torder) * (int64_t)n_bins +
+                                       c * 16 + 4 * part) = x;
+          }
         }
+        __syncwarp();
+      } else if (valid) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (c * 16 + i < n_bins) dst[c * 16 + i] = v[i];
       }
     }
     tc_fence_before();

@@ -121,7 +121,10 @@ class FlashTransport:
         self._alpha = f64(alpha[:top + 1])
         self._omega = f64(omega)
         self._log_r = f64(np.log(table.radii_m))
-        coef = table.spline_table(top).astype(np.complex64)
+        # device layout (interval, degree, order, power, omega): omega fastest, so
+        # a warp's lanes (consecutive frequencies) read each coefficient coalesced
+        coef = np.ascontiguousarray(
+            table.spline_table(top).astype(np.complex64).transpose(0, 2, 3, 4, 1))
         self._coef = torch.view_as_real(torch.from_numpy(coef)).contiguous().to(dev)
         self._edges = f64(config.relative_time_edges_ns)
         self.readout = DeviceReadout(omega, config.relative_time_edges_ns,
