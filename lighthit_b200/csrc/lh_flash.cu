@@ -297,8 +297,9 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
   __nv_bfloat16* s_alo = reinterpret_cast<__nv_bfloat16*>(smem + a_bytes);
   __nv_bfloat16* s_bhi = reinterpret_cast<__nv_bfloat16*>(smem + 2 * a_bytes);
   __nv_bfloat16* s_blo = reinterpret_cast<__nv_bfloat16*>(smem + 2 * a_bytes + b_bytes);
-  FlashPair* sp = reinterpret_cast<FlashPair*>(smem + 2 * a_bytes + 2 * b_bytes);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sp + kFlashPairs);
+  // two pair buffers: the next tile's setup runs while this tile's MMA is in flight
+  FlashPair* sp_buf = reinterpret_cast<FlashPair*>(smem + 2 * a_bytes + 2 * b_bytes);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sp_buf + 2 * kFlashPairs);
   uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 2);
   uint64_t* bar_b = bars;
   uint64_t* bar_mma = bars + 1;
@@ -331,15 +332,17 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
   uint32_t ph_mma = 0;
   bool b_ready = false, failed = false, mma_pending = false;
 
+  if (blockIdx.x < n_tiles) flash_tile_setup(p, b, sp_buf, blockIdx.x * kFlashPairs, n_pairs);
+  __syncthreads();
+  int cur = 0;
   for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
     const int64_t base = tile * kFlashPairs;
-    flash_tile_setup(p, b, sp, base, n_pairs);
+    FlashPair* sp = sp_buf + cur * kFlashPairs;  // set up before the barrier closing the last tile
     for (int i = tid; i < 128 * padw; i += blockDim.x) {
       const int off = tile_offset(i / padw, 2 * nw + i % padw);
       s_ahi[off] = __float2bfloat16_rn(0.f);
       s_alo[off] = __float2bfloat16_rn(0.f);
     }
-    __syncthreads();
     for (int i = tid; i < kFlashPairs * nw; i += blockDim.x) {
       const int lp = i / nw, w = i % nw;
       float2 r1, r2;
@@ -384,6 +387,11 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
         failed = true;
       }
     }
+    // the next tile's pair setup (two warps, float64) overlaps the MMA and this
+    // tile's order-0 stores
+    const int64_t next = tile + gridDim.x;
+    if (next < n_tiles)
+      flash_tile_setup(p, b, sp_buf + (cur ^ 1) * kFlashPairs, next * kFlashPairs, n_pairs);
     flash_tile_order0(p, b, sp, base, n_bins);
     if (__syncthreads_or(failed)) { failed = true; break; }
     const bool ok = mbar_wait(bar_mma, ph_mma);
@@ -437,6 +445,7 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
     }
     tc_fence_before();
     __syncthreads();
+    cur ^= 1;
   }
   if (failed && tid == 0) atomicOr(reinterpret_cast<unsigned*>(b.status), LH_STATUS_TIMEOUT);
   if (mma_pending) mbar_wait(bar_mma, ph_mma ^ 1u);
@@ -447,7 +456,7 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
 }
 
 size_t flash_tc_smem_bytes(int kpad, int n_tile) {
-  return 2ull * 128 * kpad * 2 + 2ull * n_tile * kpad * 2 + sizeof(FlashPair) * kFlashPairs + 64;
+  return 2ull * 128 * kpad * 2 + 2ull * n_tile * kpad * 2 + 2 * sizeof(FlashPair) * kFlashPairs + 64;
 }
 
 }  // namespace lh
