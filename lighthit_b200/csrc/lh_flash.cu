@@ -196,11 +196,13 @@ LH_DEVICE void flash_item(const lh_flash_problem& p, const lh_flash_batch& b, in
 }
 
 // Step 3 (order 0 and the mask) for the tile's pairs.
+// `threads`: the first threads of the CTA that take part (0: all).
 LH_DEVICE void flash_tile_order0(const lh_flash_problem& p, const lh_flash_batch& b,
-                                 const FlashPair* sp, int64_t base, int n_bins) {
+                                 const FlashPair* sp, int64_t base, int n_bins, int threads = 0) {
+  const int stride = threads ? threads : (int)blockDim.x;
   if ((n_bins & 3) == 0) {  // rows are 16-byte aligned: four bins per store
     const int quads = n_bins >> 2;
-    for (int i = threadIdx.x; i < kFlashPairs * quads; i += blockDim.x) {
+    for (int i = threadIdx.x; i < kFlashPairs * quads; i += stride) {
       const int lp = i / quads, bin = (i % quads) * 4;
       const FlashPair& s = sp[lp];
       if (!s.valid) continue;
@@ -210,7 +212,7 @@ LH_DEVICE void flash_tile_order0(const lh_flash_problem& p, const lh_flash_batch
       *reinterpret_cast<float4*>(b.components + ((base + lp) * 3) * n_bins + bin) = v;
     }
   } else {
-    for (int i = threadIdx.x; i < kFlashPairs * n_bins; i += blockDim.x) {
+    for (int i = threadIdx.x; i < kFlashPairs * n_bins; i += stride) {
       const int lp = i / n_bins, bin = i % n_bins;
       const FlashPair& s = sp[lp];
       if (!s.valid) continue;
@@ -230,23 +232,25 @@ LH_DEVICE void flash_tile_order0(const lh_flash_problem& p, const lh_flash_batch
   }
 }
 
+LH_DEVICE void flash_slot_setup(const lh_flash_problem& p, const lh_flash_batch& b, FlashPair& s,
+                                int64_t pair, int64_t n_pairs) {
+  if (pair < n_pairs) {
+    flash_pair_setup(p, b, pair, s);
+  } else {
+    s.valid = 0;
+    s.j = -1;
+    s.amp12 = s.amp0 = 0.f;
+    s.t12 = s.t0 = s.origin = 0.0;
+    s.inside = 0;
+    s.flags = 0;
+  }
+  s.charge[0] = s.charge[1] = s.charge[2] = 0.f;
+}
+
 LH_DEVICE void flash_tile_setup(const lh_flash_problem& p, const lh_flash_batch& b, FlashPair* sp,
                                 int64_t base, int64_t n_pairs) {
-  if (threadIdx.x < kFlashPairs) {
-    FlashPair& s = sp[threadIdx.x];
-    const int64_t pair = base + threadIdx.x;
-    if (pair < n_pairs) {
-      flash_pair_setup(p, b, pair, s);
-    } else {
-      s.valid = 0;
-      s.j = -1;
-      s.amp12 = s.amp0 = 0.f;
-      s.t12 = s.t0 = s.origin = 0.0;
-      s.inside = 0;
-      s.flags = 0;
-    }
-    s.charge[0] = s.charge[1] = s.charge[2] = 0.f;
-  }
+  if (threadIdx.x < kFlashPairs)
+    flash_slot_setup(p, b, sp[threadIdx.x], base + threadIdx.x, n_pairs);
 }
 
 // ---------------------------------------------------------------- plain path
@@ -343,23 +347,35 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
       s_ahi[off] = __float2bfloat16_rn(0.f);
       s_alo[off] = __float2bfloat16_rn(0.f);
     }
-    for (int i = tid; i < kFlashPairs * nw; i += blockDim.x) {
-      const int lp = i / nw, w = i % nw;
-      float2 r1, r2;
-      flash_item(p, b, base + lp, w, sp[lp], r1, r2);
-      __nv_bfloat16 hi, lo;
-      split_bf16(r1.x, hi, lo);
-      s_ahi[tile_offset(2 * lp, w)] = hi;       s_alo[tile_offset(2 * lp, w)] = lo;
-      split_bf16(r1.y, hi, lo);
-      s_ahi[tile_offset(2 * lp, nw + w)] = hi;  s_alo[tile_offset(2 * lp, nw + w)] = lo;
-      split_bf16(r2.x, hi, lo);
-      s_ahi[tile_offset(2 * lp + 1, w)] = hi;   s_alo[tile_offset(2 * lp + 1, w)] = lo;
-      split_bf16(r2.y, hi, lo);
-      s_ahi[tile_offset(2 * lp + 1, nw + w)] = hi; s_alo[tile_offset(2 * lp + 1, nw + w)] = lo;
+    // The last warp sets up the next tile's pairs (float64, two per lane) while
+    // the other warps compute this tile's spectra, then issues the MMAs while
+    // they write the order-0 rows: neither waits behind the other.
+    const int64_t next = tile + gridDim.x;
+    const int workers = blockDim.x - 32;
+    if (tid >= workers) {
+      if (next < n_tiles)
+        for (int k = lane; k < kFlashPairs; k += 32)
+          flash_slot_setup(p, b, sp_buf[(cur ^ 1) * kFlashPairs + k], next * kFlashPairs + k,
+                           n_pairs);
+    } else {
+      for (int i = tid; i < kFlashPairs * nw; i += workers) {
+        const int lp = i / nw, w = i % nw;
+        float2 r1, r2;
+        flash_item(p, b, base + lp, w, sp[lp], r1, r2);
+        __nv_bfloat16 hi, lo;
+        split_bf16(r1.x, hi, lo);
+        s_ahi[tile_offset(2 * lp, w)] = hi;       s_alo[tile_offset(2 * lp, w)] = lo;
+        split_bf16(r1.y, hi, lo);
+        s_ahi[tile_offset(2 * lp, nw + w)] = hi;  s_alo[tile_offset(2 * lp, nw + w)] = lo;
+        split_bf16(r2.x, hi, lo);
+        s_ahi[tile_offset(2 * lp + 1, w)] = hi;   s_alo[tile_offset(2 * lp + 1, w)] = lo;
+        split_bf16(r2.y, hi, lo);
+        s_ahi[tile_offset(2 * lp + 1, nw + w)] = hi; s_alo[tile_offset(2 * lp + 1, nw + w)] = lo;
+      }
     }
     fence_proxy_async();  // generic-proxy smem writes -> visible to the tensor core
     __syncthreads();
-    if (tid == 0) {
+    if (tid == workers) {
       bool ok = true;
       if (!b_ready) {
         ok = mbar_wait(bar_b, 0);
@@ -387,12 +403,7 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
         failed = true;
       }
     }
-    // the next tile's pair setup (two warps, float64) overlaps the MMA and this
-    // tile's order-0 stores
-    const int64_t next = tile + gridDim.x;
-    if (next < n_tiles)
-      flash_tile_setup(p, b, sp_buf + (cur ^ 1) * kFlashPairs, next * kFlashPairs, n_pairs);
-    flash_tile_order0(p, b, sp, base, n_bins);
+    if (tid < workers) flash_tile_order0(p, b, sp, base, n_bins, workers);
     if (__syncthreads_or(failed)) { failed = true; break; }
     const bool ok = mbar_wait(bar_mma, ph_mma);
     ph_mma ^= 1u;
@@ -449,7 +460,7 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
   }
   if (failed && tid == 0) atomicOr(reinterpret_cast<unsigned*>(b.status), LH_STATUS_TIMEOUT);
   if (mma_pending) mbar_wait(bar_mma, ph_mma ^ 1u);
-  if (tid == 0 && !b_ready) mbar_wait(bar_b, 0);  // never leave a bulk copy in flight
+  if (tid == blockDim.x - 32 && !b_ready) mbar_wait(bar_b, 0);  // no bulk copy left in flight
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, 256);
