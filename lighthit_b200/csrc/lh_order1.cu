@@ -734,18 +734,23 @@ LH_DEVICE void o1_deposit_panel(double t_a, double t_b, double e_a, double e_b, 
   }
 }
 
+struct O1BandDeposit {
+  double v, kappa, spread, t_base, e_emit, w0, w2, h_front, total;
+  int last, pairs, panels;
+  bool outside;
+};
+
 struct O1BatchShared {
   double s[kO1MaxNodes];
   double g0[kO1MaxNodes];
   double g2[kO1MaxNodes];
-  double t[kO1MaxNodes];
-  double h[kO1MaxNodes];
   double mom[kO1MaxValues * 128];  // moments of the batch's theta groups (<= 128)
   double sin_q[128], cos_q[128];   // per group: sin, cos of its mean angle (0, 0: empty)
   double coef[kO1MaxMono];
   int ipow[kO1MaxMono], jpow[kO1MaxMono];
   double red[kO1BatchThreads / 32];
   double stats[8];
+  O1BandDeposit band[kO1MaxBands];
   int n, last;
 };
 
@@ -919,108 +924,123 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
       S.g2[k] = a2s;
     }
     __syncthreads();
-    // _batch_deposit (_prompt_numba.py:451-551), every band
+    // _batch_deposit (_prompt_numba.py:451-551) for every band at once: the
+    // band constants in shared memory, node times and profile values evaluated
+    // from the path grid on the fly, (band, panel) items over the whole CTA,
+    // then each band's front ramp by its own thread
     const int d = work[w];
     double* accw = accum + (int64_t)w * per_om;
-    for (int lam = 0; lam < NL; ++lam) {
-      if (C.mus[lam] == 0.0) continue;
-      const double v = C.speed[lam];
-      const double kappa = -C.mut[lam] * v;
-      int last = n - 1;
-      const double limit = r_b + C.tail_exponent / C.mut[lam];
-      while (last > 2 && S.s[last - 1] > limit) last -= 1;
-      if (last < 2) continue;
-      const double spread = fmin(front_extra, (S.s[last] - r_b) / v);
-      const double front_time = t_b + r_b / v;
-      const double end_time = t_b + S.s[last] / v;
-      const bool outside = front_time - 0.5 * spread >= C.edges[nb] ||
-                           end_time + 0.5 * spread <= C.edges[0];
-      const double t_base = outside ? 0.0 : t_b;
-      const double e_emit = exp(kappa * t_base);
-      const double h_scale = C.mus[lam] * v / e_emit;
-      const double w0 = C.s0w[lam] * h_scale, w2 = C.s2w[lam] * h_scale;
-      for (int j = tid; j <= last; j += blockDim.x) {
-        S.t[j] = t_base + S.s[j] / v;
-        S.h[j] = w0 * S.g0[j] + w2 * S.g2[j];
+    const bool bins = C.compute_bins != 0;
+    if (tid < NL) {
+      const int lam = tid;
+      O1BandDeposit& B = S.band[lam];
+      B.panels = 0;
+      B.total = 0.0;
+      if (C.mus[lam] != 0.0) {
+        const double v = C.speed[lam];
+        int last = n - 1;
+        const double limit = r_b + C.tail_exponent / C.mut[lam];
+        while (last > 2 && S.s[last - 1] > limit) last -= 1;
+        if (last >= 2) {
+          B.v = v;
+          B.kappa = -C.mut[lam] * v;
+          B.last = last;
+          B.spread = fmin(front_extra, (S.s[last] - r_b) / v);
+          const double front_time = t_b + r_b / v;
+          const double end_time = t_b + S.s[last] / v;
+          B.outside = front_time - 0.5 * B.spread >= C.edges[nb] ||
+                      end_time + 0.5 * B.spread <= C.edges[0];
+          B.t_base = B.outside ? 0.0 : t_b;
+          B.e_emit = exp(B.kappa * B.t_base);
+          const double h_scale = C.mus[lam] * v / B.e_emit;
+          B.w0 = C.s0w[lam] * h_scale;
+          B.w2 = C.s2w[lam] * h_scale;
+          B.h_front = B.w0 * S.g0[0] + B.w2 * S.g2[0];
+          // panels start at even nodes with step 2; an odd `last` ends with one step
+          B.pairs = last / 2;
+          B.panels = B.pairs + (last & 1);
+        }
       }
-      __syncthreads();
-      const double h_front = S.h[0];
-      __syncthreads();
-      for (int j = tid; j <= last; j += blockDim.x) S.h[j] -= h_front;
-      __syncthreads();
+    }
+    __syncthreads();
+    int n_items = 0;
+    for (int lam = 0; lam < NL; ++lam) n_items += S.band[lam].panels;
+    for (int item = tid; item < n_items; item += blockDim.x) {
+      int lam = 0, pi = item;
+      while (pi >= S.band[lam].panels) pi -= S.band[lam].panels, ++lam;
+      const O1BandDeposit& B = S.band[lam];
+      const double v = B.v, mut = C.mut[lam];
+      auto node_t = [&](int j) { return B.t_base + S.s[j] / v; };
+      auto node_h = [&](int j) { return (B.w0 * S.g0[j] + B.w2 * S.g2[j]) - B.h_front; };
+      double t_a, t_b2, alpha, beta, gamma, e_a, e_b;
+      if (pi < B.pairs) {
+        const int j = 2 * pi;
+        t_a = node_t(j);
+        const double t_m = node_t(j + 1);
+        t_b2 = node_t(j + 2);
+        const double h0 = node_h(j), h1 = node_h(j + 1), h2 = node_h(j + 2);
+        const double u_m = t_m - t_a, u_b = t_b2 - t_a;
+        const double d1 = (h1 - h0) / u_m;
+        const double d2 = ((h2 - h1) / (t_b2 - t_m) - d1) / u_b;
+        alpha = h0;
+        beta = d1 - d2 * u_m;
+        gamma = d2;
+        e_a = B.e_emit * exp(-mut * S.s[j]);
+        e_b = B.e_emit * exp(-mut * S.s[j + 2]);
+      } else {
+        const int j = B.last - 1;
+        const double t_p = node_t(j - 1);
+        t_a = node_t(j);
+        t_b2 = node_t(j + 1);
+        const double hp = node_h(j - 1), h0 = node_h(j), h1 = node_h(j + 1);
+        const double u_m = t_a - t_p, u_b = t_b2 - t_p;
+        const double d1 = (h0 - hp) / u_m;
+        const double d2 = ((h1 - h0) / (t_b2 - t_a) - d1) / u_b;
+        alpha = h0;
+        beta = d1 - d2 * u_m + 2.0 * d2 * u_m;
+        gamma = d2;
+        e_a = B.e_emit * exp(-mut * S.s[j]);
+        e_b = B.e_emit * exp(-mut * S.s[j + 1]);
+      }
+      atomicAdd(&S.band[lam].total, o1_quad(e_a, alpha, beta, gamma, t_b2 - t_a, B.kappa, e_b));
+      if (bins && !B.outside) {
+        double* pre = accw + (int64_t)lam * (3 + 4 * nb + 1);
+        o1_deposit_panel(t_a, t_b2, e_a, e_b, alpha, beta, gamma, B.kappa, C.edges,
+                         C.eedge + (int64_t)lam * C.n_edges, nb, pre, pre + 3, C.direct_bins);
+      }
+    }
+    __syncthreads();
+    if (tid < NL && S.band[tid].panels > 0) {
+      const int lam = tid;
+      const O1BandDeposit& B = S.band[lam];
       const double* eedge = C.eedge + (int64_t)lam * C.n_edges;
       double* pre = accw + (int64_t)lam * (3 + 4 * nb + 1);
       double* acc = pre + 3;
       double* chg = acc + 4 * nb;
-      const bool bins = C.compute_bins != 0;
-      // panels start at even nodes with step 2; an odd `last` ends with one step
-      const int n_pairs = last / 2;
-      const int n_panels = n_pairs + (last & 1);
-      double total = 0.0;
-      for (int pi = tid; pi < n_panels; pi += blockDim.x) {
-        double t_a, t_b2, alpha, beta, gamma, e_a, e_b;
-        if (pi < n_pairs) {
-          const int j = 2 * pi;
-          t_a = S.t[j];
-          const double t_m = S.t[j + 1];
-          t_b2 = S.t[j + 2];
-          const double u_m = t_m - t_a, u_b = t_b2 - t_a;
-          const double d1 = (S.h[j + 1] - S.h[j]) / u_m;
-          const double d2 = ((S.h[j + 2] - S.h[j + 1]) / (t_b2 - t_m) - d1) / u_b;
-          alpha = S.h[j];
-          beta = d1 - d2 * u_m;
-          gamma = d2;
-          e_a = e_emit * exp(-C.mut[lam] * S.s[j]);
-          e_b = e_emit * exp(-C.mut[lam] * S.s[j + 2]);
-        } else {
-          const int j = last - 1;
-          const double t_p = S.t[j - 1];
-          t_a = S.t[j];
-          t_b2 = S.t[j + 1];
-          const double u_m = t_a - t_p, u_b = t_b2 - t_p;
-          const double d1 = (S.h[j] - S.h[j - 1]) / u_m;
-          const double d2 = ((S.h[j + 1] - S.h[j]) / (t_b2 - t_a) - d1) / u_b;
-          alpha = S.h[j];
-          beta = d1 - d2 * u_m + 2.0 * d2 * u_m;
-          gamma = d2;
-          e_a = e_emit * exp(-C.mut[lam] * S.s[j]);
-          e_b = e_emit * exp(-C.mut[lam] * S.s[j + 1]);
-        }
-        total += o1_quad(e_a, alpha, beta, gamma, t_b2 - t_a, kappa, e_b);
-        if (bins && !outside)
-          o1_deposit_panel(t_a, t_b2, e_a, e_b, alpha, beta, gamma, kappa, C.edges, eedge, nb,
+      double sum = B.total;
+      // front step as a mass-normalised ramp of width `spread`
+      const double e_first = B.e_emit * exp(-C.mut[lam] * S.s[0]);
+      const double e_last = B.e_emit * exp(-C.mut[lam] * S.s[B.last]);
+      const double t_f = B.t_base + S.s[0] / B.v, t_end = B.t_base + S.s[B.last] / B.v;
+      const double h_front = B.h_front, spread = B.spread, kappa = B.kappa;
+      const double exact = o1_quad(e_first, h_front, 0.0, 0.0, t_end - t_f, kappa, e_last);
+      sum += exact;
+      if (bins && spread > 0.0 && !B.outside) {
+        const double t_1 = t_f - 0.5 * spread, t_2 = t_f + 0.5 * spread;
+        const double e_1 = exp(kappa * t_1), e_2 = exp(kappa * t_2);
+        const double ramp = o1_quad(e_1, 0.0, 1.0 / spread, 0.0, spread, kappa, e_2);
+        const double flat = t_end > t_2 ? o1_quad(e_2, 1.0, 0.0, 0.0, t_end - t_2, kappa, e_last) : 0.0;
+        const double height = ramp + flat != 0.0 ? exact / (ramp + flat) : 0.0;
+        o1_deposit_panel(t_1, t_2, e_1, e_2, 0.0, height / spread, 0.0, kappa, C.edges, eedge,
+                         nb, pre, acc, C.direct_bins);
+        if (t_end > t_2)
+          o1_deposit_panel(t_2, t_end, e_2, e_last, height, 0.0, 0.0, kappa, C.edges, eedge, nb,
                            pre, acc, C.direct_bins);
+      } else if (bins && t_end > t_f && !B.outside) {
+        o1_deposit_panel(t_f, t_end, e_first, e_last, h_front, 0.0, 0.0, kappa, C.edges, eedge,
+                         nb, pre, acc, C.direct_bins);
       }
-      for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
-      if ((tid & 31) == 0) S.red[tid >> 5] = total;
-      __syncthreads();
-      if (tid == 0) {
-        double sum = 0.0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) sum += S.red[k];
-        // front step as a mass-normalised ramp of width `spread`
-        const double e_first = e_emit * exp(-C.mut[lam] * S.s[0]);
-        const double e_last = e_emit * exp(-C.mut[lam] * S.s[last]);
-        const double t_f = S.t[0], t_end = S.t[last];
-        const double exact = o1_quad(e_first, h_front, 0.0, 0.0, t_end - t_f, kappa, e_last);
-        sum += exact;
-        if (bins && spread > 0.0 && !outside) {
-          const double t_1 = t_f - 0.5 * spread, t_2 = t_f + 0.5 * spread;
-          const double e_1 = exp(kappa * t_1), e_2 = exp(kappa * t_2);
-          const double ramp = o1_quad(e_1, 0.0, 1.0 / spread, 0.0, spread, kappa, e_2);
-          const double flat = t_end > t_2 ? o1_quad(e_2, 1.0, 0.0, 0.0, t_end - t_2, kappa, e_last) : 0.0;
-          const double height = ramp + flat != 0.0 ? exact / (ramp + flat) : 0.0;
-          o1_deposit_panel(t_1, t_2, e_1, e_2, 0.0, height / spread, 0.0, kappa, C.edges, eedge,
-                           nb, pre, acc, C.direct_bins);
-          if (t_end > t_2)
-            o1_deposit_panel(t_2, t_end, e_2, e_last, height, 0.0, 0.0, kappa, C.edges, eedge, nb,
-                             pre, acc, C.direct_bins);
-        } else if (bins && t_end > t_f && !outside) {
-          o1_deposit_panel(t_f, t_end, e_first, e_last, h_front, 0.0, 0.0, kappa, C.edges, eedge,
-                           nb, pre, acc, C.direct_bins);
-        }
-        atomicAdd(chg, sum);
-      }
-      __syncthreads();
+      atomicAdd(chg, sum);
     }
     (void)d;
   }

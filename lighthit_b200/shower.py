@@ -58,6 +58,7 @@ class ShowerSettings:
     predictor_cell_m: float = 2.0
     predictor_safety: float = 2.0
     prompt_delay_ns: float = 20.0
+    delayed_cell_ns: float = 20.0        # ShowerConfig.delayed_cell_ns
     min_distance_m: float = 0.1          # PromptConfig.min_distance_m
     readout_mode: str = "split-bf16"
     # Gauss order of the order-0 ray quadrature (wavelength, along-track and
@@ -153,6 +154,7 @@ class ShowerTables:
         if self.radial[0] < low_c - 1e-9 or self.radial[1] > high_c + 1e-9:
             raise ValueError("radial window must lie inside the kernel cache")
         self.readout = DeviceReadout(self.omega, self.edges, self.readout_omega, device=device)
+        self._shifted_readout = {}
         self._pos = torch.tensor(self.positions, dtype=torch.float64, device=self.device)
         # spectral_attenuation (shower_basis.py:388-405) for the far-tail screen
         w = self.weights * self.efficiency / self.wavelengths ** 2
@@ -192,6 +194,15 @@ class ShowerTables:
             _lib.check(_lib.load().lh_om_geometry(C.byref(g), sp), "lh_om_geometry")
             out.append(res)
         return out[0].cpu().numpy(), out[1].cpu().numpy()
+
+    def readout_shifted(self, shift_ns):
+        """The readout operator on the window edges seen from a delay ``shift_ns``
+        (``edges - shift``: a delayed group's light read on its own clock)."""
+        key = float(shift_ns)
+        if key not in self._shifted_readout:
+            self._shifted_readout[key] = DeviceReadout(self.omega, self.edges - key,
+                                                       self.readout_omega, device=self.device)
+        return self._shifted_readout[key]
 
     def radial_window(self, compiled):
         """Per (event, node band, OM): basis points inside / beyond the radial range
@@ -267,6 +278,29 @@ def _concat_elements(events):
     cat = {k: np.concatenate([np.asarray(e[k], float) for e in events])
            for k in ("start_m", "direction", "length_m", "start_ns")}
     return offsets, cat
+
+
+def delay_groups(el, *, prompt_delay_ns, cell_ns, window_end_ns, group_index_max):
+    """``delay_groups`` (``shower/ge2.py:122-147``): steps split by their delay
+    behind the light front of the earliest step. Prompt steps (delay <=
+    ``prompt_delay_ns``) keep the source's clock; later steps are grouped in
+    ``cell_ns`` cells, each shifted by its smallest delay, unless none of their
+    light can arrive before the window ends (``beyond``: charge only).
+    Returns ``(prompt_mask, [(mask, shift_ns)], beyond_mask)``."""
+    first = int(np.argmin(el["start_ns"]))
+    d0 = el["start_m"] - el["start_m"][first]
+    distance = np.sqrt(d0[:, 0] * d0[:, 0] + d0[:, 1] * d0[:, 1] + d0[:, 2] * d0[:, 2])
+    delay = el["start_ns"] - el["start_ns"][first] - distance / C_M_PER_NS
+    prompt = delay <= prompt_delay_ns
+    beyond = ~prompt & (delay - (group_index_max - 1.0) * distance / C_M_PER_NS > window_end_ns)
+    within = ~prompt & ~beyond
+    groups = []
+    if np.any(within):
+        cells = np.floor(delay / cell_ns).astype(np.int64)
+        for cell in np.unique(cells[within]):
+            mask = within & (cells == cell)
+            groups.append((mask, float(delay[mask].min())))
+    return prompt, groups, beyond
 
 
 def elements_of(source):
@@ -468,16 +502,21 @@ class ShowerTransport:
             extra = np.zeros(n) if given is None else np.maximum(np.asarray(given, float), 0.0)
             if extra.shape != (n,) or not np.isfinite(extra).all():
                 raise ValueError("selection_extra_charge must hold one finite value per OM")
-            first = int(np.argmin(el["start_ns"]))
-            d0 = el["start_m"] - el["start_m"][first]
-            distance0 = np.sqrt(d0[:, 0] * d0[:, 0] + d0[:, 1] * d0[:, 1] + d0[:, 2] * d0[:, 2])
-            delay = el["start_ns"] - el["start_ns"][first] - distance0 / C_M_PER_NS
-            if np.any(delay > cfg.prompt_delay_ns):
-                raise NotImplementedError("delayed light groups (steps more than prompt_delay_ns "
-                                          "behind the light front) are not on the device route")
+            prompt, late_groups, beyond = delay_groups(
+                el, prompt_delay_ns=float(cfg.prompt_delay_ns), cell_ns=float(cfg.delayed_cell_ns),
+                window_end_ns=float(edges[-1]), group_index_max=float(np.max(T.group)))
             ev = _Event(el, extra)
-            ev.frame = axis_frame(el["start_m"], el["direction"], el["length_m"],
-                                  el["coefficient0"])
+            # the order >=2 source of the prompt steps (orders 0 and 1 take every step)
+            ev.src_el = el if np.all(prompt) else _subset(el, prompt)
+            ev.late = None
+            if not np.all(prompt):  # delayed light (shower/api.py:294-310)
+                ev.late = {"zero_el": _subset(el, ~prompt),
+                           "group_el": [(_subset(el, m), shift) for m, shift in late_groups],
+                           "steps_in_groups": int(sum(int(m.sum()) for m, _ in late_groups)),
+                           "beyond": int(beyond.sum())}
+            src = ev.src_el
+            ev.frame = axis_frame(src["start_m"], src["direction"], src["length_m"],
+                                  src["coefficient0"])
             events.append(ev)
         store = ElementBatch([ev.el for ev in events], dev)  # one upload for every stage
         stage("setup")
@@ -488,8 +527,9 @@ class ShowerTransport:
             for k, ev in enumerate(events):
                 lane = lanes[k % len(lanes)]
                 with torch.cuda.stream(lane.stream):
-                    compiled.append(lane.source.compile(ev.el, ev.frame, status=src_status,
-                                                        device_elements=store.event(k)))
+                    compiled.append(lane.source.compile(
+                        ev.src_el, ev.frame, status=src_status,
+                        device_elements=store.event(k) if ev.src_el is ev.el else None))
         npts_all = torch.stack([c[2] for c in compiled]).cpu().numpy()
         if int(src_status.item()) & _lib.LH_STATUS_OVERFLOW:
             raise ValueError("element nodes fall outside the source lattice")
@@ -515,19 +555,34 @@ class ShowerTransport:
                 parts.append(zero_host[pos:pos + int(ev.npts[b])])
                 pos += int(ev.npts[b])
             ev.zero_ch = parts
+        for ev in events:  # delayed parts: their own frames and lattices (rare)
+            if ev.late is None:
+                continue
+            ev.late["zero"] = self._part(T.source, ev.late["zero_el"])
+            ev.late["groups"] = [(self._part(T.source, part), shift)
+                                 for part, shift in ev.late["group_el"]]
         stage("source_compile")
         # ---- radial windows (shower/api.py:322-340, shower_basis.py:408-439)
         weight_ratio = float(np.sum(T.fold_scale) / np.sum(T.fold_scale[T.fold_bands]))
-        n_near, n_far, far_sum = T.radial_window(
-            [(c[0], c[1], ev.npts, ev.frame) for c, ev in zip(compiled, events)])
-        for k, ev in enumerate(events):
-            used = np.zeros(n, np.int64)
-            tail = np.zeros(n)
+        window = [(c[0], c[1], ev.npts, ev.frame) for c, ev in zip(compiled, events)]
+        owner = list(range(len(events)))
+        for k, ev in enumerate(events):  # delayed steps' points count too (api.py:327-338)
+            if ev.late is not None:
+                z = ev.late["zero"]
+                window.append((z["raw_points"], z["raw_channels"], z["npts"], z["frame"]))
+                owner.append(k)
+        n_near, n_far, far_sum = T.radial_window(window)
+        acc = [(np.zeros(n, np.int64), np.zeros(n), np.zeros(n, bool)) for _ in events]
+        for row, k in enumerate(owner):
+            used, tail, near = acc[k]
+            npts = window[row][2]
             for b, band in enumerate(T.fold_bands):
-                used = np.maximum(used, int(ev.npts[b]) - n_near[k, b] - n_far[k, b])
-                tail += weight_ratio * (10 * T.areas * T.peak_acceptance * T.efficiency[band]
-                                        * far_sum[k, b])
-            near = np.any(n_near[k] > 0, axis=0)
+                used = np.maximum(used, int(npts[b]) - n_near[row, b] - n_far[row, b])
+                tail = tail + weight_ratio * (10 * T.areas * T.peak_acceptance
+                                              * T.efficiency[band] * far_sum[row, b])
+            acc[k] = (used, tail, near | np.any(n_near[row] > 0, axis=0))
+        for k, ev in enumerate(events):
+            used, tail, near = acc[k]
             if np.any(near):
                 raise NotImplementedError("basis points inside the table's inner radius need the "
                                           "near-field clamp (near_field.py), not on the device "
@@ -610,6 +665,17 @@ class ShowerTransport:
                 ev.origins = early[k]
             if "predicted" in ev.pending:
                 ev.predicted[ev.reach] = ev.pending.pop("predicted").cpu().numpy()[:, 0].real
+        # delayed light is small and compact: its zero-frequency charge exactly on
+        # every reachable OM (shower/api.py:345-352)
+        late_req = [ev for ev in events if ev.late is not None and len(ev.reach)]
+        for ev in events:
+            ev.late_charge = np.zeros(n)
+        if late_req:
+            zs = [ev.late["zero"] for ev in late_req]
+            for ev, res in zip(late_req, self._apply_many(
+                    [(z["points"], self._zero_only(z["channels"]), z["reference"], z["frame"],
+                      ev.reach) for z in zs], zero_frequency=True)):
+                ev.late_charge[ev.reach] = res.cpu().numpy()[:, 0].real
         stage("predictor_clock")
         # ---- prompt orders 0 and 1 (transport_prompt, prompt.py:500-947)
         for k, ev in enumerate(events):
@@ -707,8 +773,8 @@ class ShowerTransport:
             ev.pending["ge2"] = {}
             prompt_charge = ev.charge.sum(axis=1)
             ev.computable = (ev.used > 0) | (prompt_charge > 0)
-            cand = (ev.used > 0) & (prompt_charge + safety * np.abs(ev.predicted) + ev.extra
-                                    >= threshold)
+            cand = (ev.used > 0) & (prompt_charge + safety * np.abs(ev.predicted)
+                                    + ev.late_charge + ev.extra >= threshold)
             if threshold == 0:
                 cand = ev.used > 0
             ev.candidate = cand
@@ -736,8 +802,8 @@ class ShowerTransport:
                                                     ev.reference, ev.frame, ids,
                                                     zero_frequency=True).cpu().numpy()[:, 0].real
             ev.fallback, ev.ratio, ev.candidate = fallback, ratio, cand
-            charge2 = ev.predicted.copy()
-            charge2[cand] = exact[cand]
+            charge2 = ev.predicted + ev.late_charge
+            charge2[cand] = exact[cand] + ev.late_charge[cand]
             ev.charge = np.column_stack((ev.charge, charge2))
             level = np.where(ev.used > 0, 1, 0).astype(np.int8)
             level[cand] = 2
@@ -771,7 +837,8 @@ class ShowerTransport:
             # relative-time spectra e^{-i w origin} N(w); the stored zero frequency is
             # the exact >=2 charge (shower/api.py:584)
             origin = np.concatenate([events[k].origins[work] for k, work in row_ev])
-            zero = np.concatenate([events[k].charge[work, 2] for k, work in row_ev])
+            zero = np.concatenate([events[k].charge[work, 2] - events[k].late_charge[work]
+                                   for k, work in row_ev])
             phase = np.exp(-1j * np.outer(origin, omega))
             phase[:, 0] = 0.0
             packed = _lib.upload(np.concatenate([phase, zero[:, None].astype(complex)], axis=1),
@@ -782,6 +849,7 @@ class ShowerTransport:
                 events[k].pending["spec"] = (work, spec)
             bins2, _ = T.readout.bins(rel.to(torch.complex64), mode=cfg.readout_mode)
             bins2 = bins2.cpu().numpy().astype(float)
+        late_bins = self._late_bins(events, row_ev, omega, cfg.readout_mode)
         responses = []
         row = 0
         row_map = {k: work for k, work in row_ev}
@@ -789,7 +857,7 @@ class ShowerTransport:
             if "spec" in ev.pending:
                 work, spec = ev.pending.pop("spec")
                 ev.spectrum[:, work] = spec.cpu().numpy().T
-            ev.spectrum[0] = ev.charge[:, 2]
+            ev.spectrum[0] = ev.charge[:, 2] - ev.late_charge  # prompt steps (api.py:450)
             components = np.zeros((n, len(edges) - 1, 3))
             ids = np.flatnonzero(ev.active)
             if len(ids):
@@ -801,6 +869,8 @@ class ShowerTransport:
                     work = row_map[k]
                     components[work, :, 2] = bins2[row:row + len(work)]
                     row += len(work)
+                    for values in late_bins.get(k, []):
+                        components[work, :, 2] += values
             metadata = {
                 "route": "lighthit_b200.shower", "ge2_charge_level": ev.level2.tolist(),
                 "ge2_predictor": {"cell_m": float(cfg.predictor_cell_m), "safety": safety,
@@ -817,12 +887,62 @@ class ShowerTransport:
                 "active_modules": int(ev.active.sum()), "threshold_pe": threshold,
                 "ge2_points": [int(v) for v in ev.npts], "source_elements": len(ev.el["beta"]),
                 "elapsed_seconds": (perf_counter() - began) / len(events),
-                "batch_size": len(events), "timings": stage.times}
+                "batch_size": len(events), "timings": stage.times,
+                "delayed_light": {
+                    "prompt_delay_ns": float(cfg.prompt_delay_ns),
+                    "delayed_cell_ns": float(cfg.delayed_cell_ns),
+                    "groups_in_window": 0 if ev.late is None else len(ev.late["groups"]),
+                    "steps_in_window_groups": 0 if ev.late is None else ev.late["steps_in_groups"],
+                    "steps_beyond_window": 0 if ev.late is None else ev.late["beyond"],
+                    "delayed_charge_pe": float(ev.late_charge.sum()),
+                    "stored_spectrum": "prompt steps only (delayed light in charge and bins)"}}
             responses.append(HybridTransportResponse(None, omega.copy(), edges.copy(),
                                                      ev.spectrum, components, ev.charge,
                                                      ev.origins, ev.active, "shower", metadata))
         stage("ge2_full_readout")
         return responses
+
+    def _part(self, compiler, part):
+        """Source compile of a delayed part with its own frame: world points per
+        band, device channels, host zero-frequency channels, sizes, frame."""
+        frame = axis_frame(part["start_m"], part["direction"], part["length_m"],
+                           part["coefficient0"])
+        pts_d, ch_d, npts_d, reference, frame = compiler.compile(part, frame)
+        npts = npts_d.cpu().numpy()
+        pts = pts_d.cpu().numpy()
+        centre, axis, e1, e2 = (np.asarray(v, float) for v in frame)
+        nb = len(npts)
+        return {"points": [centre + pts[b, :npts[b], :1] * axis + pts[b, :npts[b], 1:2] * e1
+                           + pts[b, :npts[b], 2:3] * e2 for b in range(nb)],
+                "channels": (ch_d[:, :int(npts[0])] if np.all(npts == npts[0])
+                             else [ch_d[b, :int(npts[b])] for b in range(nb)]),
+                "npts": npts, "reference": reference, "frame": frame,
+                "raw_points": pts_d, "raw_channels": ch_d}
+
+    def _late_bins(self, events, row_ev, omega, mode):
+        """Bins of the delayed groups for the readout OMs: each group's spectrum
+        demodulated by its own delay and read on the window edges seen from
+        it (shower/api.py:466-477). ``{event: [bins per group]}``."""
+        import torch
+        T = self.tables
+        req, meta = [], []
+        for k, work in row_ev:
+            ev = events[k]
+            if ev.late is None:
+                continue
+            for g, shift in ev.late["groups"]:
+                req.append((g["points"], g["channels"], g["reference"], g["frame"], work))
+                meta.append((k, work, shift))
+        out = {}
+        if not req:
+            return out
+        for (k, work, shift), spec in zip(meta, self._apply_many(req, zero_frequency=False)):
+            phase = _lib.upload(np.exp(-1j * np.outer(events[k].origins[work] + shift, omega)),
+                                torch.complex128, T.device)
+            values, _ = T.readout_shifted(shift).bins((spec * phase).to(torch.complex64),
+                                                      mode=mode)
+            out.setdefault(k, []).append(values.cpu().numpy().astype(float))
+        return out
 
     def _redo_overflow(self, events, key, tables):
         """Events whose bounded pencil table overflowed: stage A and B again at full size."""
@@ -876,7 +996,7 @@ class ShowerTransport:
         ev.charge = np.zeros((n, 2))
         ev.level1 = np.zeros(n, np.int8)
         ev.bins1 = np.zeros((n, len(T.edges) - 1))
-        ev.extra_prompt = safety * np.abs(ev.predicted) + ev.extra
+        ev.extra_prompt = safety * np.abs(ev.predicted) + np.abs(ev.late_charge) + ev.extra
         ev.pending["bins0"] = None
 
 
