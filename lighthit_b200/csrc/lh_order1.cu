@@ -879,10 +879,17 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
     }
     __syncthreads();
     // profile: _batch_add_moments (_prompt_numba.py:394-447), generic monomials
+    // With few path nodes (typically ~33) the groups are split into `parts`
+    // contiguous ranges so that every thread works: each (node, part) sum goes
+    // to the unused upper part of g0/g2 and the parts are added in order.
     const double g1 = 1.0 + g * g, gg = 2.0 * g, norm = (1.0 - g * g) / (4.0 * kPi);
-    for (int k = tid; k < n; k += blockDim.x) {
+    constexpr int kSplitNodes = kO1MaxNodes / 4;
+    const int parts = n <= kSplitNodes ? max(1, min(3, (int)blockDim.x / n)) : 1;
+    for (int it = tid; it < n * parts; it += blockDim.x) {
+      const int k = it % n, part = it / n;
+      const int q0 = part * count / parts, q1 = (part + 1) * count / parts;
       double a0s = 0.0, a2s = 0.0;
-      for (int q = 0; q < count; ++q) {
+      for (int q = q0; q < q1; ++q) {
         const double* row = S.mom + q * kO1MaxValues;
         const double omega = row[2 * nm];
         if (omega <= 0.0) continue;
@@ -920,8 +927,25 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
         a0s += a0 * value;
         a2s += a2 * value;
       }
-      S.g0[k] = a0s;
-      S.g2[k] = a2s;
+      if (parts == 1) {
+        S.g0[k] = a0s;
+        S.g2[k] = a2s;
+      } else {
+        S.g0[kSplitNodes * (part + 1) + k] = a0s;
+        S.g2[kSplitNodes * (part + 1) + k] = a2s;
+      }
+    }
+    if (parts > 1) {
+      __syncthreads();
+      for (int k = tid; k < n; k += blockDim.x) {
+        double a0s = 0.0, a2s = 0.0;
+        for (int part = 0; part < parts; ++part) {
+          a0s += S.g0[kSplitNodes * (part + 1) + k];
+          a2s += S.g2[kSplitNodes * (part + 1) + k];
+        }
+        S.g0[k] = a0s;
+        S.g2[k] = a2s;
+      }
     }
     __syncthreads();
     // _batch_deposit (_prompt_numba.py:451-551) for every band at once: the
