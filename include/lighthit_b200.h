@@ -292,7 +292,7 @@ typedef struct {
   int32_t n_gauss;             /* nodes of the Gaussian 1/theta mean (48)            */
   const double* gauss_tau;     /* [n_gauss] on [0, pi/2]                              */
   const double* gauss_w;       /* [n_gauss]                                          */
-  int32_t group_capacity;      /* group table slots per OM (power of two, <= 16384)  */
+  int32_t group_capacity;      /* group table slots per OM (power of two, <= 2^20)   */
 } lh_order1_config;
 
 typedef struct {

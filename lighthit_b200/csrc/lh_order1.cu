@@ -40,7 +40,7 @@ constexpr int kO1MaxValues = 2 * kO1MaxMono + 6;
 constexpr int kO1MaxBands = 8;
 constexpr int kO1MaxGauss = 64;
 constexpr int kO1Moments = 23;
-constexpr int kO1GroupSort = 8192;  // groups per OM sorted in one CTA
+constexpr int kO1SmemSort = 16384;  // group tables up to this size sort in shared memory
 constexpr int kO1BatchThreads = 128;
 
 LH_DEVICE uint64_t o1_mix(uint64_t v) {
@@ -536,8 +536,7 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
       if (slot < 0) {
         atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
       } else {
-        if (fresh && atomicAdd(gcount + w, 1) >= kO1GroupSort)
-          atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+        if (fresh) atomicAdd(gcount + w, 1);
         row = grows + ((int64_t)w * cap + slot) * kO1MaxValues;
       }
     }
@@ -576,12 +575,18 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
 __global__ void __launch_bounds__(1024)
 o1_batches_kernel(const lh_order1_config C, int32_t n_work, const long long* gkeys,
                   int32_t* sorted_slots, int32_t* batch_list, int32_t* batch_total,
-                  int32_t* status) {
+                  unsigned long long* sort_keys, int32_t* sort_slots, int32_t* status) {
+  // Tables up to kO1SmemSort slots sort (key << 14 | slot) in shared memory;
+  // larger ones (steps whose pencils mix times, e.g. delayed light) sort keys
+  // and slots side by side in the workspace.
   extern __shared__ __align__(16) unsigned char o1b_smem[];
-  unsigned long long* v = reinterpret_cast<unsigned long long*>(o1b_smem);
   __shared__ int n_used;
   const int w = blockIdx.x;
   const int64_t cap = C.group_capacity;
+  const bool packed = cap <= kO1SmemSort;
+  unsigned long long* v =
+      packed ? reinterpret_cast<unsigned long long*>(o1b_smem) : sort_keys + (int64_t)w * cap;
+  int32_t* vs = packed ? nullptr : sort_slots + (int64_t)w * cap;
   const long long* keys = gkeys + (int64_t)w * cap;
   if (threadIdx.x == 0) n_used = 0;
   __syncthreads();
@@ -589,17 +594,24 @@ o1_batches_kernel(const lh_order1_config C, int32_t n_work, const long long* gke
     const long long key = keys[slot];
     if (key == -1ll) continue;
     const int k = atomicAdd(&n_used, 1);
-    if (k < kO1GroupSort) v[k] = ((unsigned long long)key << 14) | (unsigned long long)slot;
+    if (packed) {
+      v[k] = ((unsigned long long)key << 14) | (unsigned long long)slot;
+    } else {
+      v[k] = (unsigned long long)key;
+      vs[k] = (int32_t)slot;
+    }
   }
   __syncthreads();
-  const int used = min(n_used, kO1GroupSort);
-  if (n_used > kO1GroupSort && threadIdx.x == 0)
-    atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+  const int used = n_used;
   int n = 1;
   while (n < used) n <<= 1;
-  for (int k = used + threadIdx.x; k < n; k += blockDim.x) v[k] = ~0ull;
+  for (int k = used + threadIdx.x; k < n; k += blockDim.x) {
+    v[k] = ~0ull;
+    if (!packed) vs[k] = -1;
+  }
   __syncthreads();
-  // bitonic sort, ascending
+  // bitonic sort, ascending (shared or, for large tables, global memory: the
+  // barrier makes the block's global writes visible to the block)
   for (int size = 2; size <= n; size <<= 1) {
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
       for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -610,26 +622,33 @@ o1_batches_kernel(const lh_order1_config C, int32_t n_work, const long long* gke
           if ((a > b) == up) {
             v[k] = b;
             v[partner] = a;
+            if (!packed) {
+              const int32_t t = vs[k];
+              vs[k] = vs[partner];
+              vs[partner] = t;
+            }
           }
         }
       }
       __syncthreads();
     }
   }
-  int32_t* out = sorted_slots + (int64_t)w * kO1GroupSort;
+  int32_t* out = sorted_slots + (int64_t)w * cap;
   const long long tb = C.theta_bins;
+  auto key_of = [&](int k) { return packed ? (long long)(v[k] >> 14) : (long long)v[k]; };
   for (int k = threadIdx.x; k < used; k += blockDim.x) {
-    out[k] = (int32_t)(v[k] & 0x3fffull);
-    const long long bk = (long long)(v[k] >> 14) / tb;
-    if (k == 0 || (long long)(v[k - 1] >> 14) / tb != bk) {
+    out[k] = packed ? (int32_t)(v[k] & 0x3fffull) : vs[k];
+    const long long bk = key_of(k) / tb;
+    if (k == 0 || key_of(k - 1) / tb != bk) {
       int stop = k + 1;
-      while (stop < used && (long long)(v[stop] >> 14) / tb == bk) ++stop;
+      while (stop < used && key_of(stop) / tb == bk) ++stop;
       const int b = atomicAdd(batch_total, 1);
       batch_list[3 * b] = w;
       batch_list[3 * b + 1] = k;
       batch_list[3 * b + 2] = stop;
     }
   }
+  (void)status;
 }
 
 // _ifuncs (_prompt_numba.py:139-154): I_k(z) = int_0^1 x^k e^{z x} dx, k = 0, 1, 2
@@ -787,7 +806,7 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
     __syncthreads();
     const int w = batch_list[3 * b], start = batch_list[3 * b + 1], stop = batch_list[3 * b + 2];
     const int count = stop - start;
-    const int32_t* slots = sorted_slots + (int64_t)w * kO1GroupSort + start;
+    const int32_t* slots = sorted_slots + (int64_t)w * cap + start;
     const double* rows = grows + (int64_t)w * cap * kO1MaxValues;
     if (count > 128) {
       if (tid == 0) atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
@@ -1130,6 +1149,8 @@ struct O1Workspace {
   int32_t* batch_list;
   int32_t* batch_total;
   double* accum;
+  unsigned long long* sort_keys;  // tables above kO1SmemSort only
+  int32_t* sort_slots;
   size_t bytes;
 };
 
@@ -1153,10 +1174,14 @@ static O1Workspace o1_layout(const lh_order1_config& C, int64_t pencil_capacity,
   W.grows = reinterpret_cast<double*>(
       take(sizeof(double) * kO1MaxValues * (size_t)n_work * C.group_capacity));
   W.gcount = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (size_t)n_work));
-  W.sorted = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (size_t)n_work * kO1GroupSort));
-  W.batch_list = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 3 * (size_t)n_work * kO1GroupSort));
+  W.sorted = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (size_t)n_work * C.group_capacity));
+  W.batch_list =
+      reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 3 * (size_t)n_work * C.group_capacity));
   W.batch_total = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 4));
   W.accum = reinterpret_cast<double*>(take(sizeof(double) * (size_t)n_work * C.n_bands * (3 + 4 * nb + 1)));
+  const size_t sort_n = C.group_capacity > kO1SmemSort ? (size_t)n_work * C.group_capacity : 0;
+  W.sort_keys = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * sort_n));
+  W.sort_slots = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * sort_n));
   (void)pencil_capacity;
   W.bytes = off;
   return W;
@@ -1194,7 +1219,7 @@ bool o1_config_valid(const lh_order1_config* C) {
   if (C->n_edges < 2 || !C->edges || !C->eedge || !C->itab) return false;
   if (C->max_path_nodes < 4 || C->max_path_nodes > lh::kO1MaxNodes) return false;
   if (C->n_gauss < 1 || C->n_gauss > lh::kO1MaxGauss || !C->gauss_tau || !C->gauss_w) return false;
-  if (C->group_capacity < 1024 || C->group_capacity > (1 << 14) ||
+  if (C->group_capacity < 1024 || C->group_capacity > (1 << 20) ||
       (C->group_capacity & (C->group_capacity - 1)))
     return false;
   if (C->theta_bins < 2 || C->theta_bins > 128 || !(C->theta_lo > 0) || !(C->theta_ratio > 0) ||
@@ -1273,12 +1298,15 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
   lh::o1_group_kernel<<<lh::grid_for((int64_t)n_work * n_pencils, 256), 256, group_smem, s>>>(
       *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows, W.gcount,
       status);
-  const size_t sort_smem = sizeof(unsigned long long) * lh::kO1GroupSort;
-  if (cudaFuncSetAttribute(lh::o1_batches_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const size_t sort_smem =
+      cap <= lh::kO1SmemSort ? sizeof(unsigned long long) * (size_t)cap : 0;
+  if (sort_smem > 48 * 1024 &&
+      cudaFuncSetAttribute(lh::o1_batches_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sort_smem) != cudaSuccess)
     return LH_ECUDA;
   lh::o1_batches_kernel<<<n_work, 1024, sort_smem, s>>>(*C, n_work, W.gkeys, W.sorted, W.batch_list,
-                                                        W.batch_total, status);
+                                                        W.batch_total, W.sort_keys, W.sort_slots,
+                                                        status);
   const size_t batch_smem = sizeof(lh::O1BatchShared);
   if (cudaFuncSetAttribute(lh::o1_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)batch_smem) != cudaSuccess)

@@ -153,6 +153,19 @@ class Order1Tables:
         self.compute_bins = bool(compute_bins)
         self._workspace = None
 
+    def widened(self, group_capacity):
+        """These tables with ``group_capacity`` group slots per OM (a power of two
+        up to 2^20) and their own workspace: for steps whose pencils mix times
+        (delayed light), which multiply the (tau, r, theta) groups per OM."""
+        import copy
+        view = copy.copy(self)
+        st = _lib.Order1Config()
+        _C.pointer(st)[0] = self.struct
+        st.group_capacity = int(group_capacity)
+        view.struct = st
+        view._workspace = None
+        return view
+
     def pencil_table(self, capacity):
         """A pencil table over this object's pooled buffer (grown when needed). Tables
         from the pool are valid until the next stage-A call on the same stream."""
@@ -337,6 +350,24 @@ def grouped(tables: Order1Tables, table: "PencilTable", work, origins, *, n_penc
     if status is None:
         _raise(int(st.item()))
     return charge, bins
+
+
+MAX_GROUP_CAPACITY = 1 << 20
+
+
+def grouped_widening(tables: Order1Tables, table, work, origins):
+    """``grouped`` that retries with 4x larger group tables while they overflow
+    (up to 2^20 slots per OM)."""
+    capacity = int(tables.struct.group_capacity)
+    current = tables
+    while True:
+        try:
+            return grouped(current, table, work, origins)
+        except MemoryError:
+            capacity *= 4
+            if capacity > MAX_GROUP_CAPACITY:
+                raise
+            current = tables.widened(capacity)
 
 
 def order1(tables: Order1Tables, elements, cone_cos, origins, work=None):

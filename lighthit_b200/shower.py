@@ -40,7 +40,7 @@ from . import _lib
 from .ge2 import AxialSources, Ge2Table
 from .order0 import ElementBatch, Order0Optics, order0, raise_status as raise_order0_status
 from .order1 import (Order1Tables, PromptSettings, acceptance_monomials, element_box, grouped,
-                     pencils)
+                     grouped_widening, pencils)
 from .readout import DeviceReadout
 from .source import ShowerBasisSettings, SourceCompiler, axis_frame
 
@@ -760,7 +760,7 @@ class ShowerTransport:
                         table = pencils(T.order1, ev.prompt_el, ev.cone_cos, status=status,
                                         device_elements=ev.device_el, capacity_full=True,
                                         box=ev.prompt_box)
-                        q1m, b1m = grouped(T.order1, table, more, ev.origins, status=status)
+                        q1m, b1m = grouped_widening(T.order1, table, more, ev.origins)
                         ev.charge[more, 1] = q1m.cpu().numpy()[more]
                         ev.bins1[more] = b1m.cpu().numpy()[more]
                         ev.level1[more] = 2
@@ -824,7 +824,7 @@ class ShowerTransport:
             if len(missing):  # the reference reruns the prompt without its screen
                 table = pencils(T.order1, ev.prompt_el, 1.0 / (ev.prompt_el["beta"] * cone),
                                 status=status, capacity_full=True, box=ev.prompt_box)
-                q1m, b1m = grouped(T.order1, table, missing, ev.origins, status=status)
+                q1m, b1m = grouped_widening(T.order1, table, missing, ev.origins)
                 ev.charge[missing, 1] = q1m.cpu().numpy()[missing]
                 ev.bins1[missing] = b1m.cpu().numpy()[missing]
             work = np.flatnonzero(ev.active & (ev.used > 0))
@@ -957,7 +957,7 @@ class ShowerTransport:
             table = pencils(tables, ev.prompt_el, ev.cone_cos, device_elements=ev.device_el,
                             capacity_full=True, box=ev.prompt_box)
             work = ev.work if key == "coarse" else ev.fine
-            res = grouped(tables, table, work, ev.origins)
+            res = grouped_widening(tables, table, work, ev.origins)
             ev.pending[key] = res[0] if key == "coarse" else res
             if key == "fine":
                 ev.table = table
