@@ -451,6 +451,68 @@ size_t lh_window_slot_bytes(int32_t n_events);
 int lh_radial_window(const lh_radial_window_problem* problem, const lh_window_event* events,
                      int32_t n_events, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------------------ near field
+ * Replaces near_field_ge2 (near_field.py:91-171) with near_portions (:39-69):
+ * the order >=2 light of every element portion closer than radius_m to an OM
+ * (points the order >=2 tables leave out), with the Green function clamped at
+ * the table's radial minimum along the same directions and the flight phase of
+ * the actual distance (_cone_many_looks with clamp_low = 0,
+ * muon/track_ge2_primitive.py:612-660), per unit-coefficient spectral cone
+ * harmonics (near_field.py:72-88), Gauss panels of panel_m along each portion.
+ * Per OM the portions are summed in element order.
+ */
+typedef struct {
+  int32_t n_lambda;            /* kernel wavelength nodes (<= 4)                      */
+  int32_t degree;              /* kernel degree L (<= 16)                             */
+  int32_t acc_degree;          /* detector degree A (<= 4)                            */
+  int32_t n_pairs;             /* detector pairs (<= 8)                               */
+  int32_t n_omega;             /* frequencies                                         */
+  const float* coef;           /* complex64 [lambda][l][pair][4][n_omega]: the first
+                                  radial interval of the per-wavelength splines        */
+  double log_r0, log_r1;       /* that interval in log m; exp(log_r0) is the clamp     */
+  double radial_high;          /* table radial maximum m                              */
+  const double* absorption;    /* [lambda] 1/m                                        */
+  const double* speed;         /* [lambda] m/ns                                       */
+  const double* omega;         /* [n_omega] rad/ns                                    */
+  const int32_t* pair_lambda;  /* [n_pairs]                                           */
+  const int32_t* pair_mu;      /* [n_pairs]                                           */
+  const double* alpha;         /* [acc_degree + 1] acceptance Legendre coefficients   */
+  const double* start_norm;    /* [(acc_degree + 1)(2 acc_degree + 1)] sqrt(binom(2j, j - nu)) */
+  int32_t flight;              /* splines hold the flight phase                       */
+  const double* wavelength_nm; /* [lambda]                                            */
+  const double* phase_index;   /* [lambda] cone phase index                           */
+  const double* spectral_weight; /* [lambda] wavelength weight nm x detector efficiency */
+  int32_t gauss_order;         /* nodes per panel (<= 16)                             */
+  const double* gauss_x;       /* [gauss_order] on (-1, 1)                            */
+  const double* gauss_w;       /* [gauss_order]                                       */
+  double panel_m;              /* panel length along a portion                        */
+} lh_near_table;
+
+typedef struct {
+  int32_t n_om;
+  const double* om_pos;        /* [n_om][3]                                           */
+  const double* om_look;       /* [n_om][3] looks = -orientations                     */
+  const double* om_area;       /* [n_om] effective area m^2                           */
+  const double* time_origin_ns; /* [n_om] clock of the response                       */
+  int32_t n_elements;
+  const double* start_m;       /* [n][3]                                              */
+  const double* direction;     /* [n][3] unit                                         */
+  const double* length_m;      /* [n] (> 0)                                           */
+  const double* coefficient0;  /* [n]                                                 */
+  const double* coefficient2;  /* [n]                                                 */
+  const double* beta;          /* [n]                                                 */
+  const double* start_ns;      /* [n]                                                 */
+  const double* end_ns;        /* [n]                                                 */
+  double radius_m;             /* portions closer than this (<= exp(log_r0))          */
+  double* spectrum;            /* complex128 [n_om][n_omega] relative to the OM clock  */
+  double* charge;              /* [n_om] zero-frequency real part                     */
+  int32_t* portions;           /* [n_om][2]: portions, portions with nonzero harmonics */
+} lh_near_problem;
+
+size_t lh_near_workspace_bytes(const lh_near_table* t, const lh_near_problem* p);
+int lh_near_field(const lh_near_table* t, const lh_near_problem* p, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

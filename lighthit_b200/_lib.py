@@ -145,6 +145,25 @@ class OmGeometry(C.Structure):
                 ("earliest_ns", P)]
 
 
+class NearTable(C.Structure):
+    _fields_ = [("n_lambda", C.c_int32), ("degree", C.c_int32), ("acc_degree", C.c_int32),
+                ("n_pairs", C.c_int32), ("n_omega", C.c_int32), ("coef", P),
+                ("log_r0", C.c_double), ("log_r1", C.c_double), ("radial_high", C.c_double),
+                ("absorption", P), ("speed", P), ("omega", P), ("pair_lambda", P),
+                ("pair_mu", P), ("alpha", P), ("start_norm", P), ("flight", C.c_int32),
+                ("wavelength_nm", P), ("phase_index", P), ("spectral_weight", P),
+                ("gauss_order", C.c_int32), ("gauss_x", P), ("gauss_w", P),
+                ("panel_m", C.c_double)]
+
+
+class NearProblem(C.Structure):
+    _fields_ = [("n_om", C.c_int32), ("om_pos", P), ("om_look", P), ("om_area", P),
+                ("time_origin_ns", P), ("n_elements", C.c_int32), ("start_m", P),
+                ("direction", P), ("length_m", P), ("coefficient0", P), ("coefficient2", P),
+                ("beta", P), ("start_ns", P), ("end_ns", P), ("radius_m", C.c_double),
+                ("spectrum", P), ("charge", P), ("portions", P)]
+
+
 # name -> (restype, argtypes); every symbol the header declares
 SIGNATURES = {
     "lh_version": (C.c_char_p, []),
@@ -180,6 +199,8 @@ SIGNATURES = {
     "lh_source_workspace_bytes": (C.c_size_t, [C.POINTER(SourceProblem)]),
     "lh_source_compile": (C.c_int, [C.POINTER(SourceProblem), C.POINTER(SourceOutput), P,
                                     C.c_size_t, P, P]),
+    "lh_near_workspace_bytes": (C.c_size_t, [C.POINTER(NearTable), C.POINTER(NearProblem)]),
+    "lh_near_field": (C.c_int, [C.POINTER(NearTable), C.POINTER(NearProblem), P, C.c_size_t, P]),
 }
 LH_ESCRATCH = 6
 

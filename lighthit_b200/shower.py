@@ -11,13 +11,16 @@ are the device kernels of this package:
   contracted by ``ge2`` (``lh_ge2_apply``) at the zero frequency (predictor,
   exact candidates) and at all frequencies (active OMs);
 * readout of the >=2 spectrum to the time bins: ``readout`` (``lh_readout_*``);
-* clocks and module selection: ``lh_om_geometry`` (float64, bit-identical).
+* clocks and module selection: ``lh_om_geometry`` (float64, bit-identical);
+* element portions closer to an OM than the tables' radial minimum: the
+  near-field clamp of ``near`` (``lh_near_field``, ``near_field.py:91-217``).
 
 Tables are built once by the reference and stored under ``tables/``
-(``build_tables.py``): the folded >=2 kernels and the route's medium and
-detector constants. What the device route does not cover raises
-``NotImplementedError`` with the reason (delayed light groups, basis points
-inside the table's inner radius, elements below threshold in a node band).
+(``build_tables.py``): the folded >=2 kernels, the first radial interval of the
+per-wavelength kernels (near field) and the route's medium and detector
+constants. What the device route does not cover raises
+``NotImplementedError`` with the reason (elements below threshold in a node
+band, receiver subsets).
 Order 1 follows the reference's global screen (``prompt.py:720-812``): a
 coarse charge pass (2 m cells, 8-pixel faces, 24 ring nodes) for every OM in
 reach, full resolution where ``q0 + extra + 3 q1_coarse`` reaches threshold,
@@ -39,6 +42,7 @@ import numpy as np
 from . import _lib
 from .ge2 import AxialSources, Ge2Table
 from .order0 import ElementBatch, Order0Optics, order0, raise_status as raise_order0_status
+from .near import NearTable, add_near_field
 from .order1 import (Order1Tables, PromptSettings, acceptance_monomials, element_box, grouped,
                      grouped_widening, pencils)
 from .readout import DeviceReadout
@@ -97,7 +101,7 @@ class HybridTransportResponse:
 class ShowerTables:
     """Everything the route reads, resident on the device (built once)."""
 
-    def __init__(self, route, folded, *, device="cuda", settings=ShowerSettings()):
+    def __init__(self, route, folded, *, near=None, device="cuda", settings=ShowerSettings()):
         import torch
         self.device = torch.device(device)
         r = dict(np.load(route)) if not isinstance(route, dict) else route
@@ -156,6 +160,17 @@ class ShowerTables:
         self.readout = DeviceReadout(self.omega, self.edges, self.readout_omega, device=device)
         self._shifted_readout = {}
         self._pos = torch.tensor(self.positions, dtype=torch.float64, device=self.device)
+        self._looks = torch.tensor(self.looks, dtype=torch.float64, device=self.device)
+        self._areas = torch.tensor(self.areas, dtype=torch.float64, device=self.device)
+        # near-field clamp (near_field.py:91-171): the first radial interval of
+        # every wavelength's order >=2 spline
+        self.near = None if near is None else NearTable(
+            near, wavelength_nm=self.wavelengths, weight_nm=self.weights,
+            efficiency=self.efficiency, phase_index=self.phase, alpha=self.alpha, device=device)
+        if self.near is not None and (
+                not np.allclose(self.near.omega, self.omega, rtol=0, atol=1e-12)
+                or abs(self.near.radial_minimum - self.radial[0]) > 1e-9 * self.radial[0]):
+            raise ValueError("near-field table and route frequencies or radial minimum differ")
         # spectral_attenuation (shower_basis.py:388-405) for the far-tail screen
         w = self.weights * self.efficiency / self.wavelengths ** 2
         lowest = float(self.absorption.min())
@@ -174,6 +189,8 @@ class ShowerTables:
         folded = {"c0": "ge2_fold_48om_2-150m.npz", "c2": "ge2_fold_384om_2-450m.npz"}
         if name not in folded:
             raise ValueError("known synthetic tables: c0, c2")
+        near = TABLES / f"near_{name}.npz"
+        kw.setdefault("near", near if near.exists() else None)
         return cls(TABLES / f"route_{name}.npz", TABLES / folded[name], **kw)
 
     def om_geometry_batch(self, prompt_store, store, group_index):
@@ -583,10 +600,10 @@ class ShowerTransport:
             acc[k] = (used, tail, near | np.any(n_near[row] > 0, axis=0))
         for k, ev in enumerate(events):
             used, tail, near = acc[k]
-            if np.any(near):
+            ev.near = bool(np.any(near))
+            if ev.near and T.near is None:
                 raise NotImplementedError("basis points inside the table's inner radius need the "
-                                          "near-field clamp (near_field.py), not on the device "
-                                          "route")
+                                          "near-field table (tables/near_<config>.npz)")
             ev.used, ev.tail, ev.reach = used, tail, np.flatnonzero(used > 0)
         stage("radial_window")
         # ---- predictor (shower/ge2.py:70-96) and its zero-frequency charge (device)
@@ -896,9 +913,15 @@ class ShowerTransport:
                     "steps_beyond_window": 0 if ev.late is None else ev.late["beyond"],
                     "delayed_charge_pe": float(ev.late_charge.sum()),
                     "stored_spectrum": "prompt steps only (delayed light in charge and bins)"}}
-            responses.append(HybridTransportResponse(None, omega.copy(), edges.copy(),
-                                                     ev.spectrum, components, ev.charge,
-                                                     ev.origins, ev.active, "shower", metadata))
+            response = HybridTransportResponse(None, omega.copy(), edges.copy(), ev.spectrum,
+                                               components, ev.charge, ev.origins, ev.active,
+                                               "shower", metadata)
+            if ev.near:  # shower/api.py:536-538
+                origins = _lib.upload(ev.origins, torch.float64, dev)
+                near = T.near.field(store.event(k), len(ev.el["beta"]), T._pos, T._looks,
+                                    T._areas, origins)
+                add_near_field(response, near, T.readout, mode=cfg.readout_mode, label="shower")
+            responses.append(response)
         stage("ge2_full_readout")
         return responses
 

@@ -2,6 +2,7 @@
 
     python lighthit_b200/tables/build_tables.py c0     # 48 OMs, 2-150 m, 48 radial nodes
     python lighthit_b200/tables/build_tables.py c2     # 384 OMs, 2-450 m, 60 radial nodes
+    python lighthit_b200/tables/build_tables.py c2 near   # only near_c2.npz
 
 The reference (LightHit, pure Python + Numba) builds its RTE caches
 (``TransportKernel.build``) and the order >=2 kernel pack
@@ -9,6 +10,10 @@ The reference (LightHit, pure Python + Numba) builds its RTE caches
 rank-3 node bands (``band_fold.py:155-208``). This script stores, for the
 device route:
 * ``ge2_fold_<n>om_<lo>-<hi>m.npz``: the folded order >=2 kernels;
+* ``near_<config>.npz``: the first radial interval of the per-wavelength order
+  >=2 kernels (``Ge2KernelStore.bundle``, not folded), the only part the
+  near-field clamp reads (``near_field.py:91-171``: every point closer than the
+  radial minimum takes the amplitude at that minimum);
 * ``route_<config>.npz``: the kernel's medium and detector constants the route
   reads (wavelength nodes and weights, phase/group indices, absorption and
   scattering, detector spectral weights, the spectral-cut phase index of
@@ -39,7 +44,30 @@ CONFIGS = {
 }
 
 
-def main(name):
+def write_near(name, route, tables):
+    """The near-field table: interval 0 of every wavelength's order >=2 spline."""
+    from lighthit.shower_basis import _frequency_indices
+    indices = _frequency_indices(route.kernel, route.config.frequency_nodes)
+    bundle = tables["store"].bundle(route.kernel, indices)
+    if bundle.get("phase") != "flight":
+        raise SystemExit("near-field table needs flight-phase splines")
+    np.savez_compressed(
+        HERE / f"near_{name}.npz",
+        coefficients=np.ascontiguousarray(np.asarray(bundle["coefficients"])[:, 0], np.complex64),
+        log_r=np.asarray(bundle["log_r"], float)[:2],
+        radial_high_m=float(np.exp(np.asarray(bundle["log_r"], float)[-1])),
+        omega=np.asarray(bundle["omega"], float),
+        absorption=np.asarray(bundle["absorption"], float),
+        speed=np.asarray(bundle["speed"], float), degree=int(bundle["degree"]),
+        acceptance_degree=int(bundle["acceptance_degree"]),
+        pair_lambda=np.asarray(bundle["pair_lambda"], np.int64),
+        pair_mu=np.asarray(bundle["pair_mu"], np.int64),
+        provenance=json.dumps({"built_by": "lighthit Ge2KernelStore.bundle (interval 0)",
+                               "frequency_indices": np.asarray(indices).tolist()}))
+    print("wrote", f"near_{name}.npz", np.asarray(bundle["coefficients"]).shape)
+
+
+def main(name, near_only=False):
     os.environ.setdefault("NUMBA_CACHE_DIR", str(REPO / "_work" / "numba-cache"))
     sys.path.insert(0, str(SRC))
     import lighthit as lh
@@ -71,6 +99,9 @@ def main(name):
         kernel.ge2_kernel_store().save(str(cache / "ge2-pack"))
     route = ShowerTransport(kernel, ShowerData.of(str(cache), str(cache / "ge2-pack")))
     tables = route.tables()
+    write_near(name, route, tables)
+    if near_only:
+        return
     folded, fold = tables["folded"], tables["fold"]
     k = route.kernel
     lo, hi = c["radial_range_m"]
@@ -127,4 +158,5 @@ def main(name):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "c0")
+    main(sys.argv[1] if len(sys.argv) > 1 else "c0",
+         near_only=len(sys.argv) > 2 and sys.argv[2] == "near")
