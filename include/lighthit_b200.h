@@ -462,7 +462,7 @@ int lh_radial_window(const lh_radial_window_problem* problem, const lh_window_ev
  * Per OM the portions are summed in element order.
  */
 typedef struct {
-  int32_t n_lambda;            /* kernel wavelength nodes (<= 4)                      */
+  int32_t n_lambda;            /* kernel wavelength nodes (<= 8)                      */
   int32_t degree;              /* kernel degree L (<= 16)                             */
   int32_t acc_degree;          /* detector degree A (<= 4)                            */
   int32_t n_pairs;             /* detector pairs (<= 8)                               */

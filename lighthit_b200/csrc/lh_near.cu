@@ -30,7 +30,7 @@
 
 namespace lh {
 
-constexpr int kNearLam = 4;        // wavelength nodes bound
+constexpr int kNearLam = 8;        // wavelength nodes bound
 constexpr int kNearDeg = 16;       // kernel degree bound
 constexpr int kNearOut = 4;        // detector degree bound
 constexpr int kNearPairs = 8;      // detector pairs bound

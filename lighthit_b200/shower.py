@@ -145,7 +145,7 @@ class ShowerTables:
                                           settings=PromptSettings().screen(), compute_bins=False,
                                           device=device)
         bands = self.fold_bands
-        self.source = SourceCompiler(self.wavelengths[bands], self.fold_phase,
+        self.source = SourceCompiler(self.wavelengths[bands], self.fold_phase[bands],
                                      self.fold_scale[bands], self.source_degree,
                                      self.azimuthal_degree, self.omega,
                                      settings=ShowerBasisSettings(), device=device)
@@ -185,10 +185,13 @@ class ShowerTables:
 
     @classmethod
     def synthetic(cls, name="c0", **kw):
-        """Synthetic Baikal-like workloads: ``c0`` (48 OMs, 2-150 m), ``c2`` (384 OMs, 2-450 m)."""
-        folded = {"c0": "ge2_fold_48om_2-150m.npz", "c2": "ge2_fold_384om_2-450m.npz"}
+        """Synthetic Baikal-like workloads: ``c0`` (48 OMs, 2-150 m), ``c2`` (384 OMs,
+        2-450 m), ``c3`` (384 OMs, 1-300 m, 8 wavelength nodes, degree 16, azimuthal
+        degree 4, 1025 readout nodes, 1 ns bins to 2000 ns)."""
+        folded = {"c0": "ge2_fold_48om_2-150m.npz", "c2": "ge2_fold_384om_2-450m.npz",
+                  "c3": "ge2_fold_384om_1-300m.npz"}
         if name not in folded:
-            raise ValueError("known synthetic tables: c0, c2")
+            raise ValueError("known synthetic tables: c0, c2, c3")
         near = TABLES / f"near_{name}.npz"
         kw.setdefault("near", near if near.exists() else None)
         return cls(TABLES / f"route_{name}.npz", TABLES / folded[name], **kw)

@@ -3,6 +3,7 @@
     python lighthit_b200/tables/build_tables.py c0     # 48 OMs, 2-150 m, 48 radial nodes
     python lighthit_b200/tables/build_tables.py c2     # 384 OMs, 2-450 m, 60 radial nodes
     python lighthit_b200/tables/build_tables.py c2 near   # only near_c2.npz
+    python lighthit_b200/tables/build_tables.py c3     # 384 OMs, 1-300 m, 8 wavelengths, L=16
 
 The reference (LightHit, pure Python + Numba) builds its RTE caches
 (``TransportKernel.build``) and the order >=2 kernel pack
@@ -37,10 +38,18 @@ REPO = HERE.parents[1]
 SRC = Path(os.environ.get("LIGHTHIT_REFERENCE_SRC", "/root/reference/src"))
 WORK = Path(os.environ.get("LIGHTHIT_TABLE_WORK", REPO / "_work" / "tables"))
 
+BASE = dict(wavelength_nodes=3, degree=8, azimuthal_degree=2, readout_nodes=321,
+            bin_ns=5.0, window_end_ns=740.0)
 CONFIGS = {
-    "c0": dict(clusters=1, radial_range_m=(2.0, 150.0), radial_nodes=48, k_panel_per_m=0.1),
-    "c2": dict(clusters=8, radial_range_m=(2.0, 450.0), radial_nodes=60,
+    "c0": dict(BASE, clusters=1, radial_range_m=(2.0, 150.0), radial_nodes=48,
+               k_panel_per_m=0.1),
+    "c2": dict(BASE, clusters=8, radial_range_m=(2.0, 450.0), radial_nodes=60,
                k_panel_per_m=2 * np.pi / 450.0),
+    # high-resolution precision study: 8 wavelength nodes, degree 16, azimuthal
+    # degree 4, 96 radial nodes over 1-300 m, 1025 readout nodes, 1 ns bins to 2000 ns
+    "c3": dict(clusters=8, radial_range_m=(1.0, 300.0), radial_nodes=96,
+               k_panel_per_m=2 * np.pi / 300.0, wavelength_nodes=8, degree=16,
+               azimuthal_degree=4, readout_nodes=1025, bin_ns=1.0, window_end_ns=2000.0),
 }
 
 
@@ -82,9 +91,11 @@ def main(name, near_only=False):
     detector = baikal_like_detector(clusters=c["clusters"])
     omega = np.linspace(0.0, 1.2, 65)
     config = lh.KernelConfig(
-        omega_per_ns=omega, readout_omega_per_ns=np.linspace(0.0, 1.2, 321),
-        relative_time_edges_ns=np.arange(-60.0, 745.0, 5.0), wavelength_nodes=3,
-        scattering_degree=8, source_degree=8, azimuthal_degree=2,
+        omega_per_ns=omega, readout_omega_per_ns=np.linspace(0.0, 1.2, c["readout_nodes"]),
+        relative_time_edges_ns=np.arange(-60.0, c["window_end_ns"] + 0.5 * c["bin_ns"],
+                                         c["bin_ns"]),
+        wavelength_nodes=c["wavelength_nodes"], scattering_degree=c["degree"],
+        source_degree=c["degree"], azimuthal_degree=c["azimuthal_degree"],
         radial_range_m=c["radial_range_m"], radial_nodes=c["radial_nodes"], k_max_per_m=4.0,
         k_panel_per_m=float(c["k_panel_per_m"]), k_order=6, threshold_pe=0.01,
         cache_directory=str(cache), cache_policy="build")
