@@ -51,6 +51,7 @@ from .source import ShowerBasisSettings, SourceCompiler, axis_frame
 __all__ = ["ShowerSettings", "ShowerTables", "ShowerTransport", "HybridTransportResponse"]
 
 C_M_PER_NS = 0.299792458
+UNFUSED_PIXEL_FACE, UNFUSED_RING_NODES = 32, 96  # PromptConfig defaults (prompt.py:172-173)
 TABLES = Path(__file__).resolve().parent / "tables"
 ELEMENT_FIELDS = ("start_m", "direction", "length_m", "coefficient0", "coefficient2", "beta",
                   "start_ns", "end_ns")
@@ -144,6 +145,7 @@ class ShowerTables:
                                           self.positions, self.looks, self.areas, self.edges,
                                           settings=PromptSettings().screen(), compute_bins=False,
                                           device=device)
+        self._order1_bands = {}
         bands = self.fold_bands
         self.source = SourceCompiler(self.wavelengths[bands], self.fold_phase[bands],
                                      self.fold_scale[bands], self.source_degree,
@@ -214,6 +216,23 @@ class ShowerTables:
             _lib.check(_lib.load().lh_om_geometry(C.byref(g), sp), "lh_om_geometry")
             out.append(res)
         return out[0].cpu().numpy(), out[1].cpu().numpy()
+
+    def order1_band(self, band, *, coarse=False):
+        """Order-1 tables of one wavelength band for the per-band units (elements
+        above threshold in only some bands): that band's constants and the
+        unfused pencil resolution ``PromptConfig.pixel_face`` / ``ring_nodes``
+        (``prompt.py:172-173``), or the coarse screen's (built once)."""
+        key = (int(band), bool(coarse))
+        if key not in self._order1_bands:
+            from dataclasses import replace
+            settings = replace(PromptSettings(), pixel_face=UNFUSED_PIXEL_FACE,
+                               ring_nodes=UNFUSED_RING_NODES)
+            self._order1_bands[key] = Order1Tables(
+                {k: v[band:band + 1] for k, v in self.prompt.items()}, self.g,
+                acceptance_monomials(self.alpha), self.positions, self.looks, self.areas,
+                self.edges, settings=settings.screen() if coarse else settings,
+                compute_bins=not coarse, device=self.device)
+        return self._order1_bands[key]
 
     def readout_shifted(self, shift_ns):
         """The readout operator on the window edges seen from a delay ``shift_ns``
@@ -376,6 +395,7 @@ class _Event:
     frame: tuple = None
     reference: float = 0.0
     points: list = None
+    coords: list = None
     channels: object = None
     zero_ch: list = None
     npts: np.ndarray = None
@@ -392,6 +412,10 @@ class _Event:
     bins1: np.ndarray = None
     fine: np.ndarray = None
     cone_cos: np.ndarray = None
+    fused_el: dict = None       # elements of the fused order-1 unit (every band)
+    fused_dev: dict = None      # their device arrays when they are all prompt elements
+    fused_box: tuple = None
+    units: list = field(default_factory=list)  # (band, elements) of the per-band units
     table: object = None
     pending: dict = field(default_factory=dict)
 
@@ -430,6 +454,7 @@ class ShowerTransport:
                     view = copy.copy(getattr(T, name))
                     view._workspace = None
                     view._pencil_pool = None
+                    view.__dict__.pop("_bands", None)  # per-band views own workspaces too
                     views[name] = view
                 lanes.append(_Lane(torch.cuda.Stream(T.device), **views))
             self._lane_list = lanes
@@ -467,12 +492,14 @@ class ShowerTransport:
             basis = (centre, first, second, axis)
             args = (T.positions[oms], T.looks[oms], T.areas[oms], T.radial)
             if all(len(p) == len(points[0]) and np.array_equal(p, points[0]) for p in points[1:]):
-                src = AxialSources(points[0], channels, np.full(len(points), reference), basis,
-                                   T.source_degree, T.azimuthal_degree)
+                refs = np.broadcast_to(np.asarray(reference, float), (len(points),)).copy()
+                src = AxialSources(points[0], channels, refs, basis, T.source_degree,
+                                   T.azimuthal_degree)
                 joint.append((i, (src,) + args))
             else:  # node bands with their own points: one band-view problem per band
+                refs = np.broadcast_to(np.asarray(reference, float), (len(points),))
                 for b in range(len(points)):
-                    src = AxialSources(points[b], channels[b][None], np.array([reference]), basis,
+                    src = AxialSources(points[b], channels[b][None], refs[b:b + 1].copy(), basis,
                                        T.source_degree, T.azimuthal_degree)
                     split.append((i, b, (src,) + args))
         if joint:
@@ -562,6 +589,7 @@ class ShowerTransport:
             _, ch_d, _, ev.reference, ev.frame = c
             ev.npts = npts
             centre, axis, e1, e2 = (np.asarray(v, float) for v in ev.frame)
+            ev.coords = [p[:npts[b]] for b, p in enumerate(pts)]  # (z, x, y) in the frame
             ev.points = [centre + p[:npts[b], :1] * axis + p[:npts[b], 1:2] * e1
                          + p[:npts[b], 2:3] * e2 for b, p in enumerate(pts)]
             ev.channels = (ch_d[:, :int(npts[0])] if np.all(npts == npts[0])
@@ -618,8 +646,9 @@ class ShowerTransport:
             centre, axis, e1, e2 = (np.asarray(v, float) for v in ev.frame)
             c_points, c_channels = [], []
             for b in range(nb_bands):
-                rel = ev.points[b] - centre
-                coords = np.column_stack((rel @ axis, rel @ e1, rel @ e2))
+                # frame coordinates as compiled (a world round trip would move points
+                # on the axis off 0 and across a predictor cell edge)
+                coords = ev.coords[b]
                 keys = np.floor(coords / float(cfg.predictor_cell_m)).astype(np.int64)
                 keys -= keys.min(axis=0)
                 span = keys.max(axis=0) + 1
@@ -642,6 +671,7 @@ class ShowerTransport:
                 c_channels.append(summed[:, :, None])
             c_ch = (np.stack(c_channels) if all(len(p) == len(c_points[0]) for p in c_points[1:])
                     else c_channels)
+            ev.predictor_points = len(c_points[0])
             predict.append((ev, (c_points, c_ch, ev.reference, ev.frame, ev.reach)))
         for (ev, _), res in zip(predict, self._apply_many([r for _, r in predict],
                                                           zero_frequency=True)):
@@ -706,10 +736,7 @@ class ShowerTransport:
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         cone = float(np.sum(T.prompt["s0w"] * T.phase) / np.sum(T.prompt["s0w"]))
         for ev in prompt_events:
-            if not np.all(ev.prompt_el["beta"] * float(np.min(T.phase)) > 1):
-                raise NotImplementedError("elements above threshold in only some bands need the "
-                                          "per-band order-1 units")
-            ev.cone_cos = 1.0 / (ev.device_el["beta"] * cone)
+            self._order1_units(ev, cone)
             ev.status = torch.zeros(1, dtype=torch.int32, device=dev)
         # the coarse order-1 screens run on the lanes while order 0 (one launch for
         # every shower) runs on this stream
@@ -718,9 +745,13 @@ class ShowerTransport:
                 for k, ev in enumerate(prompt_events):
                     lane = lanes[k % len(lanes)]
                     with torch.cuda.stream(lane.stream):
-                        coarse = pencils(lane.order1_screen, ev.prompt_el, ev.cone_cos,
-                                         status=ev.status, device_elements=ev.device_el,
-                                         box=ev.prompt_box)
+                        if ev.fused_el is None:
+                            ev.pending["coarse"] = torch.zeros(n, dtype=torch.float64,
+                                                               device=dev)
+                            continue
+                        coarse = pencils(lane.order1_screen, ev.fused_el, ev.cone_cos,
+                                         status=ev.status, device_elements=ev.fused_dev,
+                                         box=ev.fused_box)
                         ev.pending["coarse"] = grouped(lane.order1_screen, coarse, ev.work,
                                                        ev.origins, status=ev.status)[0]
             if prompt_events:
@@ -742,6 +773,8 @@ class ShowerTransport:
             ev.fine = ev.work
             if "coarse" in ev.pending:
                 coarse = ev.pending.pop("coarse").cpu().numpy()
+                if ev.units:
+                    coarse = coarse + self._units_charge(ev, ev.work, coarse=True)[0]
                 ev.charge[ev.work, 1] = coarse[ev.work]
                 ev.level1[ev.work] = 1
                 ev.pending["coarse_host"] = coarse
@@ -755,8 +788,13 @@ class ShowerTransport:
             for k, ev in enumerate(fine_events):
                 lane = lanes[k % len(lanes)]
                 with torch.cuda.stream(lane.stream):
-                    ev.table = pencils(lane.order1, ev.prompt_el, ev.cone_cos, status=ev.status,
-                                       device_elements=ev.device_el, box=ev.prompt_box)
+                    if ev.fused_el is None:
+                        ev.pending["fine"] = (
+                            torch.zeros(n, dtype=torch.float64, device=dev),
+                            torch.zeros((n, len(edges) - 1), dtype=torch.float64, device=dev))
+                        continue
+                    ev.table = pencils(lane.order1, ev.fused_el, ev.cone_cos, status=ev.status,
+                                       device_elements=ev.fused_dev, box=ev.fused_box)
                     ev.pending["fine"] = grouped(lane.order1, ev.table, ev.fine, ev.origins,
                                                  status=ev.status)
         self._redo_overflow(prompt_events, "fine", T.order1)
@@ -765,6 +803,9 @@ class ShowerTransport:
                 continue
             q1, b1 = ev.pending.pop("fine")
             q1, b1 = q1.cpu().numpy(), b1.cpu().numpy()
+            if ev.units:
+                qu, bu = self._units_charge(ev, ev.fine)
+                q1, b1 = q1 + qu, b1 + bu
             ev.charge[ev.fine, 1] = q1[ev.fine]
             ev.bins1[ev.fine] = b1[ev.fine]
             ev.level1[ev.fine] = 2
@@ -777,12 +818,9 @@ class ShowerTransport:
                                    & (ev.charge[ev.work, 0] + ev.extra_prompt[ev.work] + wider
                                       * np.maximum(coarse[ev.work], 0.0) >= threshold)]
                     if len(more):
-                        table = pencils(T.order1, ev.prompt_el, ev.cone_cos, status=status,
-                                        device_elements=ev.device_el, capacity_full=True,
-                                        box=ev.prompt_box)
-                        q1m, b1m = grouped_widening(T.order1, table, more, ev.origins)
-                        ev.charge[more, 1] = q1m.cpu().numpy()[more]
-                        ev.bins1[more] = b1m.cpu().numpy()[more]
+                        q1m, b1m = self._fine_order1(ev, more, status)
+                        ev.charge[more, 1] = q1m[more]
+                        ev.bins1[more] = b1m[more]
                         ev.level1[more] = 2
         if int(status.item()) & _lib.LH_STATUS_OVERFLOW:
             raise MemoryError("order-1 tables overflowed their device capacity")
@@ -842,11 +880,9 @@ class ShowerTransport:
             ids = np.flatnonzero(ev.active)
             missing = np.flatnonzero(ev.active & (ev.level1 < 2))
             if len(missing):  # the reference reruns the prompt without its screen
-                table = pencils(T.order1, ev.prompt_el, 1.0 / (ev.prompt_el["beta"] * cone),
-                                status=status, capacity_full=True, box=ev.prompt_box)
-                q1m, b1m = grouped_widening(T.order1, table, missing, ev.origins)
-                ev.charge[missing, 1] = q1m.cpu().numpy()[missing]
-                ev.bins1[missing] = b1m.cpu().numpy()[missing]
+                q1m, b1m = self._fine_order1(ev, missing, status)
+                ev.charge[missing, 1] = q1m[missing]
+                ev.bins1[missing] = b1m[missing]
             work = np.flatnonzero(ev.active & (ev.used > 0))
             if len(work):
                 row_ev.append((k, work))
@@ -893,11 +929,14 @@ class ShowerTransport:
                         components[work, :, 2] += values
             metadata = {
                 "route": "lighthit_b200.shower", "ge2_charge_level": ev.level2.tolist(),
-                "ge2_predictor": {"cell_m": float(cfg.predictor_cell_m), "safety": safety,
+                "ge2_predictor": {"points": int(getattr(ev, "predictor_points", 0)),
+                                  "cell_m": float(cfg.predictor_cell_m), "safety": safety,
                                   "candidates": int(ev.candidate.sum()),
                                   "reachable": int(len(ev.reach)),
                                   "fallback_to_exact": ev.fallback,
-                                  "exact_over_prediction_max": float(ev.ratio.max(initial=0.0))},
+                                  "exact_over_prediction_max": float(ev.ratio.max(initial=0.0)),
+                                  "exact_over_prediction_min": (float(ev.ratio.min())
+                                                                if len(ev.ratio) else None)},
                 "prompt_order1_level": ev.level1.tolist(), "radial_window_m": [low, high],
                 "radial_tail_estimate_max_pe": float(ev.tail.max(initial=0.0)),
                 "time_origin": ("supplied event clock" if time_origin_ns is not None else
@@ -980,13 +1019,68 @@ class ShowerTransport:
         for ev, f in zip(pend, flags):
             if not f & _lib.LH_STATUS_OVERFLOW:
                 continue
-            table = pencils(tables, ev.prompt_el, ev.cone_cos, device_elements=ev.device_el,
-                            capacity_full=True, box=ev.prompt_box)
+            table = pencils(tables, ev.fused_el, ev.cone_cos, device_elements=ev.fused_dev,
+                            capacity_full=True, box=ev.fused_box)
             work = ev.work if key == "coarse" else ev.fine
             res = grouped_widening(tables, table, work, ev.origins)
             ev.pending[key] = res[0] if key == "coarse" else res
             if key == "fine":
                 ev.table = table
+
+    def _order1_units(self, ev, cone):
+        """Order-1 evaluation units (``prompt.py:683-719`` with
+        ``muon/secondary_first.py:184-204``): one fused unit of the elements
+        above the Cherenkov threshold in every band (shared pencils, one cone at
+        the s0w-weighted mean phase index) and, per band, a unit of the elements
+        emitting in that band but not in all of them (that band's tables and
+        cone, the unfused pencil resolution)."""
+        T = self.tables
+        el = ev.prompt_el
+        beta = el["beta"]
+        everywhere = beta * float(np.min(T.phase)) > 1  # rounding is monotone in n
+        ev.units = []
+        if np.all(everywhere):
+            ev.fused_el, ev.fused_dev, ev.fused_box = el, ev.device_el, ev.prompt_box
+            ev.cone_cos = 1.0 / (ev.device_el["beta"] * cone)
+            return
+        for band, phase in enumerate(T.phase):
+            mask = (beta * float(phase) > 1) & ~everywhere
+            if np.any(mask):
+                ev.units.append((band, _subset(el, mask)))
+        ev.fused_el = _subset(el, everywhere) if np.any(everywhere) else None
+        ev.fused_dev = None
+        ev.fused_box = None if ev.fused_el is None else element_box(ev.fused_el)
+        ev.cone_cos = None if ev.fused_el is None else 1.0 / (ev.fused_el["beta"] * cone)
+
+    def _units_charge(self, ev, oms, *, coarse=False):
+        """Order-1 charge (and bins) at ``oms`` of an event's per-band units, summed."""
+        T = self.tables
+        charge = np.zeros(T.n_om)
+        bins = None if coarse else np.zeros((T.n_om, len(T.edges) - 1))
+        for band, sub in ev.units:
+            tables = T.order1_band(band, coarse=coarse)
+            table = pencils(tables, sub, 1.0 / (sub["beta"] * float(T.phase[band])),
+                            capacity_full=True)
+            q, b = grouped_widening(tables, table, oms, ev.origins)
+            charge[oms] += q.cpu().numpy()[oms]
+            if bins is not None:
+                bins[oms] += b.cpu().numpy()[oms]
+        return charge, bins
+
+    def _fine_order1(self, ev, oms, status):
+        """Full-resolution order 1 at ``oms`` over every unit (host arrays)."""
+        T = self.tables
+        q = np.zeros(T.n_om)
+        b = np.zeros((T.n_om, len(T.edges) - 1))
+        if ev.fused_el is not None:
+            table = pencils(T.order1, ev.fused_el, ev.cone_cos, status=status,
+                            device_elements=ev.fused_dev, capacity_full=True, box=ev.fused_box)
+            q1, b1 = grouped_widening(T.order1, table, oms, ev.origins)
+            q, b = q1.cpu().numpy(), b1.cpu().numpy()
+        if ev.units:
+            qu, bu = self._units_charge(ev, oms)
+            q, b = q + qu, b + bu
+        return q, b
 
     @staticmethod
     def _zero_only(channels):

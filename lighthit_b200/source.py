@@ -52,10 +52,18 @@ def axis_frame(start, direction, length, weights):
     start, direction = np.asarray(start, float), np.asarray(direction, float)
     points = start + 0.5 * np.asarray(length, float)[:, None] * direction
     share = np.asarray(weights, float) / np.sum(weights)
+    # The reference's (share[:, None] * points).sum(axis=0) and
+    # einsum("i,ij,ik->jk", share, offset, offset) add the elements in order;
+    # running sums reproduce them bit for bit (a frame one rounding apart can
+    # move a node across a slice edge or a slice across the stencil threshold).
     weighted = share[:, None] * points
-    centre = np.array([weighted[:, k].sum() for k in range(3)])  # column sums (fast)
+    centre = np.array([np.cumsum(weighted[:, k])[-1] for k in range(3)])
     offset = points - centre
-    covariance = (share[:, None] * offset).T @ offset
+    lead = share[:, None] * offset
+    covariance = np.empty((3, 3))
+    for j in range(3):
+        for k in range(3):
+            covariance[j, k] = np.cumsum(lead[:, j] * offset[:, k])[-1]
     values, vectors = np.linalg.eigh(covariance)
     if np.max(np.abs(values)) <= 1e-24:
         axis = np.sum(share[:, None] * direction, axis=0)
@@ -140,14 +148,28 @@ class SourceCompiler:
         p.n_slices, p.kmax = n_slices, kmax
         return p
 
+    def band(self, b):
+        """This compiler restricted to node band ``b`` (its own workspace)."""
+        view = SourceCompiler.__new__(SourceCompiler)
+        view.__dict__.update(self.__dict__)
+        view.wavelengths, view.phase = self.wavelengths[b:b + 1], self.phase[b:b + 1]
+        view.scale = self.scale[b:b + 1]
+        view._workspace, view._fixed = None, None
+        return view
+
     def compile(self, elements, frame=None, *, stream=None, check=True, status=None,
                 device_elements=None):
         """Points and channels of every node band (device), the emission reference.
 
         ``elements``: reference ``SpectralLightElements`` or a dict with its
-        field names, every element above threshold in every node band.
-        Returns ``(points (band, P, 3) [z, x, y], channels (band, P, nch, W)
-        complex64, n_points (band,), reference_ns, frame)``.
+        field names. Returns ``(points (band, P, 3) [z, x, y], channels (band, P,
+        nch, W) complex64, n_points (band,), reference_ns, frame)``. When every
+        element is above the Cherenkov threshold in every node band, all bands
+        share one lattice and ``reference_ns`` is a float; otherwise each band
+        compiles its own emitting elements (``_band_field``, ``shower/ge2.py:21-32``)
+        on its own lattice, a band without them takes another band's points with
+        zero channels (``node_sources``, ``:35-67``), and ``reference_ns`` is an
+        array of one emission reference per band.
         """
         import torch
 
@@ -160,8 +182,8 @@ class SourceCompiler:
         t0, t1 = field("start_ns"), field("end_ns")
         # rounding is monotone: beta n <= 1 for some band iff it holds at the smallest n
         if np.any(beta * float(np.min(self.phase)) <= 1):
-            raise NotImplementedError("device source compile needs every element above the "
-                                      "Cherenkov threshold in every node band")
+            return self._compile_per_band(elements, beta, frame, stream=stream, check=check,
+                                          status=status)
         if frame is None:
             frame = axis_frame(start, direction, length, c0)
         centre, axis = np.asarray(frame[0], float), np.asarray(frame[1], float)
@@ -219,4 +241,45 @@ class SourceCompiler:
         self._keep = arrays
         if own_status and check and int(status.item()) & _lib.LH_STATUS_OVERFLOW:
             raise ValueError("element nodes fall outside the source lattice")
+        return points, channels, n_points, reference, frame
+
+    def _compile_per_band(self, elements, beta, frame, *, stream, check, status):
+        """``node_sources`` for elements above threshold in only some node bands:
+        one compile per band on its emitting elements, padded to one layout."""
+        import torch
+        names = ("start_m", "direction", "length_m", "coefficient0", "coefficient2", "beta",
+                 "start_ns", "end_ns")
+        el = {k: np.asarray(elements[k] if isinstance(elements, dict) else getattr(elements, k),
+                            float) for k in names}
+        if frame is None:
+            frame = axis_frame(el["start_m"], el["direction"], el["length_m"],
+                               el["coefficient0"])
+        if not hasattr(self, "_bands"):
+            self._bands = [self.band(b) for b in range(len(self.phase))]
+        parts = {}
+        for b, phase in enumerate(self.phase):
+            mask = beta * float(phase) > 1
+            if np.any(mask):
+                sub = {k: v[mask] for k, v in el.items()}
+                parts[b] = self._bands[b].compile(sub, frame, stream=stream, check=check,
+                                                  status=status)
+        if not parts:
+            raise ValueError("no element emits in any node band")
+        nb = len(self.phase)
+        template = parts[min(parts)]
+        capacity = max(int(p[0].shape[1]) for p in parts.values())
+        dev = self.device
+        points = torch.zeros((nb, capacity, 3), dtype=torch.float64, device=dev)
+        channels = torch.zeros((nb, capacity, self.nch, len(self.omega)), dtype=torch.complex64,
+                               device=dev)
+        n_points = torch.zeros(nb, dtype=torch.int32, device=dev)
+        reference = np.zeros(nb)
+        for b in range(nb):
+            pts, ch, npts, ref, _ = parts.get(b, template)
+            cap = int(pts.shape[1])
+            points[b, :cap] = pts[0]
+            if b in parts:
+                channels[b, :cap] = ch[0]
+            n_points[b] = npts[0]
+            reference[b] = ref
         return points, channels, n_points, reference, frame

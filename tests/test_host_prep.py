@@ -58,3 +58,30 @@ def test_acceptance_coefficients_match_fixture(flash_golden):
     alpha = acceptance_coefficients(det.angular_acceptance, 8)
     assert np.max(np.abs(alpha - flash_golden["alpha"])) < 1e-11
     np.testing.assert_array_equal(det.positions_m, flash_golden["om_positions_m"])
+
+
+def test_axis_frame_is_bit_identical_to_the_reference_expressions():
+    """``axis_frame`` reproduces ``AxisFrame.of`` (``axial_source.py:88-118``) bit for
+    bit: its running sums equal NumPy's ``sum(axis=0)`` and three-operand ``einsum``."""
+    from lighthit_b200.source import axis_frame
+    rng = np.random.default_rng(5)
+    for n in (1, 7, 2000, 50000):
+        start = rng.normal(size=(n, 3)) * 30
+        direction = rng.normal(size=(n, 3))
+        direction /= np.linalg.norm(direction, axis=1)[:, None]
+        length = rng.uniform(0.01, 2.0, n)
+        weights = rng.uniform(0.1, 3.0, n)
+        points = start + 0.5 * length[:, None] * direction
+        share = weights / weights.sum()
+        centre = (share[:, None] * points).sum(axis=0)
+        offset = points - centre
+        covariance = np.einsum("i,ij,ik->jk", share, offset, offset)
+        values, vectors = np.linalg.eigh(covariance)
+        got = axis_frame(start, direction, length, weights)
+        assert np.array_equal(got[0], centre)
+        if n > 1:
+            axis = vectors[:, int(np.argmax(values))]
+            axis = axis / np.linalg.norm(axis)
+            if float((share * (direction @ axis)).sum()) < 0:
+                axis = -axis
+            assert np.array_equal(got[1], axis)
