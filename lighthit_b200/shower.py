@@ -133,19 +133,10 @@ class ShowerTables:
         self.source_degree = int(r["source_degree"])
         self.azimuthal_degree = int(r["azimuthal_degree"])
         self.settings = settings
-        optics = {k: np.asarray(r[f"optics_{k}"], float) for k in (
+        self._optics = {k: np.asarray(r[f"optics_{k}"], float) for k in (
             "panel_edges", "phase_nodes", "group_nodes", "extinction_nodes",
             "efficiency_coefficients")}
-        self.order0 = Order0Optics(optics, self.positions, self.looks, self.areas, self.radii,
-                                   self.alpha, order=settings.order0_gauss, device=device)
-        self.order1 = Order1Tables(self.prompt, self.g, acceptance_monomials(self.alpha),
-                                   self.positions, self.looks, self.areas, self.edges,
-                                   settings=PromptSettings(), device=device)
-        self.order1_screen = Order1Tables(self.prompt, self.g, acceptance_monomials(self.alpha),
-                                          self.positions, self.looks, self.areas, self.edges,
-                                          settings=PromptSettings().screen(), compute_bins=False,
-                                          device=device)
-        self._order1_bands = {}
+        self._om_tables()
         bands = self.fold_bands
         self.source = SourceCompiler(self.wavelengths[bands], self.fold_phase[bands],
                                      self.fold_scale[bands], self.source_degree,
@@ -161,9 +152,6 @@ class ShowerTables:
             raise ValueError("radial window must lie inside the kernel cache")
         self.readout = DeviceReadout(self.omega, self.edges, self.readout_omega, device=device)
         self._shifted_readout = {}
-        self._pos = torch.tensor(self.positions, dtype=torch.float64, device=self.device)
-        self._looks = torch.tensor(self.looks, dtype=torch.float64, device=self.device)
-        self._areas = torch.tensor(self.areas, dtype=torch.float64, device=self.device)
         # near-field clamp (near_field.py:91-171): the first radial interval of
         # every wavelength's order >=2 spline
         self.near = None if near is None else NearTable(
@@ -184,6 +172,45 @@ class ShowerTables:
                      torch.tensor(log_factor, dtype=torch.float64, device=self.device))
         self._window_ws = None
         self.n_om = n
+
+    def _om_tables(self):
+        """The OM-dependent device tables (orders 0 and 1, OM arrays)."""
+        import torch
+        dev, settings = self.device, self.settings
+        self.order0 = Order0Optics(self._optics, self.positions, self.looks, self.areas,
+                                   self.radii, self.alpha, order=settings.order0_gauss, device=dev)
+        self.order1 = Order1Tables(self.prompt, self.g, acceptance_monomials(self.alpha),
+                                   self.positions, self.looks, self.areas, self.edges,
+                                   settings=PromptSettings(), device=dev)
+        self.order1_screen = Order1Tables(self.prompt, self.g, acceptance_monomials(self.alpha),
+                                          self.positions, self.looks, self.areas, self.edges,
+                                          settings=PromptSettings().screen(), compute_bins=False,
+                                          device=dev)
+        self._order1_bands = {}
+        self._pos = torch.tensor(self.positions, dtype=torch.float64, device=dev)
+        self._looks = torch.tensor(self.looks, dtype=torch.float64, device=dev)
+        self._areas = torch.tensor(self.areas, dtype=torch.float64, device=dev)
+        self._window_ws = None
+        self.n_om = len(self.positions)
+
+    def subset(self, receivers):
+        """These tables for the OMs ``receivers`` only, with threshold zero
+        (``subset_kernel`` in ``ShowerTransport._event``, ``shower/api.py:205-212``):
+        the OM-independent device tables (>=2 kernels, source compiler, readout,
+        near field) are shared, the OM tables rebuilt for the subset."""
+        import copy
+        ids = np.asarray(receivers, np.int64).ravel()
+        if not len(ids) or ids.min() < 0 or ids.max() >= self.n_om or len(np.unique(ids)) != len(ids):
+            raise ValueError("receivers must be distinct OM indices of the detector")
+        view = copy.copy(self)
+        view.positions = np.ascontiguousarray(self.positions[ids])
+        view.looks = np.ascontiguousarray(self.looks[ids])
+        view.areas = np.ascontiguousarray(self.areas[ids])
+        view.radii = np.ascontiguousarray(self.radii[ids])
+        view.threshold = 0.0
+        view.receivers = ids
+        view._om_tables()
+        return view
 
     @classmethod
     def synthetic(cls, name="c0", **kw):
@@ -515,12 +542,25 @@ class ShowerTransport:
 
     def __call__(self, source, *, time_origin_ns=None, selection_extra_charge=None,
                  receivers=None):
-        if receivers is not None:
-            raise NotImplementedError("receiver subsets: build ShowerTables for those OMs")
+        if receivers is not None:  # shower/api.py:205-212: those OMs, threshold zero
+            return self._subset_route(receivers)(source, time_origin_ns=time_origin_ns,
+                                                 selection_extra_charge=selection_extra_charge)
         return self.batch([source], time_origin_ns=None if time_origin_ns is None
                           else [time_origin_ns],
                           selection_extra_charge=None if selection_extra_charge is None
                           else [selection_extra_charge])[0]
+
+    def _subset_route(self, receivers):
+        """A route on ``tables.subset(receivers)`` (the last few kept: an event
+        refines the same OM sets across its sources)."""
+        key = tuple(int(v) for v in np.asarray(receivers, np.int64).ravel())
+        cache = self.__dict__.setdefault("_subsets", {})
+        if key not in cache:
+            if len(cache) >= 8:
+                cache.pop(next(iter(cache)))
+            cache[key] = ShowerTransport(self.tables.subset(key), self.config,
+                                         profile=self.profile, lanes=self.n_lanes)
+        return cache[key]
 
     def batch(self, sources, *, time_origin_ns=None, selection_extra_charge=None):
         """Responses of several showers (``transport_shower`` per source)."""
