@@ -193,7 +193,7 @@ def reference_arm(args, rank):
 N_SHOWER = 96
 
 
-def shower_stream_section(dev, steps, workers=2, max_batch=8):
+def shower_stream_section(dev, steps, workers=3, max_batch=8):
     """Config 2: the served shower stream at 384 OMs through the device route.
 
     ``plain_fp32``: one shower after another on one stream, fp32 readout (the
