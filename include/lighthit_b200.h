@@ -529,6 +529,16 @@ int lh_near_field(const lh_near_table* t, const lh_near_problem* p, void* worksp
 int lh_flash_transport_noalloc(const lh_flash_problem* p, const lh_readout_operator* op,
                                const lh_flash_batch* b, void* stream);
 
+/* Failure detection without a fault (no counterpart in the reference). Every
+ * wait of the tensor-core kernels on an mbarrier gives up after 1 s of global
+ * time; the kernel then sets LH_STATUS_TIMEOUT in its status word, finishes
+ * its own copies, frees its tensor memory and returns, and the host raises.
+ * This entry point runs one such wait, limited to `limit_ns` (0 < limit_ns
+ * <= 1e9), on an mbarrier that nothing completes: `status` (device, 8-byte
+ * aligned, int32[4]) gets LH_STATUS_TIMEOUT in status[0] and the nanoseconds
+ * waited in status[2..3] (uint64). */
+int lh_wait_selftest(int32_t* status, int64_t limit_ns, void* stream);
+
 /* Library version string (host). */
 const char* lh_version(void);
 

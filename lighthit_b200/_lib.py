@@ -201,6 +201,7 @@ SIGNATURES = {
                                     C.c_size_t, P, P]),
     "lh_near_workspace_bytes": (C.c_size_t, [C.POINTER(NearTable), C.POINTER(NearProblem)]),
     "lh_near_field": (C.c_int, [C.POINTER(NearTable), C.POINTER(NearProblem), P, C.c_size_t, P]),
+    "lh_wait_selftest": (C.c_int, [P, C.c_int64, P]),
 }
 LH_ESCRATCH = 6
 

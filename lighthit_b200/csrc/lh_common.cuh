@@ -20,7 +20,7 @@ namespace lh {
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kCVacuumMPerNs = 0.299792458;
-constexpr long long kSpinLimit = 1ll << 26;  // ~ 1 s of polling at worst
+constexpr long long kWaitLimitNs = 1000000000ll;  // a bounded device wait gives up after 1 s
 
 // ---------------------------------------------------------------- float64 geometry
 // The reference computes its geometry in NumPy float64 without fused
@@ -67,11 +67,19 @@ LH_DEVICE void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-// Returns true when the phase with the given parity completed, false after
-// the spin limit.
-LH_DEVICE bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t addr = smem_addr(bar);
-  for (long long spin = 0; spin < kSpinLimit; ++spin) {
+// Nanoseconds of the GPU's global timer.
+LH_DEVICE unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Returns true when the phase with the given parity completed, false once
+// `limit_ns` of global time have passed (checked every 256 polls).
+LH_DEVICE bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit_ns = kWaitLimitNs) {
+  const uint32_t addr = smem_addr(bar);
+  const unsigned long long start = global_ns();
+  for (unsigned spin = 0; spin < 0x7fffffffu; ++spin) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -81,6 +89,7 @@ LH_DEVICE bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((spin & 255u) == 255u && global_ns() - start > (unsigned long long)limit_ns) return false;
   }
   return false;
 }
