@@ -27,6 +27,13 @@ constexpr int kFlashPairs = 64;  // pairs per tile -> 128 readout rows
 constexpr int kMaxAcc = 8;       // highest acceptance degree handled
 constexpr int kFlashThreads = 256;    // plain path
 constexpr int kFlashTcThreads = 512;  // fused path: 16 warps hide the table-load latency
+// A tile of the fused path: K-major, no swizzle, [k/8][row][k%8] with each
+// 8-column chunk of the 128 rows padded by 16 bytes (2064 B apart, the MMA's
+// leading byte offset). A warp stores 32 consecutive columns of one row: the
+// padding puts their four chunks in different banks (2048 B apart they shared
+// four banks: 4-way conflicts on every A-tile store).
+constexpr int kAChunk = 128 * 8 + 8;   // elements per 8-column chunk
+LH_DEVICE int a_offset(int row, int k) { return (k >> 3) * kAChunk + row * 8 + (k & 7); }
 
 struct FlashPair {
   double origin;  // time_origin_ns of the OM for this flash
@@ -295,7 +302,7 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
                 const __nv_bfloat16* __restrict__ g_blo, int kpad, int n_bins, int n_tile,
                 int passes) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  const uint32_t a_bytes = 128u * kpad * 2u;
+  const uint32_t a_bytes = (uint32_t)(kpad / 8) * kAChunk * 2u;
   const uint32_t b_bytes = (uint32_t)n_tile * kpad * 2u;
   __nv_bfloat16* s_ahi = reinterpret_cast<__nv_bfloat16*>(smem);
   __nv_bfloat16* s_alo = reinterpret_cast<__nv_bfloat16*>(smem + a_bytes);
@@ -343,7 +350,7 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
     const int64_t base = tile * kFlashPairs;
     FlashPair* sp = sp_buf + cur * kFlashPairs;  // set up before the barrier closing the last tile
     for (int i = tid; i < 128 * padw; i += blockDim.x) {
-      const int off = tile_offset(i / padw, 2 * nw + i % padw);
+      const int off = a_offset(i / padw, 2 * nw + i % padw);
       s_ahi[off] = __float2bfloat16_rn(0.f);
       s_alo[off] = __float2bfloat16_rn(0.f);
     }
@@ -364,13 +371,13 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
         flash_item(p, b, base + lp, w, sp[lp], r1, r2);
         __nv_bfloat16 hi, lo;
         split_bf16(r1.x, hi, lo);
-        s_ahi[tile_offset(2 * lp, w)] = hi;       s_alo[tile_offset(2 * lp, w)] = lo;
+        s_ahi[a_offset(2 * lp, w)] = hi;       s_alo[a_offset(2 * lp, w)] = lo;
         split_bf16(r1.y, hi, lo);
-        s_ahi[tile_offset(2 * lp, nw + w)] = hi;  s_alo[tile_offset(2 * lp, nw + w)] = lo;
+        s_ahi[a_offset(2 * lp, nw + w)] = hi;  s_alo[a_offset(2 * lp, nw + w)] = lo;
         split_bf16(r2.x, hi, lo);
-        s_ahi[tile_offset(2 * lp + 1, w)] = hi;   s_alo[tile_offset(2 * lp + 1, w)] = lo;
+        s_ahi[a_offset(2 * lp + 1, w)] = hi;   s_alo[a_offset(2 * lp + 1, w)] = lo;
         split_bf16(r2.y, hi, lo);
-        s_ahi[tile_offset(2 * lp + 1, nw + w)] = hi; s_alo[tile_offset(2 * lp + 1, nw + w)] = lo;
+        s_ahi[a_offset(2 * lp + 1, nw + w)] = hi; s_alo[a_offset(2 * lp + 1, nw + w)] = lo;
       }
     }
     fence_proxy_async();  // generic-proxy smem writes -> visible to the tensor core
@@ -384,7 +391,7 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
       if (ok) {
         tc_fence_after();
         const int ksteps = kpad / 16;
-        const uint32_t lbo_a = 128u * 16u, lbo_b = (uint32_t)n_tile * 16u;
+        const uint32_t lbo_a = kAChunk * 2u, lbo_b = (uint32_t)n_tile * 16u;
         int first = 1;
         for (int pass = 0; pass < passes; ++pass) {
           const __nv_bfloat16* pa = (pass == 2) ? s_alo : s_ahi;
@@ -467,7 +474,8 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
 }
 
 size_t flash_tc_smem_bytes(int kpad, int n_tile) {
-  return 2ull * 128 * kpad * 2 + 2ull * n_tile * kpad * 2 + 2 * sizeof(FlashPair) * kFlashPairs + 64;
+  return 2ull * (kpad / 8) * kAChunk * 2 + 2ull * n_tile * kpad * 2 +
+         2 * sizeof(FlashPair) * kFlashPairs + 64;
 }
 
 }  // namespace lh
