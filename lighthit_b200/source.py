@@ -52,17 +52,17 @@ def axis_frame(start, direction, length, weights):
     start, direction = np.asarray(start, float), np.asarray(direction, float)
     points = start + 0.5 * np.asarray(length, float)[:, None] * direction
     share = np.asarray(weights, float) / np.sum(weights)
-    # The reference's (share[:, None] * points).sum(axis=0) and
-    # einsum("i,ij,ik->jk", share, offset, offset) add the elements in order;
-    # running sums reproduce them bit for bit (a frame one rounding apart can
-    # move a node across a slice edge or a slice across the stencil threshold).
-    weighted = share[:, None] * points
-    centre = np.array([np.cumsum(weighted[:, k])[-1] for k in range(3)])
+    # Bit for bit the reference's frame (one rounding apart can move a node
+    # across a slice edge or a slice across the stencil threshold): its centre
+    # expression, and its einsum("i,ij,ik->jk") covariance, which adds the
+    # elements in order, as running sums of the lower triangle (eigh reads
+    # only that).
+    centre = (share[:, None] * points).sum(axis=0)
     offset = points - centre
     lead = share[:, None] * offset
-    covariance = np.empty((3, 3))
+    covariance = np.zeros((3, 3))
     for j in range(3):
-        for k in range(3):
+        for k in range(j + 1):
             covariance[j, k] = np.cumsum(lead[:, j] * offset[:, k])[-1]
     values, vectors = np.linalg.eigh(covariance)
     if np.max(np.abs(values)) <= 1e-24:
