@@ -39,7 +39,7 @@ TABLE = ROOT / "lighthit_b200" / "tables" / "flash_450nm_2-250m.npz"
 N_FLASH = 4096
 # DRAM bytes (read + write) of one 4096-flash flash_tc_kernel launch, measured with
 # ncu on a B200 (profiles/flash_tc_kernel_4096flashes.txt).
-FLASH_TC_TRAFFIC = 637_070_336
+FLASH_TC_TRAFFIC = 636_147_456
 
 
 def workload():
