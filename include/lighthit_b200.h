@@ -124,6 +124,30 @@ int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op,
                        const lh_flash_batch* b, void* workspace, size_t workspace_bytes,
                        void* stream);
 
+/* Broadband flashes (transport.py:1049-1164): the flash is transported at the
+ * kernel's wavelength nodes, one lh_flash_transport per node with that node's
+ * table and photons (_flash_nodes), the common clock of the fastest node
+ * (origin_speed) and threshold +infinity (no mask, no range check); this call
+ * sums the node outputs into `b` (spectrum, components, charge) and sets the
+ * mask and the range check of the sum: active = inside and total charge >=
+ * threshold, unsafe = outside and 10 x sum of the nodes' absorption-only
+ * estimates >= threshold (status as lh_flash_transport). `p` is the problem of
+ * any node with the real threshold; b->origin is not written (every node run
+ * wrote the same clock). */
+#define LH_FLASH_MAX_NODES 8
+typedef struct {
+  int32_t n_nodes;                                /* <= LH_FLASH_MAX_NODES              */
+  const float* spectrum[LH_FLASH_MAX_NODES];      /* node runs, layouts of lh_flash_batch */
+  const float* components[LH_FLASH_MAX_NODES];
+  const double* charge[LH_FLASH_MAX_NODES];
+  const double* photons[LH_FLASH_MAX_NODES];      /* [n_flash] photons at each node       */
+  double efficiency[LH_FLASH_MAX_NODES];          /* detector spectral weight at the node */
+  double absorption[LH_FLASH_MAX_NODES];          /* 1/m at the node                      */
+} lh_flash_nodes;
+
+int lh_flash_combine(const lh_flash_problem* p, const lh_flash_nodes* nodes,
+                     const lh_flash_batch* b, void* stream);
+
 /* ------------------------------------------------------------------ order >= 2
  * Replaces apply_folded -> apply_multi_spectral -> _apply_multi_spectral
  * (shower/ge2.py:99-119, _shower_basis.py:894-1198): node-band axial sources

@@ -46,6 +46,12 @@ class FlashBatch(C.Structure):
                 ("block_threads", C.c_int32)]
 
 
+class FlashNodes(C.Structure):
+    _fields_ = [("n_nodes", C.c_int32), ("spectrum", P * 8), ("components", P * 8),
+                ("charge", P * 8), ("photons", P * 8), ("efficiency", C.c_double * 8),
+                ("absorption", C.c_double * 8)]
+
+
 class Ge2Table(C.Structure):
     _fields_ = [("n_bands", C.c_int32), ("n_intervals", C.c_int32), ("degree", C.c_int32),
                 ("acc_degree", C.c_int32), ("max_m", C.c_int32), ("n_pairs", C.c_int32),
@@ -178,6 +184,8 @@ SIGNATURES = {
                                      C.POINTER(FlashBatch), P, C.c_size_t, P]),
     "lh_flash_transport_noalloc": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(ReadoutOperator),
                                              C.POINTER(FlashBatch), P]),
+    "lh_flash_combine": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(FlashNodes),
+                                   C.POINTER(FlashBatch), P]),
     "lh_ge2_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem)]),
     "lh_ge2_apply": (C.c_int, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem), P, C.c_size_t, P]),
     "lh_window_slot_bytes": (C.c_size_t, [C.c_int32]),

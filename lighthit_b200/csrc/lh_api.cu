@@ -13,6 +13,7 @@ __global__ void flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv
                                 const __nv_bfloat16* g_blo, int kpad, int n_bins, int n_tile,
                                 int passes);
 size_t flash_tc_smem_bytes(int kpad, int n_tile);
+__global__ void flash_combine_kernel(lh_flash_problem p, lh_flash_nodes nd, lh_flash_batch b);
 }  // namespace lh
 
 using namespace lh;
@@ -154,6 +155,24 @@ int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op,
   flash_tc_kernel<<<grid, threads, smem, s>>>(*p, *b, reinterpret_cast<const __nv_bfloat16*>(op->b_hi),
                                           reinterpret_cast<const __nv_bfloat16*>(op->b_lo),
                                           op->k_pad, op->n_bins, op->n_tile, passes_of(mode));
+  return check_launch();
+}
+
+int lh_flash_combine(const lh_flash_problem* p, const lh_flash_nodes* nodes,
+                     const lh_flash_batch* b, void* stream) {
+  if (!p || !nodes || !b || p->n_om <= 0 || b->n_flash < 0 || p->acc_top < 0 || p->acc_top > 8 ||
+      p->n_omega < 1 || p->n_edges < 2 || nodes->n_nodes < 1 ||
+      nodes->n_nodes > LH_FLASH_MAX_NODES || !b->status || !b->spectrum || !b->components ||
+      !b->charge || !b->active || !b->pos)
+    return LH_EINVAL;
+  for (int n = 0; n < nodes->n_nodes; ++n)
+    if (!nodes->spectrum[n] || !nodes->components[n] || !nodes->charge[n] || !nodes->photons[n])
+      return LH_EINVAL;
+  if (b->n_flash == 0) return LH_OK;
+  const int64_t work = (int64_t)b->n_flash * p->n_om * p->n_omega * 6;
+  const int64_t want = (work + 255) / 256;
+  const int grid = (int)(want < 16 * sm_count() ? want : 16 * sm_count());
+  flash_combine_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(*p, *nodes, *b);
   return check_launch();
 }
 

@@ -480,6 +480,80 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
   if (warp == 0) tmem_dealloc(tmem, 256);
 }
 
+// ---------------------------------------------------------------- broadband
+// Sum of the node runs of a broadband flash and the mask and range check of
+// the sum (transport.py:1088-1164). Grid-stride over the spectrum and bins
+// (node order fixed: identical results alone or in a batch), then one thread
+// per pair: charge, the absorption-only estimate over the nodes, flags.
+__global__ void flash_combine_kernel(lh_flash_problem p, lh_flash_nodes nd, lh_flash_batch b) {
+  const int64_t n_pairs = (int64_t)flash_count(b) * p.n_om;
+  const int nb = p.n_edges - 1;
+  const int64_t first = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t n_spec = n_pairs * p.n_omega * 6;  // floats
+  for (int64_t i = first; i < n_spec; i += stride) {
+    float v = 0.f;
+    for (int n = 0; n < nd.n_nodes; ++n) v += nd.spectrum[n][i];
+    b.spectrum[i] = v;
+  }
+  const int64_t n_comp = n_pairs * 3 * nb;
+  for (int64_t i = first; i < n_comp; i += stride) {
+    float v = 0.f;
+    for (int n = 0; n < nd.n_nodes; ++n) v += nd.components[n][i];
+    b.components[i] = v;
+  }
+  for (int64_t pair = first; pair < n_pairs; pair += stride) {
+    double q[3] = {0.0, 0.0, 0.0};
+    for (int n = 0; n < nd.n_nodes; ++n)
+      for (int o = 0; o < 3; ++o) q[o] += nd.charge[n][pair * 3 + o];
+    for (int o = 0; o < 3; ++o) b.charge[pair * 3 + o] = q[o];
+    // geometry and acceptance as flash_pair_setup
+    const int64_t f = pair / p.n_om;
+    const int d = (int)(pair % p.n_om);
+    const double sx = b.pos[3 * f], sy = b.pos[3 * f + 1], sz = b.pos[3 * f + 2];
+    const double px = p.om_pos[3 * d], py = p.om_pos[3 * d + 1], pz = p.om_pos[3 * d + 2];
+    const double dx = __dsub_rn(px, sx), dy = __dsub_rn(py, sy), dz = __dsub_rn(pz, sz);
+    const double r = sqrt(dot3_rn(dx, dy, dz, dx, dy, dz));
+    int flags = 0;
+    if (r == 0.0) {
+      atomicOr(reinterpret_cast<unsigned*>(b.status), LH_STATUS_COINCIDENT);
+      flags |= 4;
+    }
+    const double tx = __dsub_rn(sx, px), ty = __dsub_rn(sy, py), tz = __dsub_rn(sz, pz);
+    const double tn = sqrt(dot3_rn(tx, ty, tz, tx, ty, tz));
+    const double cosine = dot3_rn(p.om_look[3 * d], p.om_look[3 * d + 1], p.om_look[3 * d + 2],
+                                  tx / tn, ty / tn, tz / tn);
+    double pl_prev = 1.0, pl = cosine, acc = 0.0;
+    for (int l = 0; l <= p.acc_top; ++l) {
+      double P;
+      if (l == 0) P = 1.0;
+      else if (l == 1) P = cosine;
+      else {
+        P = ((2 * l - 1) * cosine * pl - (l - 1) * pl_prev) / l;
+        pl_prev = pl;
+        pl = P;
+      }
+      acc += p.alpha[l] * (2 * l + 1) * P / (4 * kPi);
+    }
+    const double four_pi_r2 = 4 * kPi * r * r;
+    double upper = 0.0;
+    for (int n = 0; n < nd.n_nodes; ++n)
+      upper += nd.photons[n][f] * p.om_area[d] * nd.efficiency[n] * acc *
+               exp(-nd.absorption[n] * r) / four_pi_r2;
+    const bool inside = (r >= p.r_low) && (r <= p.r_high);
+    if (!inside && 10 * upper >= p.threshold) {
+      flags |= 2;
+      atomicOr(reinterpret_cast<unsigned*>(b.status), LH_STATUS_UNSAFE);
+      atomicAdd(b.status + 1, 1);
+      atomicMax(reinterpret_cast<unsigned long long*>(b.status + 2),
+                (unsigned long long)__double_as_longlong(r));
+    }
+    const double total = (q[0] + q[1]) + q[2];
+    const bool active = p.threshold == 0.0 ? inside : (inside && total >= p.threshold);
+    b.active[pair] = (uint8_t)((active ? 1 : 0) | flags);
+  }
+}
+
 size_t flash_tc_smem_bytes(int kpad, int n_tile) {
   return 2ull * (kpad / 8) * kAChunk * 2 + 2ull * n_tile * kpad * 2 +
          2 * sizeof(FlashPair) * kFlashPairs + 64;

@@ -24,7 +24,7 @@ from .model import C_VACUUM_M_PER_NS, Medium, TransportResponse, acceptance_coef
 from .readout import DeviceReadout
 from .spline import spline_coefficients
 
-__all__ = ["FlashTable", "FlashTransport"]
+__all__ = ["FlashTable", "FlashTransport", "BroadbandFlashTransport"]
 
 
 @dataclass
@@ -224,7 +224,8 @@ class FlashTransport:
     def transport(self, source, *, method="isotropic"):
         """``TransportKernel.transport(IsotropicFlash)``: one flash -> ``TransportResponse``."""
         if getattr(source, "wavelength_nm", None) is None:
-            raise NotImplementedError("broadband flashes need one table per wavelength node")
+            raise ValueError("a broadband flash needs one table per wavelength node: "
+                             "BroadbandFlashTransport")
         if not np.isclose(float(source.wavelength_nm), self.wavelength_nm, rtol=0, atol=1e-9):
             raise ValueError("flash wavelength differs from the table's wavelength")
         out = self.run(np.asarray(source.position_m, float)[None, :], [float(source.photons)],
@@ -248,6 +249,104 @@ class FlashTransport:
              "fourier_inverted_orders": [1, 2],
              "radial_range_m": list(map(float, self.config.radial_range_m)),
              "readout_precision": self.mode, "route": "lighthit_b200.flash"})
+
+
+class BroadbandFlashTransport:
+    """Isotropic flashes with a spectral shape (``IsotropicFlash.broadband``).
+
+    The reference transports them at the kernel's wavelength nodes
+    (``transport.py:1049-1164``): node photons ``photons * weight * shape /
+    (weight . shape)`` (``_flash_nodes``), every node with its own multipole
+    table, attenuation, flight time and order-0 arrival, one OM clock for the
+    fastest node, the mask and range check on the sum. Here each node is one
+    fused device launch (:class:`FlashTransport` on that node's table, with the
+    common clock and no mask of its own) and ``lh_flash_combine`` sums the node
+    outputs and sets the mask and range check. ``tables``: one
+    :class:`FlashTable` per node, in the order of ``node_wavelengths_nm``.
+    """
+
+    def __init__(self, detector, config, tables, node_wavelengths_nm, node_weights_nm, *,
+                 device="cuda", mode="split-bf16"):
+        import torch
+        nodes = np.asarray(node_wavelengths_nm, float)
+        if len(tables) != len(nodes) or not 1 <= len(nodes) <= 8:
+            raise ValueError("one flash table per wavelength node (at most 8)")
+        for t, w in zip(tables, nodes):
+            if not np.isclose(float(t.medium.wavelength_nm), w, rtol=0, atol=1e-6):
+                raise ValueError("flash tables must follow the node wavelengths")
+        self.detector, self.config, self.mode = detector, config, mode
+        self.device = torch.device(device)
+        self.nodes, self.weights = nodes, np.asarray(node_weights_nm, float)
+        self.threshold = float(config.threshold_pe)
+        fastest = min(float(t.medium.group_index) for t in tables)
+        self.node = []
+        for t in tables:
+            ft = FlashTransport(detector, config, t, device=device, mode=mode)
+            ft.problem.origin_speed = C_VACUUM_M_PER_NS / fastest  # transport.py:1124-1125
+            ft.problem.threshold = float("inf")                     # the mask is the sum's
+            self.node.append(ft)
+        self.problem = _lib.FlashProblem.from_buffer_copy(self.node[0].problem)
+        self.problem.threshold = self.threshold
+        self.n_om, self.n_omega, self.n_bins = (self.node[0].n_om, self.node[0].n_omega,
+                                                self.node[0].n_bins)
+
+    def node_photons(self, photons, spectral_shape):
+        """``_flash_nodes`` (``transport.py:1049-1059``): (node, flash) photons."""
+        shape = np.asarray(spectral_shape(self.nodes), float)
+        if shape.shape != self.nodes.shape or not np.isfinite(shape).all() or np.any(shape < 0):
+            raise ValueError("flash spectral_shape must return finite nonnegative values")
+        norm = float(self.weights @ shape)
+        if norm <= 0:
+            raise ValueError("flash spectral_shape has zero integral")
+        return np.outer(self.weights * shape / norm, np.asarray(photons, float))
+
+    def run(self, positions, photons, time_ns, spectral_shape, *, stream=None):
+        """A batch of flashes sharing one spectral shape: device outputs (checked)."""
+        import torch
+        F = len(positions)
+        dev = self.device
+        pos = torch.tensor(np.asarray(positions, float).reshape(F, 3), dtype=torch.float64,
+                           device=dev)
+        t = torch.tensor(np.broadcast_to(np.asarray(time_ns, float), (F,)).copy(),
+                         dtype=torch.float64, device=dev)
+        per_node = self.node_photons(np.broadcast_to(np.asarray(photons, float), (F,)),
+                                     spectral_shape)
+        ph = [torch.tensor(per_node[n], dtype=torch.float64, device=dev)
+              for n in range(len(self.node))]
+        outs = [ft.launch(pos, ph[n], t, ft.allocate(F), stream=stream)
+                for n, ft in enumerate(self.node)]
+        out = self.node[0].allocate(F)
+        out["origin"] = outs[0]["origin"]  # every node run wrote the common clock
+        nd = _lib.FlashNodes()
+        nd.n_nodes = len(self.node)
+        for n, (ft, o) in enumerate(zip(self.node, outs)):
+            nd.spectrum[n] = o["spectrum"].data_ptr()
+            nd.components[n] = o["components"].data_ptr()
+            nd.charge[n] = o["charge"].data_ptr()
+            nd.photons[n] = ph[n].data_ptr()
+            nd.efficiency[n] = ft.efficiency
+            nd.absorption[n] = float(ft.table.medium.absorption_per_m)
+        batch = _lib.FlashBatch(
+            F, pos.data_ptr(), 0, t.data_ptr(), out["spectrum"].data_ptr(),
+            out["components"].data_ptr(), out["charge"].data_ptr(), out["origin"].data_ptr(),
+            out["active"].data_ptr(), out["status"].data_ptr(), None, 0)
+        s = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
+        _lib.check(_lib.load().lh_flash_combine(self.problem, nd, batch, s), "lh_flash_combine")
+        torch.cuda.synchronize(dev)
+        for o in outs:  # coincident sources and wait timeouts of the node runs
+            self.node[0].raise_for_status(o)
+        self.node[0].raise_for_status(out)
+        return out
+
+    def transport(self, source, *, method="isotropic"):
+        """``TransportKernel.transport(IsotropicFlash)`` for a broadband flash."""
+        if getattr(source, "spectral_shape", None) is None:
+            raise ValueError("BroadbandFlashTransport takes flashes with a spectral_shape")
+        out = self.run(np.asarray(source.position_m, float)[None, :], [float(source.photons)],
+                       [float(source.time_ns)], source.spectral_shape)
+        r = self.node[0].response(out, 0, method=method)
+        r.metadata["wavelength_nm"] = self.nodes.tolist()
+        return r
 
 
 def _main(argv=None):

@@ -45,6 +45,10 @@ class IsotropicFlash:
     def monochromatic(cls, position_m, photons, wavelength_nm, *, time_ns=0.0):
         return cls(position_m, photons, wavelength_nm=float(wavelength_nm), time_ns=time_ns)
 
+    @classmethod
+    def broadband(cls, position_m, photons, spectral_shape, *, time_ns=0.0):
+        return cls(position_m, photons, spectral_shape=spectral_shape, time_ns=time_ns)
+
 
 @dataclass(frozen=True)
 class Medium:

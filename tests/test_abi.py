@@ -42,7 +42,8 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
              "lh_source_problem": _lib.SourceProblem, "lh_source_output": _lib.SourceOutput,
              "lh_om_geometry_problem": _lib.OmGeometry, "lh_window_event": _lib.WindowEvent,
              "lh_radial_window_problem": _lib.RadialWindowProblem,
-             "lh_near_table": _lib.NearTable, "lh_near_problem": _lib.NearProblem}
+             "lh_near_table": _lib.NearTable, "lh_near_problem": _lib.NearProblem,
+             "lh_flash_nodes": _lib.FlashNodes}
     cc = shutil.which("gcc") or shutil.which("cc")
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lighthit_b200.h"',
              "int main(void) {"]
