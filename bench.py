@@ -42,6 +42,23 @@ N_FLASH = 4096
 FLASH_TC_TRAFFIC = 636_147_456
 
 
+def max_over_ranks(ms, device):
+    """The slowest rank's time (ms): every rank takes the same collective step;
+    one rank alone returns its own time."""
+    import torch
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return float(ms)
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, ms):
+    """Whole-job throughput of ``world`` replicas (weak scaling): the units all
+    ranks processed over the slowest rank's time."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def workload():
     from lighthit_b200.model import KernelConfig, synthetic_detector
     from lighthit_b200.workloads import flash_batch_sizes, flash_positions
@@ -324,11 +341,8 @@ def ours(args, rank, world, local_rank):
         torch.distributed.barrier()
     step_ms = np.array([a.elapsed_time(b) for a, b in ev])
     total_ms = float(step_ms.sum())
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * F * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks(total_ms, dev)
+    value = job_rate(F * args.steps, world, total_ms)
 
     # roofline of the fused kernel: algorithmic bytes = outputs written per (flash, OM)
     per_pair = 65 * 3 * 8 + 3 * 160 * 4 + 3 * 8 + 8 + 1
@@ -401,11 +415,8 @@ def ours(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     wall = time.perf_counter() - w0
     e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * F * e2e_steps / (e2e_ms / 1e3)
+    e2e_ms = max_over_ranks(e2e_ms, dev)
+    e2e_value = job_rate(F * e2e_steps, world, e2e_ms)
     h2d = F * (3 * 8 + 8 + 8)
     d2h = F * 48 * per_pair
 
