@@ -100,6 +100,13 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to start: wait for its first sample (taken
+        # before the timed region, not kept) so that sampling runs throughout
+        import select
+        ready, _, _ = select.select([self.proc.stdout], [], [], 10.0)
+        if ready:
+            self.proc.stdout.readline()
         return self
 
     def __exit__(self, *exc):
