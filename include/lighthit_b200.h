@@ -120,6 +120,9 @@ typedef struct {
 size_t lh_flash_workspace_bytes(const lh_flash_problem* p, const lh_readout_operator* op,
                                 int mode, int32_t n_flash);
 
+/* The fused modes (LH_MODE_SPLIT_BF16, LH_MODE_BF16) read op->b_hi / b_lo with
+ * their K columns as (Re, Im) per frequency (the A tile's order: one bf16x2
+ * store per value); LH_MODE_PLAIN_FP32 reads op->b_fp32 in the order above. */
 int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op, int mode,
                        const lh_flash_batch* b, void* workspace, size_t workspace_bytes,
                        void* stream);

@@ -376,15 +376,18 @@ flash_tc_kernel(lh_flash_problem p, lh_flash_batch b, const __nv_bfloat16* __res
         const int lp = i / nw, w = i % nw;
         float2 r1, r2;
         flash_item(p, b, base + lp, w, sp[lp], r1, r2);
-        __nv_bfloat16 hi, lo;
-        split_bf16(r1.x, hi, lo);
-        s_ahi[a_offset(2 * lp, w)] = hi;       s_alo[a_offset(2 * lp, w)] = lo;
-        split_bf16(r1.y, hi, lo);
-        s_ahi[a_offset(2 * lp, nw + w)] = hi;  s_alo[a_offset(2 * lp, nw + w)] = lo;
-        split_bf16(r2.x, hi, lo);
-        s_ahi[a_offset(2 * lp + 1, w)] = hi;   s_alo[a_offset(2 * lp + 1, w)] = lo;
-        split_bf16(r2.y, hi, lo);
-        s_ahi[a_offset(2 * lp + 1, nw + w)] = hi; s_alo[a_offset(2 * lp + 1, nw + w)] = lo;
+        // K columns (Re, Im) per frequency: one bf16x2 store per row and part
+        const __nv_bfloat162 h1 = __floats2bfloat162_rn(r1.x, r1.y);
+        const __nv_bfloat162 l1 = __floats2bfloat162_rn(r1.x - __low2float(h1),
+                                                        r1.y - __high2float(h1));
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(r2.x, r2.y);
+        const __nv_bfloat162 l2 = __floats2bfloat162_rn(r2.x - __low2float(h2),
+                                                        r2.y - __high2float(h2));
+        const int o1 = a_offset(2 * lp, 2 * w), o2 = a_offset(2 * lp + 1, 2 * w);
+        *reinterpret_cast<__nv_bfloat162*>(s_ahi + o1) = h1;
+        *reinterpret_cast<__nv_bfloat162*>(s_alo + o1) = l1;
+        *reinterpret_cast<__nv_bfloat162*>(s_ahi + o2) = h2;
+        *reinterpret_cast<__nv_bfloat162*>(s_alo + o2) = l2;
       }
     }
     fence_proxy_async();  // generic-proxy smem writes -> visible to the tensor core

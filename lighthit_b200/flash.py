@@ -128,7 +128,8 @@ class FlashTransport:
         self._coef = torch.view_as_real(torch.from_numpy(coef)).contiguous().to(dev)
         self._edges = f64(config.relative_time_edges_ns)
         self.readout = DeviceReadout(omega, config.relative_time_edges_ns,
-                                     config.readout_omega_per_ns, device=dev)
+                                     config.readout_omega_per_ns, device=dev,
+                                     interleaved_tc=True)
         medium = table.medium
         self.problem = _lib.FlashProblem(
             n, self._om_pos.data_ptr(), self._om_look.data_ptr(), self._om_area.data_ptr(), top,

@@ -68,7 +68,11 @@ def readout_matrix(omega, edges_ns, readout_omega=None):
 class DeviceReadout:
     """The readout operator resident on the device in every precision layout."""
 
-    def __init__(self, omega, edges_ns, readout_omega=None, *, device="cuda"):
+    def __init__(self, omega, edges_ns, readout_omega=None, *, device="cuda",
+                 interleaved_tc=False):
+        """``interleaved_tc``: the BF16 operands (``b_hi``, ``b_lo``) take their K
+        columns as (Re, Im) per frequency, the layout the fused flash kernel's
+        A tile uses; ``b_fp32`` keeps (Re..., Im...)."""
         import torch
         W = readout_matrix(omega, edges_ns, readout_omega)
         n_bins, n_omega = W.shape
@@ -84,7 +88,13 @@ class DeviceReadout:
         self.b_fp32 = torch.tensor(B, dtype=torch.float32, device=device)
         padded = torch.zeros((self.n_tiles * self.n_tile, self.k_pad), dtype=torch.float32,
                              device=device)
-        padded[:n_bins] = self.b_fp32
+        if interleaved_tc:
+            Bi = np.zeros((n_bins, self.k_pad))
+            Bi[:, 0:2 * n_omega:2] = W.real
+            Bi[:, 1:2 * n_omega:2] = -W.imag
+            padded[:n_bins] = torch.tensor(Bi, dtype=torch.float32, device=device)
+        else:
+            padded[:n_bins] = self.b_fp32
         hi = padded.to(torch.bfloat16)
         lo = (padded - hi.float()).to(torch.bfloat16)
 
