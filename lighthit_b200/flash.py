@@ -24,7 +24,7 @@ from .model import C_VACUUM_M_PER_NS, Medium, TransportResponse, acceptance_coef
 from .readout import DeviceReadout
 from .spline import spline_coefficients
 
-__all__ = ["FlashTable", "FlashTransport", "BroadbandFlashTransport"]
+__all__ = ["FlashTable", "FlashTransport", "BroadbandFlashTransport", "flash_node_photons"]
 
 
 @dataclass
@@ -252,6 +252,20 @@ class FlashTransport:
              "readout_precision": self.mode, "route": "lighthit_b200.flash"})
 
 
+def flash_node_photons(nodes_nm, weights_nm, photons, spectral_shape):
+    """``_flash_nodes`` (``transport.py:1049-1059``): photons of each flash at each
+    wavelength node, ``photons * weight * shape / (weight . shape)`` ((node, flash))."""
+    nodes = np.asarray(nodes_nm, float)
+    weights = np.asarray(weights_nm, float)
+    shape = np.asarray(spectral_shape(nodes), float)
+    if shape.shape != nodes.shape or not np.isfinite(shape).all() or np.any(shape < 0):
+        raise ValueError("flash spectral_shape must return finite nonnegative values")
+    norm = float(weights @ shape)
+    if norm <= 0:
+        raise ValueError("flash spectral_shape has zero integral")
+    return np.outer(weights * shape / norm, np.atleast_1d(np.asarray(photons, float)))
+
+
 class BroadbandFlashTransport:
     """Isotropic flashes with a spectral shape (``IsotropicFlash.broadband``).
 
@@ -293,13 +307,7 @@ class BroadbandFlashTransport:
 
     def node_photons(self, photons, spectral_shape):
         """``_flash_nodes`` (``transport.py:1049-1059``): (node, flash) photons."""
-        shape = np.asarray(spectral_shape(self.nodes), float)
-        if shape.shape != self.nodes.shape or not np.isfinite(shape).all() or np.any(shape < 0):
-            raise ValueError("flash spectral_shape must return finite nonnegative values")
-        norm = float(self.weights @ shape)
-        if norm <= 0:
-            raise ValueError("flash spectral_shape has zero integral")
-        return np.outer(self.weights * shape / norm, np.asarray(photons, float))
+        return flash_node_photons(self.nodes, self.weights, photons, spectral_shape)
 
     def run(self, positions, photons, time_ns, spectral_shape, *, stream=None):
         """A batch of flashes sharing one spectral shape: device outputs (checked)."""
