@@ -18,9 +18,10 @@ are the device kernels of this package:
 Tables are built once by the reference and stored under ``tables/``
 (``build_tables.py``): the folded >=2 kernels, the first radial interval of the
 per-wavelength kernels (near field) and the route's medium and detector
-constants. What the device route does not cover raises
-``NotImplementedError`` with the reason (elements below threshold in a node
-band, receiver subsets).
+constants. Elements above the Cherenkov threshold in only some bands run as
+the reference's per-band order-1 units and per-band source lattices; receiver
+subsets (``receivers=``) run on ``ShowerTables.subset``. A table without its
+near-field file raises ``NotImplementedError`` when a shower needs the clamp.
 Order 1 follows the reference's global screen (``prompt.py:720-812``): a
 coarse charge pass (2 m cells, 8-pixel faces, 24 ring nodes) for every OM in
 reach, full resolution where ``q0 + extra + 3 q1_coarse`` reaches threshold,
