@@ -113,7 +113,9 @@ typedef struct {
   uint8_t* active;             /* [n_flash][n_om] bit0 active, bit1 unsafe, bit2 coincident */
   int32_t* status;             /* [4]: flags, unsafe count, max unsafe radius (double bits) */
   const int32_t* n_flash_device; /* optional: device count (<= n_flash) read by the kernel, so
-                                    one captured CUDA graph sized for n_flash serves any batch */
+                                    one captured CUDA graph sized for n_flash serves any batch;
+                                    the plain FP32 path writes zero order-1/2 bins for the
+                                    flashes past it, the fused path leaves them untouched */
   int32_t block_threads;       /* fused kernel CTA size: 0 (default 512), 256 or 512 */
 } lh_flash_batch;
 
@@ -550,8 +552,11 @@ int lh_near_field(const lh_near_table* t, const lh_near_problem* p, void* worksp
  * 48-OM array at k_pad = 144; larger batches return LH_ESCRATCH and launch
  * nothing. The caller still passes inputs and outputs. The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with that
- * device current, so make it before any stream capture. All calls on a device
- * share the array: calls that overlap on the GPU race and must be serialised. */
+ * device current, so make it before any stream capture. The address is kept
+ * for the life of the process: after cudaDeviceReset on a device (which ends
+ * the context the address belongs to) this entry point must not be called on
+ * that device again. All calls on a device share the array: calls that overlap
+ * on the GPU race and must be serialised. */
 #define LH_ESCRATCH 6   /* request larger than the static scratch of the entry point below */
 int lh_flash_transport_noalloc(const lh_flash_problem* p, const lh_readout_operator* op,
                                const lh_flash_batch* b, void* stream);

@@ -278,20 +278,25 @@ flash_plain_kernel(lh_flash_problem p, lh_flash_batch b, int kpad, int n_bins, f
   flash_tile_setup(p, b, sp, base, n_pairs);
   __syncthreads();
   const int nw = p.n_omega;
+  // Every row the readout reads (2 per pair of the host count, whose grid
+  // follows) is written in full here: pairs past the device count get zero
+  // rows (flash_item yields zero spectra for them), and the padding columns
+  // 2 nw .. kpad-1 are zeroed whatever their number.
+  const int64_t host_pairs = (int64_t)b.n_flash * p.n_om;
   for (int i = threadIdx.x; i < kFlashPairs * nw; i += blockDim.x) {
     const int lp = i / nw, w = i % nw;
     float2 r1, r2;
     flash_item(p, b, base + lp, w, sp[lp], r1, r2);
-    if (sp[lp].valid) {
+    if (base + lp < host_pairs) {
       float* row1 = a_rows + (2 * (base + lp)) * (int64_t)kpad;
       float* row2 = row1 + kpad;
       row1[w] = r1.x;
       row1[nw + w] = r1.y;
       row2[w] = r2.x;
       row2[nw + w] = r2.y;
-      if (w < kpad - 2 * nw) {
-        row1[2 * nw + w] = 0.f;
-        row2[2 * nw + w] = 0.f;
+      for (int c = 2 * nw + w; c < kpad; c += nw) {
+        row1[c] = 0.f;
+        row2[c] = 0.f;
       }
     }
   }

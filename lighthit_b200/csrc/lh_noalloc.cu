@@ -11,10 +11,12 @@
 // The array's host-side name is only a stand-in for the symbol, not a device
 // address. Its device address is looked up with cudaGetSymbolAddress once per
 // device, with that device current, on the first call made on that device; that
-// first call should therefore come before any stream capture. Every call on a
-// device shares the one array and it keeps the last call's contents: calls whose
-// work overlaps on the GPU (other streams, other host threads) race on it and
-// must be serialised by the caller.
+// first call should therefore come before any stream capture. The address is
+// cached for the life of the process; cudaDeviceReset ends the context it
+// belongs to, so a process that resets a device must not call this entry point
+// on that device afterwards. Every call on a device shares the one array and it
+// keeps the last call's contents: calls whose work overlaps on the GPU (other
+// streams, other host threads) race on it and must be serialised by the caller.
 #include <cstdio>
 #include <mutex>
 
@@ -81,8 +83,10 @@ extern "C" int lh_flash_transport_noalloc(const lh_flash_problem* p, const lh_re
   void* scratch = nullptr;
   int rc = scratch_address(&scratch);
   if (rc != LH_OK) return rc;
-  // Nothing in the scratch has to start at zero: every readout row the second
-  // kernel reads is written in full (padding included) by the first.
+  // Nothing in the scratch has to start at zero: flash_plain_kernel writes all
+  // 2 * n_flash * n_om rows the readout reads (zero rows for flashes past a
+  // device count, every padding column zeroed), so no earlier call's rows
+  // reach the output.
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   float* rows = static_cast<float*>(scratch);
   const int64_t tiles = (n_pairs + 63) / 64;

@@ -35,8 +35,13 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-SRC = Path(os.environ.get("LIGHTHIT_REFERENCE_SRC", "/root/reference/src"))
-WORK = Path(os.environ.get("LIGHTHIT_TABLE_WORK", REPO / "_work" / "tables"))
+
+
+def _required(name, what):
+    value = os.environ.get(name)
+    if not value:
+        raise SystemExit(f"set {name} to {what}")
+    return Path(value)
 
 BASE = dict(wavelength_nodes=3, degree=8, azimuthal_degree=2, readout_nodes=321,
             bin_ns=5.0, window_end_ns=740.0)
@@ -77,8 +82,10 @@ def write_near(name, route, tables):
 
 
 def main(name, near_only=False):
-    os.environ.setdefault("NUMBA_CACHE_DIR", str(REPO / "_work" / "numba-cache"))
-    sys.path.insert(0, str(SRC))
+    src = _required("LIGHTHIT_REFERENCE_SRC", "the reference's src folder")
+    work = _required("LIGHTHIT_TABLE_WORK", "a writable folder for the reference's RTE caches")
+    os.environ.setdefault("NUMBA_CACHE_DIR", str(work / "numba-cache"))
+    sys.path.insert(0, str(src))
     import lighthit as lh
     from lighthit.ballistic_interval import BallisticIntervalConfig, prepare_optics
     from lighthit.examples.synthetic import baikal_like_detector, synthetic_medium_model
@@ -86,7 +93,7 @@ def main(name, near_only=False):
     from lighthit.shower import ShowerData, ShowerTransport
 
     c = CONFIGS[name]
-    cache = WORK / f"shower-{name}"
+    cache = work / f"shower-{name}"
     medium = synthetic_medium_model()
     detector = baikal_like_detector(clusters=c["clusters"])
     omega = np.linspace(0.0, 1.2, 65)

@@ -27,7 +27,7 @@ from pathlib import Path
 import numpy as np
 
 sys.path.insert(0, str(Path(__file__).resolve().parent))
-from _refenv import REPO, use_reference  # noqa: E402
+from _refenv import REPO, table_work as _refenv_table_work, use_reference  # noqa: E402
 
 lh = use_reference()
 sys.path.insert(0, str(REPO))
@@ -37,7 +37,7 @@ from lighthit.shower import ShowerData, ShowerTransport  # noqa: E402
 from lighthit_b200.workloads import gaussian_shower, shower_stream  # noqa: E402
 
 N_SHOWERS = 12
-CACHE = Path(os.environ.get("LIGHTHIT_TABLE_WORK", REPO / "_work" / "tables")) / "shower-c2"
+CACHE = _refenv_table_work() / "shower-c2"
 
 
 def elements(s):
