@@ -6,9 +6,54 @@ Restates ``apply_folded`` (``shower/ge2.py:99-119``) ->
 small-d recurrence and real harmonics of ``_directional_numba.py:37-128,389-397``
 in float64 NumPy (loops over OM and point, vectorised over band and frequency).
 """
+import ctypes as C
 from math import exp, lgamma
 
 import numpy as np
+
+from .build import build
+
+_LIB = None
+
+
+def _apply_c(points, receivers, looks, channels, out_scale, starts, degree, max_m, max_out, alpha,
+             pair_lambda, pair_mu, log_r, coefficients, absorption, velocity, omega, flight,
+             radial_low, radial_high):
+    """``apply_multi_spectral_local`` in C (``o2c_apply``): (receiver, frequency)."""
+    global _LIB
+    if _LIB is None:
+        _LIB = C.CDLL(str(build()))
+        _LIB.o2c_apply.restype = C.c_int
+
+    def f(a):
+        return np.ascontiguousarray(a, dtype=np.float64)
+
+    def c(a):
+        return np.ascontiguousarray(a, dtype=np.complex128)
+
+    def i(a):
+        return np.ascontiguousarray(a, dtype=np.int64)
+
+    def p(a):
+        return C.c_void_p(a.ctypes.data)
+
+    points, receivers, looks = f(points), f(receivers), f(looks)
+    channels, coefficients = c(channels), c(coefficients)
+    out_scale, alpha, log_r = f(out_scale), f(alpha), f(log_r)
+    absorption, velocity, omega = f(absorption), f(velocity), f(omega)
+    starts, pair_lambda, pair_mu = i(starts), i(pair_lambda), i(pair_mu)
+    result = np.zeros((len(receivers), len(omega)), complex)
+    rc = _LIB.o2c_apply(C.c_int64(len(points)), p(points), C.c_int64(len(receivers)), p(receivers),
+                        p(looks), C.c_int(channels.shape[0]), C.c_int(channels.shape[2]),
+                        p(channels), p(out_scale), p(starts), C.c_int(degree), C.c_int(max_m),
+                        C.c_int(max_out), p(alpha), C.c_int(len(pair_lambda)), p(pair_lambda),
+                        p(pair_mu), C.c_int(len(log_r)), p(log_r), p(coefficients),
+                        p(absorption), p(velocity), C.c_int(len(omega)), p(omega),
+                        C.c_int(int(bool(flight))), C.c_double(radial_low),
+                        C.c_double(radial_high), p(result))
+    if rc:
+        raise MemoryError("oracle order >=2 apply: scratch allocation failed")
+    return result
 
 
 def parity(n):
@@ -200,8 +245,9 @@ def apply_multi_spectral_local(points, receivers, looks, channels, out_scale, st
     return result
 
 
-def apply_folded(folded, sources, positions, looks, alpha, area, window):
-    """``apply_folded`` -> ``apply_multi_spectral`` for sources sharing one point set.
+def apply_folded(folded, sources, positions, looks, alpha, area, window, *, fast=False):
+    """``apply_folded`` -> ``apply_multi_spectral`` for sources sharing one point set
+    (``fast``: the same loops in C, ``oracle/ge2.c``).
 
     ``sources``: dict with ``points_m`` (P,3), ``channels`` (band, P, nch, W),
     ``reference_ns`` (band,), ``frame`` (centre, first, second, axis),
@@ -228,6 +274,15 @@ def apply_folded(folded, sources, positions, looks, alpha, area, window):
     max_m = min(az, int(folded["degree"]))
     acc = int(folded["acceptance_degree"])
     out_scale = np.repeat(np.asarray(area, float)[None, :], channels.shape[0], axis=0)
+    if fast:
+        result = _apply_c(
+            rotate(np.asarray(sources["points_m"], float) - centre),
+            rotate(np.asarray(positions) - centre), rotate(looks), channels, out_scale,
+            np.asarray(starts), int(folded["degree"]), max_m, acc, np.asarray(alpha, float)[:acc + 1],
+            folded["pair_lambda"], folded["pair_mu"], np.asarray(folded["log_r"], float),
+            np.asarray(folded["coefficients"]), np.asarray(folded["absorption"], float),
+            np.asarray(folded["speed"], float), omega, str(folded["phase"]) == "flight", low, high)
+        return result.T * np.exp(1j * omega * reference)[:, None]
     result = apply_multi_spectral_local(
         rotate(np.asarray(sources["points_m"], float) - centre), rotate(np.asarray(positions) - centre),
         rotate(looks), channels, out_scale, np.asarray(starts), int(folded["degree"]), max_m, acc,
