@@ -322,6 +322,15 @@ typedef struct {
   const double* gauss_tau;     /* [n_gauss] on [0, pi/2]                              */
   const double* gauss_w;       /* [n_gauss]                                          */
   int32_t group_capacity;      /* group table slots per OM (power of two, <= 2^20)   */
+  /* The coarse charge screen (compress_screen / screen_order1,
+   * _prompt_screen.py:91-503) when nonzero: stage A builds pencils at
+   * pixel_face under parents at parent_face (pixel_face a multiple of it) and
+   * writes parents then children with each child's parent row; stage B uses a
+   * parent unless the OM lies inside its angular extent, else its children,
+   * keys without the arrival time, the two-node radial rule near the pencil
+   * direction and path grids without a window edge (charge only). */
+  int32_t screen;
+  int32_t parent_face;
 } lh_order1_config;
 
 typedef struct {
@@ -351,6 +360,8 @@ typedef struct {
   double* var_major;           /* [capacity]                                         */
   double* var_minor;           /* [capacity]                                         */
   double* pos_cov;             /* [capacity][6] xx yy zz xy xz yz                    */
+  int32_t* parent;             /* [capacity] screen tables: parent row of a child,
+                                  -1 for a parent (NULL otherwise)                   */
 } lh_order1_pencil_table;
 
 /* Workspace for n_subseg sub-segments and n_work OMs (both stages). */
@@ -541,6 +552,28 @@ typedef struct {
 size_t lh_near_workspace_bytes(const lh_near_table* t, const lh_near_problem* p);
 int lh_near_field(const lh_near_table* t, const lh_near_problem* p, void* workspace,
                   size_t workspace_bytes, void* stream);
+
+/* Kernel timing for measurement runs (the reference reports per-stage wall
+ * times in metadata['timings'], shower/api.py:243-420; these are the device
+ * durations of the main kernels behind those stages). lh_kernel_timing(1)
+ * clears the record and starts it; while on, every timed launch records a CUDA
+ * event pair on its own stream (not while that stream is being captured).
+ * lh_kernel_timing_read waits for the recorded events and returns per kernel
+ * id the launch count and the summed milliseconds. */
+enum {
+  LH_KT_ORDER0 = 0,      /* order0_kernel (lh_order0)                */
+  LH_KT_O1_RING = 1,     /* o1_ring_kernel (lh_order1_pencils)       */
+  LH_KT_O1_GROUP = 2,    /* o1_group_kernel (lh_order1_grouped)      */
+  LH_KT_O1_BATCH = 3,    /* o1_batch_kernel (lh_order1_grouped)      */
+  LH_KT_GE2_APPLY = 4,   /* ge2_apply_batch_kernel (lh_ge2_apply_batch) */
+  LH_KT_SRC_GROUP = 5,   /* src_group_kernel (lh_source_compile)     */
+  LH_KT_SRC_TRANSFORM = 6, /* src_transform_kernel (lh_source_compile) */
+  LH_KT_READOUT = 7,     /* readout_tc_kernel (lh_readout_rows)      */
+  LH_KT_FLASH = 8,       /* flash_tc_kernel (lh_flash_transport)     */
+  LH_KT_COUNT = 9
+};
+int lh_kernel_timing(int enable);
+int lh_kernel_timing_read(int32_t n_kernels, int64_t* launches, double* total_ms);
 
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory

@@ -109,7 +109,8 @@ class Order1Config(C.Structure):
                 ("smoothing_factor", C.c_double), ("theta_lo", C.c_double),
                 ("theta_ratio", C.c_double), ("tau_step", C.c_double), ("log_r_step", C.c_double),
                 ("theta_bins", C.c_int32), ("speed_ref", C.c_double), ("n_gauss", C.c_int32),
-                ("gauss_tau", P), ("gauss_w", P), ("group_capacity", C.c_int32)]
+                ("gauss_tau", P), ("gauss_w", P), ("group_capacity", C.c_int32),
+                ("screen", C.c_int32), ("parent_face", C.c_int32)]
 
 
 class Order1Elements(C.Structure):
@@ -121,7 +122,8 @@ class Order1Elements(C.Structure):
 
 class Order1PencilTable(C.Structure):
     _fields_ = [("capacity", C.c_int32), ("position", P), ("direction", P), ("w0", P), ("w2", P),
-                ("time", P), ("major", P), ("var_major", P), ("var_minor", P), ("pos_cov", P)]
+                ("time", P), ("major", P), ("var_major", P), ("var_minor", P), ("pos_cov", P),
+                ("parent", P)]
 
 
 class SourceProblem(C.Structure):
@@ -184,6 +186,8 @@ SIGNATURES = {
                                      C.POINTER(FlashBatch), P, C.c_size_t, P]),
     "lh_flash_transport_noalloc": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(ReadoutOperator),
                                              C.POINTER(FlashBatch), P]),
+    "lh_kernel_timing": (C.c_int, [C.c_int]),
+    "lh_kernel_timing_read": (C.c_int, [C.c_int32, P, P]),
     "lh_flash_combine": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(FlashNodes),
                                    C.POINTER(FlashBatch), P]),
     "lh_ge2_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem)]),
@@ -212,6 +216,10 @@ SIGNATURES = {
     "lh_wait_selftest": (C.c_int, [P, C.c_int64, P]),
 }
 LH_ESCRATCH = 6
+# kernel ids of lh_kernel_timing_read
+TIMED_KERNELS = ("order0_kernel", "o1_ring_kernel", "o1_group_kernel", "o1_batch_kernel",
+                 "ge2_apply_batch_kernel", "src_group_kernel", "src_transform_kernel",
+                 "readout_tc_kernel", "flash_tc_kernel")
 
 _lib = None
 
@@ -280,3 +288,20 @@ def upload_parts(parts, dtype, device):
 
 def stream_ptr(stream):
     return C.c_void_p(stream.cuda_stream) if stream is not None else None
+
+
+def kernel_timing(enable=True):
+    """Start (clearing the record) or stop the library's kernel timing."""
+    check(load().lh_kernel_timing(int(bool(enable))), "lh_kernel_timing")
+
+
+def kernel_times():
+    """``{kernel: (launches, total_ms)}`` of the timed launches since the last read."""
+    import numpy as np
+    n = len(TIMED_KERNELS)
+    launches = np.zeros(n, np.int64)
+    total = np.zeros(n)
+    check(load().lh_kernel_timing_read(n, launches.ctypes.data, total.ctypes.data),
+          "lh_kernel_timing_read")
+    return {name: (int(launches[k]), float(total[k])) for k, name in enumerate(TIMED_KERNELS)
+            if launches[k]}

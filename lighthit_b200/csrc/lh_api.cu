@@ -4,6 +4,7 @@
 #include <cstdio>
 
 #include "lh_common.cuh"
+#include "lh_timing.cuh"
 #include "lh_readout.cuh"
 
 namespace lh {
@@ -107,10 +108,13 @@ int lh_readout_rows(const lh_readout_operator* op, int mode, const void* a_packe
   if (smem > 227 * 1024) return LH_EUNSUPPORTED;
   cudaFuncSetAttribute(readout_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int grid = (int)(tiles < sm_count() ? tiles : sm_count());
-  readout_tc_kernel<<<grid, 128, smem, s>>>(
-      hi, lo, rows, op->k_pad, reinterpret_cast<const __nv_bfloat16*>(op->b_hi),
-      reinterpret_cast<const __nv_bfloat16*>(op->b_lo), op->n_bins, op->n_tile, op->n_tiles,
-      passes_of(mode), map, out, status);
+  {
+    lh::TimedLaunch timed_launch(LH_KT_READOUT, s);
+    readout_tc_kernel<<<grid, 128, smem, s>>>(
+        hi, lo, rows, op->k_pad, reinterpret_cast<const __nv_bfloat16*>(op->b_hi),
+        reinterpret_cast<const __nv_bfloat16*>(op->b_lo), op->n_bins, op->n_tile, op->n_tiles,
+        passes_of(mode), map, out, status);
+  }
   return check_launch();
 }
 
@@ -152,9 +156,12 @@ int lh_flash_transport(const lh_flash_problem* p, const lh_readout_operator* op,
   int grid = (int)(tiles < sm_count() ? tiles : sm_count());
   const int threads = b->block_threads == 0 ? 512 : b->block_threads;
   if (threads != 256 && threads != 512) return LH_EINVAL;
-  flash_tc_kernel<<<grid, threads, smem, s>>>(*p, *b, reinterpret_cast<const __nv_bfloat16*>(op->b_hi),
-                                          reinterpret_cast<const __nv_bfloat16*>(op->b_lo),
-                                          op->k_pad, op->n_bins, op->n_tile, passes_of(mode));
+  {
+    lh::TimedLaunch timed_launch(LH_KT_FLASH, s);
+    flash_tc_kernel<<<grid, threads, smem, s>>>(*p, *b, reinterpret_cast<const __nv_bfloat16*>(op->b_hi),
+                                            reinterpret_cast<const __nv_bfloat16*>(op->b_lo),
+                                            op->k_pad, op->n_bins, op->n_tile, passes_of(mode));
+  }
   return check_launch();
 }
 

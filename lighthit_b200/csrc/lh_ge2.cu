@@ -23,6 +23,7 @@
 #include <algorithm>
 
 #include "lh_common.cuh"
+#include "lh_timing.cuh"
 #include "lh_harmonics.cuh"
 
 namespace lh {
@@ -459,7 +460,10 @@ int ge2_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n, 
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(ge2_apply_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
-    ge2_apply_batch_kernel<<<dim3(max_om, max_chunks, n), 256, smem, s>>>(T, slots, A);
+    {
+      lh::TimedLaunch timed_launch(LH_KT_GE2_APPLY, s);
+      ge2_apply_batch_kernel<<<dim3(max_om, max_chunks, n), 256, smem, s>>>(T, slots, A);
+    }
   }
   ge2_reduce_batch_kernel<<<dim3((unsigned)((max_outs + 255) / 256), n), 256, 0, s>>>(T, slots, A);
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;

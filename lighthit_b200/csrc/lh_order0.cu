@@ -35,6 +35,7 @@
 #include <algorithm>
 
 #include "lh_common.cuh"
+#include "lh_timing.cuh"
 
 namespace lh {
 
@@ -750,7 +751,10 @@ int order0_launch(const lh_order0_optics& O, const lh_order0_batch& B, cudaStrea
   order0_candidates_kernel<false><<<blocks, 256, 0, s>>>(O, B, W);
   order0_scan_kernel<<<1, 1024, 0, s>>>((int32_t)keys, W);
   order0_candidates_kernel<true><<<blocks, 256, 0, s>>>(O, B, W);
-  order0_kernel<<<148 * 8, kO0Threads, smem, s>>>(O, B, W);
+  {
+    lh::TimedLaunch timed_launch(LH_KT_ORDER0, s);
+    order0_kernel<<<148 * 8, kO0Threads, smem, s>>>(O, B, W);
+  }
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }
 

@@ -31,6 +31,7 @@
 #include <algorithm>
 
 #include "lh_common.cuh"
+#include "lh_timing.cuh"
 
 namespace lh {
 
@@ -261,6 +262,59 @@ LH_DEVICE int o1_block_exclusive_scan(int v, int& total) {
   return inclusive - v + (warp ? warp_sums[warp - 1] : 0);
 }
 
+// The slot of `key` in an ordered-start table, or -1 when absent.
+LH_DEVICE int64_t o1_find(const long long* keys, int64_t capacity, long long key) {
+  const uint64_t mask = (uint64_t)capacity - 1;
+  uint64_t slot = (uint64_t)key & mask;
+  for (int64_t probe = 0; probe < capacity; ++probe) {
+    const long long k = keys[slot];
+    if (k == key) return (int64_t)slot;
+    if (k == -1ll) return -1;
+    slot = (slot + 1) & mask;
+  }
+  return -1;
+}
+
+// parent_keys (_prompt_screen.py:44-54): the pixel of the nested parent face
+// in the same position cell.
+LH_DEVICE long long o1_parent_key(long long key, int face, int parent_face) {
+  const long long per_cell = 6ll * face * face;
+  const long long cell = key / per_cell, pixel = key % per_cell;
+  const long long cube = pixel / ((long long)face * face), ij = pixel % ((long long)face * face);
+  const long long i = ij / face, j = ij % face, factor = face / parent_face;
+  return cell * (6ll * parent_face * parent_face) + (cube * parent_face + i / factor) * parent_face +
+         j / factor;
+}
+
+// compress_screen's parents (_prompt_screen.py:56-85): every occupied child
+// slot adds its moments to its parent pixel's slot (the parents of one cell
+// are the sums of its children, as finish_pencils sums them).
+__global__ void __launch_bounds__(kO1FinishThreads)
+o1_parent_kernel(const long long* keys, const double* rows, int64_t capacity, int face,
+                 int parent_face, long long* parent_keys, double* parent_rows,
+                 int64_t parent_capacity, int32_t* status) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t slot = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; slot < capacity;
+       slot += stride) {
+    const long long key = keys[slot];
+    if (key == -1ll) continue;
+    bool fresh;
+    const int64_t ps = o1_insert(parent_keys, parent_capacity,
+                                 o1_parent_key(key, face, parent_face), fresh, true);
+    if (ps < 0) {
+      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+      continue;
+    }
+    for (int k = 0; k < kO1Moments; ++k)
+      atomicAdd(parent_rows + ps * kO1Moments + k, rows[slot * kO1Moments + k]);
+  }
+}
+
+// Pencils of a screen table: parents plus children.
+__global__ void o1_total_kernel(const int32_t* children, const int32_t* parents, int32_t* total) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *total = *children + *parents;
+}
+
 // Used slots per tile of the ring table.
 __global__ void __launch_bounds__(kO1FinishThreads)
 o1_tile_count_kernel(const long long* keys, const double* rows, int64_t capacity,
@@ -297,14 +351,20 @@ LH_DEVICE void o1_write_pencil(const double* a, lh_order1_pencil_table& Pn, int 
 // over kO1Tile / kO1FinishThreads consecutive slots, ranks by a CTA scan plus
 // the tile's offset. Slot order follows the keys, so pencils of a cell are
 // neighbours in the table.
+// Screen tables (the coarse charge screen) take their parents first: parent
+// rows [0, n_parents) record their row per slot in `slot_row`; child rows
+// follow from `base_count` and look up their parent's row by its key.
 __global__ void __launch_bounds__(kO1FinishThreads)
 o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
                  lh_order1_pencil_table Pn, const int32_t* tile_offset, const int32_t* count,
+                 const int32_t* base_count, int32_t* slot_row, const long long* parent_keys,
+                 int64_t parent_capacity, const int32_t* parent_row, int face, int parent_face,
                  int32_t* status) {
   const int per = kO1Tile / kO1FinishThreads;
   const int64_t begin = blockIdx.x * (int64_t)kO1Tile + threadIdx.x * per;
   const int64_t n = *count;
-  if (n > Pn.capacity) {  // the caller redoes the stage with a larger table
+  const int64_t base = base_count ? *base_count : 0;
+  if (base + n > Pn.capacity) {  // the caller redoes the stage with a larger table
     if (blockIdx.x == 0 && threadIdx.x == 0)
       atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
     return;
@@ -321,7 +381,19 @@ o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
     // rank q goes to row (q * 2^31-1) mod n, a fixed permutation (2^31 - 1 is
     // prime and n < 2^31): stage B's warps then see pencils of many cells, not
     // a run of one cell's pencils competing for the same group rows
-    o1_write_pencil(rows + slot * kO1Moments, Pn, (int)((q * 2147483647ll) % n));
+    const int row = (int)(base + (q * 2147483647ll) % n);
+    o1_write_pencil(rows + slot * kO1Moments, Pn, row);
+    if (slot_row) slot_row[slot] = row;
+    if (Pn.parent) {
+      int32_t parent = -1;
+      if (parent_keys) {
+        const int64_t ps = o1_find(parent_keys, parent_capacity,
+                                   o1_parent_key(keys[slot], face, parent_face));
+        if (ps < 0) atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+        else parent = parent_row[ps];
+      }
+      Pn.parent[row] = parent;
+    }
     ++q;
   }
 }
@@ -387,6 +459,59 @@ LH_DEVICE double o1_gauss_inverse_mean(double u, double v, double var_u, double 
   return 2.0 / sqrt(kPi) * s0 * total;
 }
 
+// The coarse screen's refinement test (_prompt_screen.py:233-240): the OM
+// looks into pencil x's angular extent (forward, theta^2 < s^2 extent^2).
+LH_DEVICE bool o1_refined(const lh_order1_config& C, const lh_order1_pencil_table& Pn, int x,
+                          double rx, double ry, double rz) {
+  const double dx = rx - Pn.position[3 * x], dy = ry - Pn.position[3 * x + 1],
+               dz = rz - Pn.position[3 * x + 2];
+  const double r = sqrt(dx * dx + dy * dy + dz * dz);
+  const double hx = dx / r, hy = dy / r, hz = dz / r;
+  const double sx = Pn.direction[3 * x], sy = Pn.direction[3 * x + 1], sz = Pn.direction[3 * x + 2];
+  const double cosine = hx * sx + hy * sy + hz * sz;
+  const double qx = hx - cosine * sx, qy = hy - cosine * sy, qz = hz - cosine * sz;
+  const double theta = atan2(sqrt(qx * qx + qy * qy + qz * qz), cosine);
+  const double* cov = Pn.pos_cov + 6 * x;
+  const double extent2 = Pn.var_major[x] + (cov[0] + cov[1] + cov[2]) / (r * r);
+  const double sf = C.smoothing_factor;
+  return theta < 0.5 * kPi && theta * theta < sf * sf * extent2;
+}
+
+// inverse_radius_rule (_prompt_screen.py:101-140): a positive two-node rule
+// for the Gaussian measure over the radius (w0, t0, w1, t1).
+LH_DEVICE void o1_inverse_radius_rule(double u, double v, double var_u, double var_v,
+                                      const double* tangent, const double* wsec2, int n,
+                                      double& w0, double& t0, double& w1, double& t1) {
+  w0 = t0 = w1 = t1 = 0.0;
+  const double scale = 2.0 * (var_u + var_v) + u * u + v * v;
+  if (scale <= 0.0) return;
+  const double s0 = 1.0 / sqrt(scale);
+  double inverse = 0.0, radial = 0.0;
+  for (int k = 0; k < n; ++k) {
+    const double t = s0 * tangent[k];
+    const double a = 1.0 + 2.0 * t * t * var_u, b = 1.0 + 2.0 * t * t * var_v;
+    const double mass = wsec2[k] * exp(-t * t * (u * u / a + v * v / b)) / sqrt(a * b);
+    inverse += mass;
+    radial += mass * (var_u / a + var_v / b + u * u / (a * a) + v * v / (b * b));
+  }
+  const double multiplier = 2.0 / sqrt(kPi) * s0;
+  inverse *= multiplier;
+  radial *= multiplier;
+  if (inverse <= 0.0) return;
+  const double mean = 1.0 / inverse, second = radial / inverse;
+  const double variance = second - mean * mean;
+  if (variance <= 0.0) {
+    w0 = inverse; t0 = mean; t1 = mean;
+    return;
+  }
+  const double third = (u * u + v * v + var_u + var_v) / inverse;
+  const double other = (third - 2.0 * mean * second + mean * mean * mean) / variance;
+  const double disc = sqrt((mean - other) * (mean - other) + 4.0 * variance);
+  const double low = 0.5 * (mean + other - disc), high = 0.5 * (mean + other + disc);
+  const double low_weight = inverse * (high - mean) / (high - low);
+  w0 = low_weight; t0 = low; w1 = inverse - low_weight; t1 = high;
+}
+
 struct O1GroupShared {
   double tangent[kO1MaxGauss], wsec2[kO1MaxGauss];
   double coef[kO1MaxMono];
@@ -439,13 +564,22 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
                  dz = rz - Pn.position[3 * p + 2];
     const double r = sqrt(dx * dx + dy * dy + dz * dz);
     const double hx = dx / r, hy = dy / r, hz = dz / r;
-    const double t_emit = Pn.time[p] - origins[d];
-    const double tau = t_emit + r / C.speed_ref;
+    // the screen's charge batches ignore emission time (_prompt_screen.py:220-229)
+    const double t_emit = C.screen ? 0.0 : Pn.time[p] - origins[d];
+    const double tau = C.screen ? 0.0 : t_emit + r / C.speed_ref;
     const double log_r = log(r);
     const long long key0 = (long long)floor(log_r / C.log_r_step) + (1ll << 20);
     const long long key1 =
         min(max((long long)floor(tau / C.tau_step) + (1ll << 20), 0ll), (1ll << 21) - 1);
-    const long long base = ((key1 << 21) + key0) * 2 * theta_bins;
+    const long long base = C.screen ? key0 * 2 * theta_bins : ((key1 << 21) + key0) * 2 * theta_bins;
+    if (C.screen && live) {  // a parent unless the OM looks into it, else its children
+      const int parent = Pn.parent[p];
+      // rows of a table whose stage A overflowed are not written (the caller
+      // redoes it): an index outside the table is never followed
+      if (parent >= n_pencils || parent < -1) live = false;
+      else live = parent < 0 ? !o1_refined(C, Pn, p, rx, ry, rz)
+                             : o1_refined(C, Pn, parent, rx, ry, rz);
+    }
     // _pencil_frame_from_ray_cached_look (_prompt_numba.py:594-606)
     const double sx = Pn.direction[3 * p], sy = Pn.direction[3 * p + 1], sz = Pn.direction[3 * p + 2];
     const double c1 = sx * nx + sy * ny + sz * nz;
@@ -455,7 +589,7 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
     const double c3 = sine > 1e-300 ? (qx * nx + qy * ny + qz * nz) / sine : 0.0;
     double theta = atan2(sine, cosine);
     const bool backward = theta > 0.5 * kPi;
-    double weight;
+    double weight, weight2 = 0.0, theta2 = theta;
     bool averaged = false;
     const double ax = Pn.major[3 * p], ay = Pn.major[3 * p + 1], az = Pn.major[3 * p + 2];
     const double* cov = Pn.pos_cov + 6 * p;
@@ -497,7 +631,35 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
         }
         const double u_ = hx * ax + hy * ay + hz * az, v_ = hx * bx + hy * by + hz * bz;
         double factor;
-        if (!far && extent > 0.0 && theta < sf * extent) {
+        bool done = false;
+        if (C.screen) {
+          // pencil_radial_rule (_prompt_screen.py:143-169): two radial nodes where the
+          // OM lies within the pencil's angular smoothing extent
+          const double half_tr = 0.5 * (m11 + m22);
+          const double disc = sqrt(fmax(0.25 * (m11 - m22) * (m11 - m22) + m12 * m12, 0.0));
+          const double r_mu1 = half_tr + disc;
+          const double r_mu2 = fmax(half_tr - disc, 1e-16 * r_mu1 + 1e-300);
+          const double r_extent = sqrt(fmax(r_mu1, 0.0));
+          if (r_extent > 0.0 && theta < sf * r_extent) {
+            const double st = sine > 0.0 ? theta / sine : 1.0;
+            const double uu = u_ * st, vv = v_ * st;
+            double sa, ca;
+            sincos(0.5 * atan2(2.0 * m12, m11 - m22), &sa, &ca);
+            double w0r, t0r, w1r, t1r;
+            o1_inverse_radius_rule(ca * uu + sa * vv, -sa * uu + ca * vv, r_mu1, r_mu2, S.tangent,
+                                   S.wsec2, C.n_gauss, w0r, t0r, w1r, t1r);
+            if (t0r > 0.0 && t1r < 0.5 * kPi && w0r > 0.0 && w1r >= 0.0) {
+              averaged = theta < r_extent;
+              factor = w0r * t0r / sin(t0r);
+              weight2 = (w1r * t1r / sin(t1r)) / r;
+              theta = t0r;
+              theta2 = t1r;
+              done = true;
+            }
+          }
+        }
+        if (done) {
+        } else if (!far && extent > 0.0 && theta < sf * extent) {
           double sa, ca;
           sincos(0.5 * atan2(2.0 * m12, m11 - m22), &sa, &ca);
           const double mean = o1_gauss_inverse_mean(ca * u_ + sa * v_, -sa * u_ + ca * v_, mu1,
@@ -518,29 +680,7 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
         weight = factor / r;
       }
     }
-    // theta index (scalar_theta_index, _prompt_numba.py:1628-1631)
-    int i_theta;
-    if (!(theta >= C.theta_lo)) i_theta = 0;
-    else i_theta = min(1 + (int)(log(theta / C.theta_lo) / log_theta_ratio), theta_bins - 1);
-    const long long key = base + (backward ? theta_bins : 0) + i_theta;
-    // lanes with the same (OM, group key) sum their moments in registers; the
-    // group's lowest lane inserts the key and adds the sums
-    const unsigned group = __match_any_sync(0xffffffffu, live ? key : -1ll) &
-                           __match_any_sync(0xffffffffu, live ? w : -1);
-    const bool leader = live && lane == __ffs(group) - 1;
-    double* row = nullptr;
-    if (leader) {
-      bool fresh;
-      long long* keys = gkeys + (int64_t)w * cap;
-      const int64_t slot = o1_insert(keys, cap, key, fresh);
-      if (slot < 0) {
-        atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
-      } else {
-        if (fresh) atomicAdd(gcount + w, 1);
-        row = grows + ((int64_t)w * cap + slot) * kO1MaxValues;
-      }
-    }
-    // _fill_moments_averaged_pair (_prompt_numba.py:1260-1277)
+    // _fill_moments_averaged_pair (_prompt_numba.py:1260-1277): the angular powers
     double cpw[5], spw[5];
     cpw[0] = 1.0;
     spw[0] = 1.0;
@@ -550,24 +690,54 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
       if (averaged) spw[q] = (q & 1) ? 0.0 : spw[q - 2] * perp2 * (q - 1.0) / q;
       else spw[q] = spw[q - 1] * c3;
     }
-    const double weight0 = weight * Pn.w0[p], weight2 = weight * Pn.w2[p];
     const int nm = C.n_mono;
-    double omega = 0.0;
-    double* mine = stage + lane * n_values;
-    for (int m = 0; m < nm; ++m) {
-      const double basis = cpw[S.ipow[m]] * spw[S.jpow[m]];
-      const double v0 = weight0 * basis;
-      if (m == 0) omega = fabs(v0);
-      mine[m] = v0;
-      mine[nm + m] = weight2 * basis;
+    // one group entry per radial node: the screen's two-node rule adds a second
+    // (_prompt_screen.py:281-336); every lane of the warp takes both rounds
+    const int nodes = C.screen ? 2 : 1;
+    for (int node = 0; node < nodes; ++node) {
+      const bool live_n = live && (node == 0 || weight2 > 0.0);
+      const double wn = node == 0 ? weight : weight2;
+      const double th = node == 0 ? theta : theta2;
+      // theta index (scalar_theta_index, _prompt_numba.py:1628-1631)
+      int i_theta;
+      if (!(th >= C.theta_lo)) i_theta = 0;
+      else i_theta = min(1 + (int)(log(th / C.theta_lo) / log_theta_ratio), theta_bins - 1);
+      const long long key = base + (backward ? theta_bins : 0) + i_theta;
+      // lanes with the same (OM, group key) sum their moments in registers; the
+      // group's lowest lane inserts the key and adds the sums
+      const unsigned group = __match_any_sync(0xffffffffu, live_n ? key : -1ll) &
+                             __match_any_sync(0xffffffffu, live_n ? w : -1);
+      const bool leader = live_n && lane == __ffs(group) - 1;
+      double* row = nullptr;
+      if (leader) {
+        bool fresh;
+        long long* keys = gkeys + (int64_t)w * cap;
+        const int64_t slot = o1_insert(keys, cap, key, fresh);
+        if (slot < 0) {
+          atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
+        } else {
+          if (fresh) atomicAdd(gcount + w, 1);
+          row = grows + ((int64_t)w * cap + slot) * kO1MaxValues;
+        }
+      }
+      const double field0 = wn * Pn.w0[p], field2 = wn * Pn.w2[p];
+      double omega = 0.0;
+      double* mine = stage + lane * n_values;
+      for (int m = 0; m < nm; ++m) {
+        const double basis = cpw[S.ipow[m]] * spw[S.jpow[m]];
+        const double v0 = field0 * basis;
+        if (m == 0) omega = fabs(v0);
+        mine[m] = v0;
+        mine[nm + m] = field2 * basis;
+      }
+      mine[2 * nm] = omega;
+      mine[2 * nm + 1] = omega * th;
+      mine[2 * nm + 2] = omega * r;
+      mine[2 * nm + 3] = omega * t_emit;
+      mine[2 * nm + 4] = omega * tau;
+      mine[2 * nm + 5] = omega * tau * tau;
+      o1_warp_group_add(stage, n_values, group, leader, row);
     }
-    mine[2 * nm] = omega;
-    mine[2 * nm + 1] = omega * theta;
-    mine[2 * nm + 2] = omega * r;
-    mine[2 * nm + 3] = omega * t_emit;
-    mine[2 * nm + 4] = omega * tau;
-    mine[2 * nm + 5] = omega * tau * tau;
-    o1_warp_group_add(stage, n_values, group, leader, row);
   }
 }
 
@@ -850,7 +1020,9 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
         }
         // _batch_grid (_prompt_numba.py:258-286): node counts
         const double ext_end = C.tail_exponent / mut_min;
-        double ext_win = speed_max * (C.edges[nb] - t_b) - r_b;
+        // the screen's grids run to the tail without a window edge
+        // (_prompt_screen.py:413: edge_end = inf)
+        double ext_win = C.screen ? ext_end : speed_max * (C.edges[nb] - t_b) - r_b;
         ext_win = fmin(fmax(ext_win, 0.0), ext_end);
         const double u_end = asinh(ext_end / sigma), u_win = asinh(ext_win / sigma);
         if (!(u_win >= 0.0) || !(u_end >= u_win) || !(u_end < 1e6)) {
@@ -1142,6 +1314,10 @@ struct O1Workspace {
   double* prows;
   int32_t* pcount;
   int32_t* tiles;
+  long long* parent_keys;  // screen tables: parent pixels (same capacity as pkeys)
+  double* parent_rows;
+  int32_t* parent_tiles;
+  int32_t* parent_row;     // row of each parent slot in the pencil table
   long long* gkeys;
   double* grows;
   int32_t* gcount;
@@ -1170,6 +1346,11 @@ static O1Workspace o1_layout(const lh_order1_config& C, int64_t pencil_capacity,
   W.prows = reinterpret_cast<double*>(take(sizeof(double) * kO1Moments * ring_capacity));
   W.pcount = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 4));
   W.tiles = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (ring_capacity / kO1Tile + 1)));
+  const int64_t parent_cap = C.screen ? ring_capacity : 0;
+  W.parent_keys = reinterpret_cast<long long*>(take(sizeof(long long) * parent_cap));
+  W.parent_rows = reinterpret_cast<double*>(take(sizeof(double) * kO1Moments * parent_cap));
+  W.parent_tiles = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (parent_cap / kO1Tile + 1)));
+  W.parent_row = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * parent_cap));
   W.gkeys = reinterpret_cast<long long*>(take(sizeof(long long) * (size_t)n_work * C.group_capacity));
   W.grows = reinterpret_cast<double*>(
       take(sizeof(double) * kO1MaxValues * (size_t)n_work * C.group_capacity));
@@ -1226,6 +1407,8 @@ bool o1_config_valid(const lh_order1_config* C) {
       !(C->tau_step > 0) || !(C->log_r_step > 0))
     return false;
   if (C->pixel_face < 1 || C->ring_nodes < 1 || !(C->cell_m > 0)) return false;
+  if (C->screen && (C->parent_face < 1 || C->pixel_face % C->parent_face || C->compute_bins))
+    return false;
   return true;
 }
 }  // namespace
@@ -1242,6 +1425,7 @@ extern "C" int lh_order1_pencils(const lh_order1_config* C, const lh_order1_elem
                                  void* workspace, size_t workspace_bytes, int32_t* status,
                                  void* stream) {
   if (!o1_config_valid(C) || !E || !P || !n_pencils_device || !status) return LH_EINVAL;
+  if (C->screen && !P->parent) return LH_EINVAL;
   if (E->n_el < 0 || E->n_subseg < 0 || (E->n_el && (!E->subseg_offset || !E->start ||
                                                      !E->direction || !E->length || !E->c0 ||
                                                      !E->c2 || !E->cone_cos || !E->t0 || !E->t1)))
@@ -1256,14 +1440,42 @@ extern "C" int lh_order1_pencils(const lh_order1_config* C, const lh_order1_elem
   cudaMemsetAsync(W.prows, 0, sizeof(double) * lh::kO1Moments * ring_cap, s);
   const int64_t ring_threads = ((E->n_subseg + 31) / 32) * 32 *
                                ((C->ring_nodes + lh::kO1RingBlock - 1) / lh::kO1RingBlock);
-  lh::o1_ring_kernel<<<lh::grid_for(ring_threads, lh::kO1RingThreads), lh::kO1RingThreads, 0, s>>>(
-      *C, *E, E->subseg_offset, E->n_subseg, W.pkeys, ring_cap, W.prows, status);
+  {
+    lh::TimedLaunch timed_launch(LH_KT_O1_RING, s);
+    lh::o1_ring_kernel<<<lh::grid_for(ring_threads, lh::kO1RingThreads), lh::kO1RingThreads, 0, s>>>(
+        *C, *E, E->subseg_offset, E->n_subseg, W.pkeys, ring_cap, W.prows, status);
+  }
   const int64_t n_tiles = (ring_cap + lh::kO1Tile - 1) / lh::kO1Tile;
-  lh::o1_tile_count_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(W.pkeys, W.prows,
-                                                                             ring_cap, W.tiles);
-  lh::o1_tile_scan_kernel<<<1, 1024, 0, s>>>(W.tiles, n_tiles, n_pencils_device);
+  if (!C->screen) {
+    lh::o1_tile_count_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(
+        W.pkeys, W.prows, ring_cap, W.tiles);
+    lh::o1_tile_scan_kernel<<<1, 1024, 0, s>>>(W.tiles, n_tiles, n_pencils_device);
+    lh::o1_finish_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(
+        W.pkeys, ring_cap, W.prows, *P, W.tiles, n_pencils_device, nullptr, nullptr, nullptr, 0,
+        nullptr, 0, 0, status);
+    return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+  }
+  // the coarse screen: parents (sums of their children) take rows [0, n_parents),
+  // children follow with their parent's row
+  cudaMemsetAsync(W.parent_keys, 0xff, sizeof(long long) * ring_cap, s);
+  cudaMemsetAsync(W.parent_rows, 0, sizeof(double) * lh::kO1Moments * ring_cap, s);
+  cudaMemsetAsync(W.parent_row, 0xff, sizeof(int32_t) * ring_cap, s);
+  lh::o1_parent_kernel<<<lh::grid_for(ring_cap, lh::kO1FinishThreads), lh::kO1FinishThreads, 0, s>>>(
+      W.pkeys, W.prows, ring_cap, C->pixel_face, C->parent_face, W.parent_keys, W.parent_rows,
+      ring_cap, status);
+  lh::o1_tile_count_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(
+      W.parent_keys, W.parent_rows, ring_cap, W.parent_tiles);
+  lh::o1_tile_scan_kernel<<<1, 1024, 0, s>>>(W.parent_tiles, n_tiles, W.pcount + 1);
   lh::o1_finish_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(
-      W.pkeys, ring_cap, W.prows, *P, W.tiles, n_pencils_device, status);
+      W.parent_keys, ring_cap, W.parent_rows, *P, W.parent_tiles, W.pcount + 1, nullptr,
+      W.parent_row, nullptr, 0, nullptr, 0, 0, status);
+  lh::o1_tile_count_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(
+      W.pkeys, W.prows, ring_cap, W.tiles);
+  lh::o1_tile_scan_kernel<<<1, 1024, 0, s>>>(W.tiles, n_tiles, W.pcount);
+  lh::o1_finish_kernel<<<(unsigned)n_tiles, lh::kO1FinishThreads, 0, s>>>(
+      W.pkeys, ring_cap, W.prows, *P, W.tiles, W.pcount, W.pcount + 1, nullptr, W.parent_keys,
+      ring_cap, W.parent_row, C->pixel_face, C->parent_face, status);
+  lh::o1_total_kernel<<<1, 32, 0, s>>>(W.pcount, W.pcount + 1, n_pencils_device);
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }
 
@@ -1274,6 +1486,7 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
                                  void* workspace, size_t workspace_bytes, int32_t* status,
                                  void* stream) {
   if (!o1_config_valid(C) || !P || n_pencils < 0 || n_work < 0 || !status || !charge) return LH_EINVAL;
+  if (C->screen && !P->parent) return LH_EINVAL;
   if (n_work && (!work || !origins)) return LH_EINVAL;
   if (C->compute_bins && !bins) return LH_EINVAL;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1295,9 +1508,12 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
       cudaFuncSetAttribute(lh::o1_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)group_smem) != cudaSuccess)
     return LH_ECUDA;
-  lh::o1_group_kernel<<<lh::grid_for((int64_t)n_work * n_pencils, 256), 256, group_smem, s>>>(
-      *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows, W.gcount,
-      status);
+  {
+    lh::TimedLaunch timed_launch(LH_KT_O1_GROUP, s);
+    lh::o1_group_kernel<<<lh::grid_for((int64_t)n_work * n_pencils, 256), 256, group_smem, s>>>(
+        *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows, W.gcount,
+        status);
+  }
   const size_t sort_smem =
       cap <= lh::kO1SmemSort ? sizeof(unsigned long long) * (size_t)cap : 0;
   if (sort_smem > 48 * 1024 &&
@@ -1311,8 +1527,11 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
   if (cudaFuncSetAttribute(lh::o1_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)batch_smem) != cudaSuccess)
     return LH_ECUDA;
-  lh::o1_batch_kernel<<<148 * 2, lh::kO1BatchThreads, batch_smem, s>>>(
-      *C, work, W.gkeys, W.grows, W.sorted, W.batch_list, W.batch_total, W.accum, status);
+  {
+    lh::TimedLaunch timed_launch(LH_KT_O1_BATCH, s);
+    lh::o1_batch_kernel<<<148 * 2, lh::kO1BatchThreads, batch_smem, s>>>(
+        *C, work, W.gkeys, W.grows, W.sorted, W.batch_list, W.batch_total, W.accum, status);
+  }
   const size_t fin_smem = sizeof(double) * C->n_bands * nb;
   if (fin_smem > 200 * 1024) return LH_EUNSUPPORTED;
   if (cudaFuncSetAttribute(lh::o1_finalize_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

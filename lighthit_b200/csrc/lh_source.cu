@@ -26,6 +26,7 @@
 #include <algorithm>
 
 #include "lh_common.cuh"
+#include "lh_timing.cuh"
 
 namespace lh {
 
@@ -558,14 +559,20 @@ extern "C" int lh_source_compile(const lh_source_problem* P, const lh_source_out
   if (cudaFuncSetAttribute(lh::src_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)gsmem) != cudaSuccess)
     return LH_ECUDA;
-  lh::src_group_kernel<<<148 * 4, lh::kSrcThreads, gsmem, s>>>(
-      *P, W.nodes, W.offsets, W.counts, W.order, W.groups, W.n_groups, W.deposit, W.zero);
+  {
+    lh::TimedLaunch timed_launch(LH_KT_SRC_GROUP, s);
+    lh::src_group_kernel<<<148 * 4, lh::kSrcThreads, gsmem, s>>>(
+        *P, W.nodes, W.offsets, W.counts, W.order, W.groups, W.n_groups, W.deposit, W.zero);
+  }
   lh::src_layout_kernel<<<1, 32, 0, s>>>(*P, W.slice_lo, W.slice_hi, W.zero, W.slice_point,
                                          W.slice_wide, W.centroid, W.n_occ, *O);
   const int w_block = std::max(1, std::min(lh::kSrcOmegaBlock, 1024 / P->nch));
   dim3 grid((unsigned)P->n_slices, (unsigned)NB, (unsigned)((P->n_omega + w_block - 1) / w_block));
   const int threads = ((P->nch * w_block + 31) / 32) * 32;
-  lh::src_transform_kernel<<<grid, threads, lh::kSrcStageBytes, s>>>(
-      *P, W.slice_lo, W.slice_hi, W.deposit, W.slice_point, W.slice_wide, W.n_occ, *O, w_block);
+  {
+    lh::TimedLaunch timed_launch(LH_KT_SRC_TRANSFORM, s);
+    lh::src_transform_kernel<<<grid, threads, lh::kSrcStageBytes, s>>>(
+        *P, W.slice_lo, W.slice_hi, W.deposit, W.slice_point, W.slice_wide, W.n_occ, *O, w_block);
+  }
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }

@@ -19,7 +19,8 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["Order0Optics", "DirectLight", "ElementBatch", "order0", "ELEMENT_FIELDS",
+__all__ = ["Order0Optics", "DirectLight", "ElementBatch", "ResidentElements", "order0",
+           "ELEMENT_FIELDS",
            "OPTICS_FIELDS"]
 
 ELEMENT_FIELDS = ("start_m", "direction", "length_m", "coefficient0", "coefficient2", "beta",
@@ -102,6 +103,19 @@ class Order0Optics:
                    kernel.acceptance()["alpha"], **kw)
 
 
+class ResidentElements(dict):
+    """One source's element arrays on the host (which the route's host logic
+    reads: delay groups, frames, selection) and already in device memory (which
+    its kernels read), uploaded once when the source is created."""
+
+    def __init__(self, elements, device):
+        import torch
+        super().__init__((k, np.ascontiguousarray(_field(elements, k), float))
+                         for k in ELEMENT_FIELDS)
+        self.device_arrays = {k: torch.tensor(v, dtype=torch.float64, device=device)
+                              for k, v in self.items()}
+
+
 class ElementBatch:
     """Elements of several events, concatenated on the device in one upload.
 
@@ -120,8 +134,14 @@ class ElementBatch:
         offsets[1:] = np.cumsum(counts)
         self.offsets = offsets
         self.n_elements = n = int(offsets[-1])
-        parts = [_field(e, name) for name in ELEMENT_FIELDS for e in events]
-        flat, _ = _lib.upload_parts(parts + [offsets], torch.float64, device)
+        if events and all(isinstance(e, ResidentElements) for e in events):
+            # already on the device: one concatenation there, only the offsets travel
+            flat = torch.cat([e.device_arrays[name].reshape(-1) for name in ELEMENT_FIELDS
+                              for e in events]
+                             + [_lib.upload(offsets.astype(float), torch.float64, device)])
+        else:
+            parts = [_field(e, name) for name in ELEMENT_FIELDS for e in events]
+            flat, _ = _lib.upload_parts(parts + [offsets], torch.float64, device)
         self._t = {}
         pos = 0
         for name in ELEMENT_FIELDS:

@@ -39,6 +39,8 @@ class PromptSettings:
     merge_theta_ratio: float = 0.08
     merge_tau_ns: float = 0.5
     merge_log_r: float = 0.02
+    screen: bool = False      # the coarse charge screen (compress_screen / screen_order1)
+    parent_face: int = 0      # the screen's parent pixels per face edge
 
     @classmethod
     def of(cls, config, *, fused=True):
@@ -54,13 +56,15 @@ class PromptSettings:
                    merge_theta_ratio=config.merge_theta_ratio,
                    merge_tau_ns=config.merge_tau_ns, merge_log_r=config.merge_log_r)
 
-    def screen(self):
-        """The coarse charge screen's pencils and merge (``prompt.py:1155-1160``,
-        ``_prompt_screen.compress_screen``: 2 m cells, 8-pixel faces, 24 ring
-        nodes; merge ratio 0.3 and 2 ns)."""
+    def coarse(self):
+        """The coarse charge screen (``prompt.py:1155-1160``, ``compress_screen``
+        and ``screen_order1``, ``_prompt_screen.py:91-503``): 2 m cells, 24 ring
+        nodes, 32-pixel faces under 8-pixel parents refined near each OM, merge
+        ratio 0.3 and 2 ns, one path step inside and beyond the window."""
         from dataclasses import replace
-        return replace(self, cell_m=2.0, pixel_face=8, ring_nodes=24, merge_theta_ratio=0.3,
-                       merge_tau_ns=2.0)
+        return replace(self, cell_m=2.0, pixel_face=32, ring_nodes=24, merge_theta_ratio=0.3,
+                       merge_tau_ns=2.0, path_step_tail=self.path_step, screen=True,
+                       parent_face=8)
 
 
 def _ifuncs(z):
@@ -149,7 +153,8 @@ class Order1Tables:
             float(s.tail_exponent), int(s.direct_bins), int(s.max_path_nodes),
             float(s.smoothing_factor), float(s.merge_theta_min), float(s.merge_theta_ratio),
             float(s.merge_tau_ns), float(s.merge_log_r), self.theta_bins, float(np.max(speed)),
-            GAUSS_NODES, t["gauss_tau"].data_ptr(), t["gauss_w"].data_ptr(), int(group_capacity))
+            GAUSS_NODES, t["gauss_tau"].data_ptr(), t["gauss_w"].data_ptr(), int(group_capacity),
+            int(bool(s.screen)), int(s.parent_face))
         self.compute_bins = bool(compute_bins)
         self._workspace = None
 
@@ -174,7 +179,8 @@ class Order1Tables:
         if getattr(self, "_pencil_pool", None) is None or self._pencil_pool.numel() < need:
             self._pencil_pool = torch.empty(max(need, 1 << 22), dtype=torch.float64,
                                             device=self.device)
-        table = PencilTable(capacity, self.device, self._pencil_pool[:need])
+        table = PencilTable(capacity, self.device, self._pencil_pool[:need],
+                            screen=self.settings.screen)
         table.pooled = True
         return table
 
@@ -195,7 +201,7 @@ class PencilTable:
               ("major", 3), ("var_major", 1), ("var_minor", 1), ("pos_cov", 6))
     ROW = sum(c for _, c in FIELDS)
 
-    def __init__(self, capacity, device, buffer=None):
+    def __init__(self, capacity, device, buffer=None, *, screen=False):
         import torch
         self.capacity = int(capacity)
         if buffer is None:
@@ -209,8 +215,12 @@ class PencilTable:
             pos += self.capacity * c
         self._buffer = buffer
         self.count = torch.zeros(1, dtype=torch.int32, device=device)
+        # the screen's parent row of every child (-1 for parents)
+        self.parent = (torch.empty(self.capacity, dtype=torch.int32, device=device) if screen
+                       else None)
         self.struct = _lib.Order1PencilTable(self.capacity,
-                                             *[self.t[k].data_ptr() for k, _ in self.FIELDS])
+                                             *[self.t[k].data_ptr() for k, _ in self.FIELDS],
+                                             self.parent.data_ptr() if screen else None)
 
     def host(self, n=None):
         n = int(self.count.item()) if n is None else n
@@ -298,8 +308,11 @@ def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=Non
     nodes = max(n_sub * s.ring_nodes, 1)
     # Pencils are distinct (cell, pixel) keys: far fewer than ring nodes when many
     # elements share cells. A table that overflows is redone at the full bound.
+    if s.screen:  # parents and children
+        nodes *= 2
     capacity = nodes if capacity_full else min(nodes, max(1 << 17, nodes // 4))
-    table = PencilTable(capacity, dev) if capacity_full else tables.pencil_table(capacity)
+    table = (PencilTable(capacity, dev, screen=s.screen) if capacity_full
+             else tables.pencil_table(capacity))
     ws = tables.workspace(n_sub, 0)
     st = status if status is not None else torch.zeros(1, dtype=torch.int32, device=dev)
     sp = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))

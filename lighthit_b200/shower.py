@@ -23,12 +23,12 @@ the reference's per-band order-1 units and per-band source lattices; receiver
 subsets (``receivers=``) run on ``ShowerTables.subset``. A table without its
 near-field file raises ``NotImplementedError`` when a shower needs the clamp.
 Order 1 follows the reference's global screen (``prompt.py:720-812``): a
-coarse charge pass (2 m cells, 8-pixel faces, 24 ring nodes) for every OM in
-reach, full resolution where ``q0 + extra + 3 q1_coarse`` reaches threshold,
-widened when the coarse pass underestimated. The coarse pass is the grouped
-evaluator on coarse pencils; the reference refines its coarse pixels near each
-OM (``_prompt_screen.py``), so coarse-only OMs (below threshold by
-construction) carry a different coarse order-1 charge.
+coarse charge pass for every OM in reach (``compress_screen``/``screen_order1``,
+``_prompt_screen.py``: 2 m cells, 24 ring nodes, 8-pixel parent faces refined
+to 32-pixel children near each OM, a two-node radial rule, charge batches
+without emission time), full resolution where ``q0 + extra + 3 q1_coarse``
+reaches threshold, widened when the coarse pass underestimated. Coarse-only
+OMs keep the coarse charge, as in the reference.
 """
 from __future__ import annotations
 
@@ -42,7 +42,8 @@ import numpy as np
 
 from . import _lib
 from .ge2 import AxialSources, Ge2Table
-from .order0 import ElementBatch, Order0Optics, order0, raise_status as raise_order0_status
+from .order0 import (ElementBatch, Order0Optics, ResidentElements, order0,
+                     raise_status as raise_order0_status)
 from .near import NearTable, add_near_field
 from .order1 import (Order1Tables, PromptSettings, acceptance_monomials, element_box, grouped,
                      grouped_widening, pencils)
@@ -185,7 +186,7 @@ class ShowerTables:
                                    settings=PromptSettings(), device=dev)
         self.order1_screen = Order1Tables(self.prompt, self.g, acceptance_monomials(self.alpha),
                                           self.positions, self.looks, self.areas, self.edges,
-                                          settings=PromptSettings().screen(), compute_bins=False,
+                                          settings=PromptSettings().coarse(), compute_bins=False,
                                           device=dev)
         self._order1_bands = {}
         self._pos = torch.tensor(self.positions, dtype=torch.float64, device=dev)
@@ -258,7 +259,7 @@ class ShowerTables:
             self._order1_bands[key] = Order1Tables(
                 {k: v[band:band + 1] for k, v in self.prompt.items()}, self.g,
                 acceptance_monomials(self.alpha), self.positions, self.looks, self.areas,
-                self.edges, settings=settings.screen() if coarse else settings,
+                self.edges, settings=settings.coarse() if coarse else settings,
                 compute_bins=not coarse, device=self.device)
         return self._order1_bands[key]
 
@@ -373,6 +374,8 @@ def delay_groups(el, *, prompt_delay_ns, cell_ns, window_end_ns, group_index_max
 def elements_of(source):
     """Element arrays of a shower source (reference objects or dicts with its names)."""
     el = getattr(source, "elements", source)
+    if isinstance(el, ResidentElements):  # host arrays plus their device copies
+        return el
     if isinstance(el, dict):
         out = {k: np.asarray(el[k], float) for k in ELEMENT_FIELDS}
         cone = el.get("cone_model", "spectral")

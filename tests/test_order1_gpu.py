@@ -112,3 +112,34 @@ def test_work_subset_leaves_other_oms_zero():
     rest = np.setdiff1d(np.arange(tables.n_om), work)
     assert np.all(q[rest] == 0) and np.all(b[rest] == 0)
     check(q[work], b[work], g["sub_charge"][work], g["sub_bins"][work])
+
+
+def test_screen_pack_matches_oracle():
+    """The coarse screen's stage A on the device: parents (8-pixel faces) and
+    children (32-pixel faces) equal the oracle's pack (compress_screen,
+    _prompt_screen.py:56-98), each child pointing at its own parent."""
+    from lighthit_b200.order1 import Order1Tables, PromptSettings, pencils
+    from oracle import order1 as O1
+    g = np.load(GOLDEN / "order1_c0.npz")
+    el = {k: g[k] for k in ("start_m", "direction", "length_m", "coefficient0", "coefficient2",
+                            "beta", "start_ns", "end_ns")}
+    tables = Order1Tables({k: g[k] for k in ("mus", "mut", "speed", "s0w", "s2w")},
+                          float(g["g"]), (g["coef"], g["ipow"], g["jpow"], int(g["degree"])),
+                          g["positions_m"], g["looks"], g["areas_m2"], g["edges_ns"],
+                          settings=PromptSettings().coarse(), compute_bins=False)
+    table = pencils(tables, el, g["cone_cos"])
+    n = int(table.count.item())
+    dev = {k: v[:n].cpu().numpy() for k, v in table.t.items()}
+    parent = table.parent[:n].cpu().numpy()
+    ref = O1.screen_pencils(el, g["cone_cos"])
+    roots = parent < 0
+    assert n == len(ref["w0"]) and roots.sum() == (ref["hierarchy_parent"] == -2).sum()
+    for mask_dev, mask_ref in ((roots, ref["hierarchy_parent"] == -2),
+                               (~roots, ref["hierarchy_parent"] >= 0)):
+        a = np.sort(dev["w0"][mask_dev])
+        b = np.sort(ref["w0"][mask_ref])
+        assert np.abs(a - b).max() <= 1e-12 * b.max()
+    # every child's parent carries its weight: parents equal their children's sums
+    sums = np.bincount(parent[~roots], weights=dev["w0"][~roots], minlength=n)
+    assert np.allclose(sums[roots], dev["w0"][roots], rtol=1e-12, atol=0)
+    assert np.all(roots[parent[~roots]])

@@ -91,3 +91,20 @@ def test_bins_per_order(routed):
         for order in range(3):
             l1 = np.abs(got[:, :, order] - ref[:, :, order]).sum(axis=1) / charge
             assert l1.max() <= BINS_L1, (k, order, l1.max())
+
+
+def test_coarse_only_order1_charge(routed):
+    """OMs the coarse screen left below threshold keep the screen's charge
+    (compress_screen / screen_order1: parents refined near the OM, the two-node
+    radial rule): equal to the reference's coarse charge."""
+    responses, g, _ = routed
+    seen = 0
+    for k, r in enumerate(responses):
+        level = np.asarray(r.metadata["prompt_order1_level"])
+        coarse = level == 1
+        ref = g[f"s{k}_charge"][coarse, 1]
+        got = r.charge_components_pe[coarse, 1]
+        scale = np.maximum(np.abs(ref), 1e-12)
+        assert (np.abs(got - ref) / scale).max(initial=0.0) <= ORDER1, k
+        seen += int(coarse.sum())
+    assert seen > 100
