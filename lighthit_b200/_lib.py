@@ -286,6 +286,21 @@ def upload_parts(parts, dtype, device):
     return host.to(device, non_blocking=True), offsets
 
 
+def fetch(tensors):
+    """Device tensors -> host NumPy arrays with one wait: each is copied into
+    pinned memory asynchronously on the current stream, then the stream is
+    synchronised once (instead of one blocking read per tensor)."""
+    import torch
+    hosts = []
+    for t in tensors:
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t, non_blocking=True)
+        hosts.append(h)
+    if hosts:
+        torch.cuda.current_stream(tensors[0].device).synchronize()
+    return [h.numpy() for h in hosts]
+
+
 def stream_ptr(stream):
     return C.c_void_p(stream.cuda_stream) if stream is not None else None
 

@@ -227,8 +227,9 @@ class ShowerTables:
         kw.setdefault("near", near if near.exists() else None)
         return cls(TABLES / f"route_{name}.npz", TABLES / folded[name], **kw)
 
-    def om_geometry_batch(self, prompt_store, store, group_index):
-        """Per shower: distances to the prompt elements and earliest arrivals (device)."""
+    def om_geometry_batch(self, prompt_store, store, group_index, *, host=True):
+        """Per shower: distances to the prompt elements and earliest arrivals
+        (host arrays, or the device tensors with ``host=False``)."""
         import torch
         dev = self.device
         n = self.n_om
@@ -244,7 +245,7 @@ class ShowerTables:
             sp = _lib.stream_ptr(torch.cuda.current_stream(dev))
             _lib.check(_lib.load().lh_om_geometry(C.byref(g), sp), "lh_om_geometry")
             out.append(res)
-        return out[0].cpu().numpy(), out[1].cpu().numpy()
+        return tuple(_lib.fetch(out)) if host else tuple(out)
 
     def order1_band(self, band, *, coarse=False):
         """Order-1 tables of one wavelength band for the per-band units (elements
@@ -621,15 +622,14 @@ class ShowerTransport:
                     compiled.append(lane.source.compile(
                         ev.src_el, ev.frame, status=src_status,
                         device_elements=store.event(k) if ev.src_el is ev.el else None))
-        npts_all = torch.stack([c[2] for c in compiled]).cpu().numpy()
-        if int(src_status.item()) & _lib.LH_STATUS_OVERFLOW:
+        # one read of every shower's point counts, points and zero-frequency
+        # channels (full capacity; sliced here) and the overflow flag
+        host = _lib.fetch([src_status] + [t for c in compiled
+                                          for t in (c[2], c[0], c[1][:, :, :, 0])])
+        if int(host[0][0]) & _lib.LH_STATUS_OVERFLOW:
             raise ValueError("element nodes fall outside the source lattice")
-        flat_pts = torch.cat([c[0].reshape(-1) for c in compiled]).cpu().numpy()
-        host_pts, at = [], 0
-        for c in compiled:
-            host_pts.append(flat_pts[at:at + c[0].numel()].reshape(c[0].shape))
-            at += c[0].numel()
-        for ev, c, pts, npts in zip(events, compiled, host_pts, npts_all):
+        for k, (ev, c) in enumerate(zip(events, compiled)):
+            npts, pts, zero = host[1 + 3 * k], host[2 + 3 * k], host[3 + 3 * k]
             _, ch_d, _, ev.reference, ev.frame = c
             ev.npts = npts
             centre, axis, e1, e2 = (np.asarray(v, float) for v in ev.frame)
@@ -638,15 +638,7 @@ class ShowerTransport:
                          + p[:npts[b], 2:3] * e2 for b, p in enumerate(pts)]
             ev.channels = (ch_d[:, :int(npts[0])] if np.all(npts == npts[0])
                            else [ch_d[b, :int(npts[b])] for b in range(nb_bands)])
-            ev.zero_ch = [ch_d[b, :int(npts[b]), :, 0] for b in range(nb_bands)]
-        zero_host = torch.cat([z for ev in events for z in ev.zero_ch]).cpu().numpy()
-        pos = 0
-        for ev in events:
-            parts = []
-            for b in range(nb_bands):
-                parts.append(zero_host[pos:pos + int(ev.npts[b])])
-                pos += int(ev.npts[b])
-            ev.zero_ch = parts
+            ev.zero_ch = [zero[b, :int(npts[b])] for b in range(nb_bands)]
         for ev in events:  # delayed parts: their own frames and lattices (rare)
             if ev.late is None:
                 continue
@@ -753,12 +745,15 @@ class ShowerTransport:
             ev.prompt_box = ev.box if pel is el else element_box(pel)
         same = all(ev.prompt_el is ev.el for ev in events)
         prompt_store = store if same else ElementBatch([ev.prompt_el for ev in events], dev)
-        dist, early = T.om_geometry_batch(prompt_store, store, fastest)
+        dist_d, early_d = T.om_geometry_batch(prompt_store, store, fastest, host=False)
+        pred = [ev for ev in events if "predicted" in ev.pending]
+        host = _lib.fetch([dist_d, early_d] + [ev.pending.pop("predicted")[:, 0] for ev in pred])
+        dist, early = host[0], host[1]
+        for ev, values in zip(pred, host[2:]):
+            ev.predicted[ev.reach] = values.real
         for k, ev in enumerate(events):
             if ev.origins is None:
                 ev.origins = early[k]
-            if "predicted" in ev.pending:
-                ev.predicted[ev.reach] = ev.pending.pop("predicted").cpu().numpy()[:, 0].real
         # delayed light is small and compact: its zero-frequency charge exactly on
         # every reachable OM (shower/api.py:345-352)
         late_req = [ev for ev in events if ev.late is not None and len(ev.reach)]
@@ -804,19 +799,20 @@ class ShowerTransport:
                           ElementBatch([ev.prompt_el for ev in prompt_events], dev))
                 out0 = order0(T.order0, batch0, origins, edges, check=False)
         if prompt_events:
-            raise_order0_status(int(out0["status"].item()))
-            q0_all = out0["charge"].cpu().numpy()
+            extra0 = [out0["status"], out0["charge"]]
+            coarse_host = self._collect(prompt_events, "coarse", T.order1_screen, extra0)
+            raise_order0_status(int(extra0[0][0]))
+            q0_all = extra0[1]
             bins0_all = out0["bins"]
             for k, ev in enumerate(prompt_events):
                 ev.charge[ev.work, 0] = q0_all[k][ev.work]
                 ev.pending["bins0"] = bins0_all[k]
-        self._redo_overflow(prompt_events, "coarse", T.order1_screen)
         stage("order0_screen")
         fine_events = []
         for ev in prompt_events:
             ev.fine = ev.work
-            if "coarse" in ev.pending:
-                coarse = ev.pending.pop("coarse").cpu().numpy()
+            if id(ev) in coarse_host:
+                coarse = coarse_host[id(ev)]
                 if ev.units:
                     coarse = coarse + self._units_charge(ev, ev.work, coarse=True)[0]
                 ev.charge[ev.work, 1] = coarse[ev.work]
@@ -841,12 +837,11 @@ class ShowerTransport:
                                        device_elements=ev.fused_dev, box=ev.fused_box)
                     ev.pending["fine"] = grouped(lane.order1, ev.table, ev.fine, ev.origins,
                                                  status=ev.status)
-        self._redo_overflow(prompt_events, "fine", T.order1)
+        fine_host = self._collect(prompt_events, "fine", T.order1)
         for ev in prompt_events:
-            if "fine" not in ev.pending:
+            if id(ev) not in fine_host:
                 continue
-            q1, b1 = ev.pending.pop("fine")
-            q1, b1 = q1.cpu().numpy(), b1.cpu().numpy()
+            q1, b1 = fine_host[id(ev)]
             if ev.units:
                 qu, bu = self._units_charge(ev, ev.fine)
                 q1, b1 = q1 + qu, b1 + bu
@@ -866,8 +861,6 @@ class ShowerTransport:
                         ev.charge[more, 1] = q1m[more]
                         ev.bins1[more] = b1m[more]
                         ev.level1[more] = 2
-        if int(status.item()) & _lib.LH_STATUS_OVERFLOW:
-            raise MemoryError("order-1 tables overflowed their device capacity")
         stage("order1")
         # ---- exact zero-frequency >=2 where the decision needs it (shower/api.py:488-525)
         exact_req = []
@@ -883,15 +876,20 @@ class ShowerTransport:
             ids = np.flatnonzero(cand)
             if len(ids):
                 exact_req.append((ev, ids))
-        for (ev, ids), res in zip(exact_req, self._apply_many(
-                [(ev.points, self._zero_only(ev.channels), ev.reference, ev.frame, ids)
-                 for ev, ids in exact_req], zero_frequency=True)):
-            ev.pending["exact"] = (ids, res)
+        exact_res = self._apply_many(
+            [(ev.points, self._zero_only(ev.channels), ev.reference, ev.frame, ids)
+             for ev, ids in exact_req], zero_frequency=True)
+        # one read: the order-1 status word and every exact charge
+        host = _lib.fetch([status] + [res[:, 0] for res in exact_res])
+        if int(host[0][0]) & _lib.LH_STATUS_OVERFLOW:
+            raise MemoryError("order-1 tables overflowed their device capacity")
+        for (ev, ids), values in zip(exact_req, host[1:]):
+            ev.pending["exact"] = (ids, values)
         for ev in events:
             exact = np.zeros(n)
             if "exact" in ev.pending:
                 ids, values = ev.pending.pop("exact")
-                exact[ids] = values.cpu().numpy()[:, 0].real
+                exact[ids] = values.real
             cand = ev.candidate
             ratio = np.abs(exact[cand]) / np.maximum(np.abs(ev.predicted[cand]), 1e-300)
             fallback = bool(np.any(np.abs(exact[cand]) > safety * np.abs(ev.predicted[cand])))
@@ -945,10 +943,17 @@ class ShowerTransport:
                                  torch.complex128, dev)
             rel = torch.cat(specs) * packed[:, :-1]
             rel[:, 0] = packed[:, -1]
-            for (k, work), spec in zip(row_ev, specs):
+            bins2_d, _ = T.readout.bins(rel.to(torch.complex64), mode=cfg.readout_mode)
+        # one read: the >=2 bins and spectra of the active OMs, the order-0 bins
+        with_bins0 = [k for k, ev in enumerate(events) if np.any(ev.active)]
+        host = _lib.fetch(([bins2_d] + list(specs) if row_ev else [])
+                          + [events[k].pending["bins0"] for k in with_bins0])
+        if row_ev:
+            bins2 = host[0].astype(float)
+            for (k, work), spec in zip(row_ev, host[1:1 + len(row_ev)]):
                 events[k].pending["spec"] = (work, spec)
-            bins2, _ = T.readout.bins(rel.to(torch.complex64), mode=cfg.readout_mode)
-            bins2 = bins2.cpu().numpy().astype(float)
+        for k, values in zip(with_bins0, host[(1 + len(row_ev)) if row_ev else 0:]):
+            events[k].pending["bins0"] = values
         late_bins = self._late_bins(events, row_ev, omega, cfg.readout_mode)
         responses = []
         row = 0
@@ -956,14 +961,14 @@ class ShowerTransport:
         for k, ev in enumerate(events):
             if "spec" in ev.pending:
                 work, spec = ev.pending.pop("spec")
-                ev.spectrum[:, work] = spec.cpu().numpy().T
+                ev.spectrum[:, work] = spec.T
             ev.spectrum[0] = ev.charge[:, 2] - ev.late_charge  # prompt steps (api.py:450)
             components = np.zeros((n, len(edges) - 1, 3))
             ids = np.flatnonzero(ev.active)
             if len(ids):
                 if not np.all(ev.inside[ids]):
                     raise ValueError("prompt did not compute every active OM")
-                components[ids, :, 0] = ev.pending["bins0"].cpu().numpy()[ids]
+                components[ids, :, 0] = ev.pending["bins0"][ids]
                 components[ids, :, 1] = ev.bins1[ids]
                 if k in row_map:
                     work = row_map[k]
@@ -1053,23 +1058,36 @@ class ShowerTransport:
             out.setdefault(k, []).append(values.cpu().numpy().astype(float))
         return out
 
-    def _redo_overflow(self, events, key, tables):
-        """Events whose bounded pencil table overflowed: stage A and B again at full size."""
-        import torch
+    def _collect(self, events, key, tables, extra=None):
+        """Host values of the events' pending ``key`` results (coarse charge, or
+        fine charge and bins) read in one wait with their status words and the
+        tensors of ``extra`` (replaced in place by their host arrays). Events
+        whose bounded pencil table overflowed run stage A and B again at full
+        size. Returns ``{id(event): host values}``."""
         pend = [ev for ev in events if key in ev.pending]
-        if not pend:
-            return
-        flags = torch.cat([ev.status for ev in pend]).cpu().numpy()
-        for ev, f in zip(pend, flags):
-            if not f & _lib.LH_STATUS_OVERFLOW:
-                continue
-            table = pencils(tables, ev.fused_el, ev.cone_cos, device_elements=ev.fused_dev,
-                            capacity_full=True, box=ev.fused_box)
-            work = ev.work if key == "coarse" else ev.fine
-            res = grouped_widening(tables, table, work, ev.origins)
-            ev.pending[key] = res[0] if key == "coarse" else res
-            if key == "fine":
-                ev.table = table
+        extra = [] if extra is None else extra
+        parts = list(extra) + [ev.status for ev in pend]
+        for ev in pend:
+            parts.extend([ev.pending[key]] if key == "coarse" else list(ev.pending[key]))
+        host = _lib.fetch(parts) if parts else []
+        extra[:] = host[:len(extra)]
+        flags = host[len(extra):len(extra) + len(pend)]
+        values = host[len(extra) + len(pend):]
+        out = {}
+        width = 1 if key == "coarse" else 2
+        for i, (ev, f) in enumerate(zip(pend, flags)):
+            got = values[width * i:width * (i + 1)]
+            ev.pending.pop(key)
+            if f[0] & _lib.LH_STATUS_OVERFLOW:
+                table = pencils(tables, ev.fused_el, ev.cone_cos, device_elements=ev.fused_dev,
+                                capacity_full=True, box=ev.fused_box)
+                work = ev.work if key == "coarse" else ev.fine
+                res = grouped_widening(tables, table, work, ev.origins)
+                got = _lib.fetch([res[0]] if key == "coarse" else list(res))
+                if key == "fine":
+                    ev.table = table
+            out[id(ev)] = got[0] if key == "coarse" else tuple(got)
+        return out
 
     def _order1_units(self, ev, cone):
         """Order-1 evaluation units (``prompt.py:683-719`` with

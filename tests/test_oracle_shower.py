@@ -144,3 +144,10 @@ def test_route_matches_reference_config2(k):
     comp[g[f"s{k}_active_ids"]] = g[f"s{k}_components"]
     check_route(out, g[f"s{k}_charge"], g[f"s{k}_active"], g[f"s{k}_origin"], comp,
                 float(route.threshold), charge_tol=1e-7, bins_tol=1e-5)
+    # OMs the coarse screen left below threshold keep the screen's charge
+    # (compress_screen / screen_order1 with the receiver-local refinement)
+    coarse = out["prompt_order1_level"] == 1
+    assert coarse.sum() > 100
+    ref = g[f"s{k}_charge"][coarse, 1]
+    got = out["charge_components_pe"][coarse, 1]
+    assert (np.abs(got - ref) / np.maximum(np.abs(ref), 1e-12)).max() <= 1e-10
