@@ -66,19 +66,42 @@ def common_time_origins(tables, sources):
 
 
 class EventTransport:
-    """``EventTransport(...)(components | IsotropicFlash)`` on the device routes.
+    """``EventTransport(kernel, *, muon_data=None, shower_data=None, laser_kernel=None,
+    threads=None, safety=3.0, max_rounds=4)(components | IsotropicFlash)`` on the
+    device routes (``event.py:94-296``).
 
-    ``shower_route``: a :class:`lighthit_b200.shower.ShowerTransport`;
-    ``flash``: a flash transport (:class:`lighthit_b200.flash.FlashTransport` or
-    :class:`~lighthit_b200.flash.BroadbandFlashTransport`) for calibration flashes.
+    ``kernel``: the device shower route (a :class:`lighthit_b200.shower.ShowerTransport`),
+    its tables (:class:`~lighthit_b200.shower.ShowerTables`), or the reference's
+    ``TransportKernel`` (the shower route is then built from ``shower_data`` as
+    the reference's ``shower_route`` does, ``event.py:124-129``).
+    ``laser_kernel``: a flash transport (:class:`lighthit_b200.flash.FlashTransport`
+    or :class:`~lighthit_b200.flash.BroadbandFlashTransport`) for calibration
+    flashes; ``flash`` is the same argument under its earlier name.
+    ``muon_data`` and ``threads`` are accepted for the reference's signature:
+    muon components raise ``NotImplementedError`` (the muon route is not on the
+    device) and the device routes take no thread count.
     """
 
-    def __init__(self, shower_route, *, flash=None, safety=3.0, max_rounds=4):
+    def __init__(self, kernel, *, muon_data=None, shower_data=None, laser_kernel=None,
+                 threads=None, safety=3.0, max_rounds=4, flash=None):
+        from .shower import ShowerTables, ShowerTransport
         if not np.isfinite(safety) or safety < 1 or int(max_rounds) < 1:
             raise ValueError("safety must be >= 1 and max_rounds positive")
-        self.shower = shower_route
-        self.flash_transport = flash
+        if isinstance(kernel, ShowerTransport):
+            self.shower = kernel
+        elif isinstance(kernel, ShowerTables):
+            self.shower = ShowerTransport(kernel)
+        else:
+            self.shower = ShowerTransport(kernel, shower_data, threads=threads)
+        self.kernel = kernel
+        self.muon_data, self.shower_data, self.threads = muon_data, shower_data, threads
+        self.flash_transport = laser_kernel if laser_kernel is not None else flash
         self.safety, self.max_rounds = float(safety), int(max_rounds)
+        self.route_fallbacks = {}
+
+    def shower_route(self):
+        """The device shower route (``event.py:124-129``)."""
+        return self.shower
 
     def _run(self, component, **options):
         if component.kind != "shower":
@@ -89,7 +112,7 @@ class EventTransport:
     def flash(self, flash):
         """A calibration flash, transported alone (``event.py:184-190``)."""
         if self.flash_transport is None:
-            raise ValueError("a calibration flash needs EventTransport(flash=...)")
+            raise ValueError("a calibration flash needs EventTransport(laser_kernel=...)")
         response = self.flash_transport.transport(flash)
         response.metadata["route"] = "lighthit_b200.flash (isotropic flash)"
         return response

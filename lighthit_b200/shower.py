@@ -33,6 +33,7 @@ OMs keep the coarse charge, as in the reference.
 from __future__ import annotations
 
 import ctypes as C
+import functools
 from contextlib import contextmanager
 from dataclasses import dataclass, field
 from pathlib import Path
@@ -213,6 +214,21 @@ class ShowerTables:
         view.receivers = ids
         view._om_tables()
         return view
+
+    @classmethod
+    def from_reference(cls, kernel, data=None, *, config=None, **kw):
+        """Tables of a reference ``TransportKernel`` and its prepared shower data
+        (``ShowerData``, a manifest path, or None to search next to the kernel's
+        cache), read through the reference's own ``ShowerTransport``
+        (``shower/api.py:124-174``): the folded order >=2 kernels, the
+        near-field interval and the route constants, uploaded once. Needs the
+        reference package; the device route reads nothing of it afterwards."""
+        from lighthit.shower import ShowerTransport as ReferenceRoute
+        from .tables.build_tables import folded_kernels, near_interval, route_constants
+        route = ReferenceRoute(kernel, data, config=config)
+        tables = route.tables()
+        return cls(route_constants(route, tables), folded_kernels(route, tables),
+                   near=near_interval(route, tables), **kw)
 
     @classmethod
     def synthetic(cls, name="c0", **kw):
@@ -452,20 +468,62 @@ class _Event:
     pending: dict = field(default_factory=dict)
 
 
-class ShowerTransport:
-    """``ShowerTransport(kernel, data)(source, ...)`` on the device route.
+def settings_of(config, base=None):
+    """``ShowerSettings`` from a reference ``ShowerConfig`` (``shower/api.py:47-90``:
+    the predictor, delayed-light and screen fields the route reads), or the
+    settings themselves."""
+    from dataclasses import replace
+    base = base or ShowerSettings()
+    if config is None or isinstance(config, ShowerSettings):
+        return config or base
+    return replace(base, predictor_cell_m=float(config.predictor_cell_m),
+                   predictor_safety=float(config.predictor_safety),
+                   prompt_delay_ns=float(config.prompt_delay_ns),
+                   delayed_cell_ns=float(config.delayed_cell_ns),
+                   screen=bool(config.prompt.screen),
+                   screen_margin=float(config.prompt.screen_margin),
+                   min_distance_m=float(config.prompt.min_distance_m))
 
-    ``batch(sources)`` runs many showers stage by stage: every stage launches
-    its kernels for all showers back to back on the current stream and the
-    host reads the device once per stage, not once per shower.
-    ``profile=True`` synchronises the device between stages so that
-    ``metadata['timings']`` attributes the GPU time to each stage.
+
+@functools.lru_cache(maxsize=1)
+def response_class():
+    """The reference's ``HybridTransportResponse`` when the reference package
+    is importable (so that ``isinstance`` checks against it hold), else the
+    local class with the same fields."""
+    try:
+        from lighthit.transport import HybridTransportResponse as Reference
+    except ImportError:
+        return HybridTransportResponse
+    return Reference
+
+
+class ShowerTransport:
+    """``ShowerTransport(kernel, data=None, *, config=None, threads=None)(source, ...)``
+    on the device route (``shower/api.py:114-318``).
+
+    ``kernel`` is ``ShowerTables`` (the route's device tables) or the
+    reference's ``TransportKernel``, whose prepared tables are then read once
+    through the reference (``ShowerTables.from_reference`` with ``data``).
+    ``config``: ``ShowerSettings`` or the reference's ``ShowerConfig``.
+    ``threads`` is accepted for the reference's signature; the device route
+    ignores it. ``batch(sources)`` runs many showers stage by stage: every stage
+    launches its kernels for all showers back to back and the host reads the
+    device once per stage, not once per shower. ``profile=True`` synchronises
+    the device between stages so that ``metadata['timings']`` attributes the
+    GPU time to each stage.
     """
 
-    def __init__(self, tables: ShowerTables, config: ShowerSettings | None = None, *,
-                 profile=False, lanes=4):
+    def __init__(self, kernel, data=None, *, config=None, threads=None, profile=False, lanes=4,
+                 device="cuda"):
+        if isinstance(kernel, ShowerTables):
+            tables = kernel
+        else:
+            tables = ShowerTables.from_reference(kernel, data, config=config, device=device,
+                                                 settings=settings_of(config))
+        self.kernel = None if isinstance(kernel, ShowerTables) else kernel
         self.tables = tables
-        self.config = config or tables.settings
+        self.config = settings_of(config, tables.settings)
+        self.threads = threads
         self.profile = profile
         self.n_lanes = max(1, int(lanes))
         self._lane_list = None
@@ -545,8 +603,8 @@ class ShowerTransport:
                 out[i] = res if out[i] is None else out[i] + res
         return out
 
-    def __call__(self, source, *, time_origin_ns=None, selection_extra_charge=None,
-                 receivers=None):
+    def __call__(self, source, *, progress=None, time_origin_ns=None,
+                 selection_extra_charge=None, receivers=None):
         if receivers is not None:  # shower/api.py:205-212: those OMs, threshold zero
             return self._subset_route(receivers)(source, time_origin_ns=time_origin_ns,
                                                  selection_extra_charge=selection_extra_charge)
@@ -563,7 +621,7 @@ class ShowerTransport:
         if key not in cache:
             if len(cache) >= 8:
                 cache.pop(next(iter(cache)))
-            cache[key] = ShowerTransport(self.tables.subset(key), self.config,
+            cache[key] = ShowerTransport(self.tables.subset(key), config=self.config,
                                          profile=self.profile, lanes=self.n_lanes)
         return cache[key]
 
@@ -1004,9 +1062,10 @@ class ShowerTransport:
                     "steps_beyond_window": 0 if ev.late is None else ev.late["beyond"],
                     "delayed_charge_pe": float(ev.late_charge.sum()),
                     "stored_spectrum": "prompt steps only (delayed light in charge and bins)"}}
-            response = HybridTransportResponse(None, omega.copy(), edges.copy(), ev.spectrum,
-                                               components, ev.charge, ev.origins, ev.active,
-                                               "shower", metadata)
+            response = response_class()(
+                None if self.kernel is None else self.kernel.detector, omega.copy(),
+                edges.copy(), ev.spectrum, components, ev.charge, ev.origins, ev.active,
+                "shower", metadata)
             if ev.near:  # shower/api.py:536-538
                 origins = _lib.upload(ev.origins, torch.float64, dev)
                 near = T.near.field(store.event(k), len(ev.el["beta"]), T._pos, T._looks,

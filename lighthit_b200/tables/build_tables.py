@@ -43,6 +43,7 @@ def _required(name, what):
         raise SystemExit(f"set {name} to {what}")
     return Path(value)
 
+
 BASE = dict(wavelength_nodes=3, degree=8, azimuthal_degree=2, readout_nodes=321,
             bin_ns=5.0, window_end_ns=740.0)
 CONFIGS = {
@@ -58,15 +59,15 @@ CONFIGS = {
 }
 
 
-def write_near(name, route, tables):
-    """The near-field table: interval 0 of every wavelength's order >=2 spline."""
+def near_interval(route, tables):
+    """The near-field table (a dict): interval 0 of every wavelength's order >=2
+    spline of a reference ``ShowerTransport`` (``Ge2KernelStore.bundle``)."""
     from lighthit.shower_basis import _frequency_indices
     indices = _frequency_indices(route.kernel, route.config.frequency_nodes)
     bundle = tables["store"].bundle(route.kernel, indices)
     if bundle.get("phase") != "flight":
-        raise SystemExit("near-field table needs flight-phase splines")
-    np.savez_compressed(
-        HERE / f"near_{name}.npz",
+        raise ValueError("near-field table needs flight-phase splines")
+    return dict(
         coefficients=np.ascontiguousarray(np.asarray(bundle["coefficients"])[:, 0], np.complex64),
         log_r=np.asarray(bundle["log_r"], float)[:2],
         radial_high_m=float(np.exp(np.asarray(bundle["log_r"], float)[-1])),
@@ -78,7 +79,77 @@ def write_near(name, route, tables):
         pair_mu=np.asarray(bundle["pair_mu"], np.int64),
         provenance=json.dumps({"built_by": "lighthit Ge2KernelStore.bundle (interval 0)",
                                "frequency_indices": np.asarray(indices).tolist()}))
-    print("wrote", f"near_{name}.npz", np.asarray(bundle["coefficients"]).shape)
+
+
+def folded_kernels(route, tables):
+    """The folded order >=2 kernels (a dict) of a reference ``ShowerTransport``
+    (``ShowerTransport.tables()``, ``band_fold.py:155-208``)."""
+    folded, fold = tables["folded"], tables["fold"]
+    cfg = route.kernel.config
+    lo, hi = (float(v) for v in cfg.radial_range_m)
+    return dict(
+        coefficients=np.asarray(folded["coefficients"], np.complex64),
+        log_r=np.asarray(folded["log_r"], float), omega=np.asarray(folded["omega"], float),
+        absorption=np.asarray(folded["absorption"], float), speed=np.asarray(folded["speed"], float),
+        degree=int(folded["degree"]), acceptance_degree=int(folded["acceptance_degree"]),
+        pair_lambda=np.asarray(folded["pair_lambda"], np.int64),
+        pair_mu=np.asarray(folded["pair_mu"], np.int64), phase=str(folded["phase"]),
+        bands=np.asarray(fold.bands, np.int64), scale=np.asarray(fold.scale, float),
+        provenance=json.dumps({"built_by": "lighthit ShowerTransport.tables() (BandFold rank "
+                                           f"{len(fold.bands)})",
+                               "kernel": {"radial_range_m": [lo, hi],
+                                          "radial_nodes": int(cfg.radial_nodes),
+                                          "k_panel_per_m": float(cfg.k_panel_per_m)}}))
+
+
+def route_constants(route, tables):
+    """The route's medium and detector constants (a dict) of a reference
+    ``ShowerTransport``: wavelength nodes and weights, phase/group indices,
+    absorption and scattering, detector spectral weights, the spectral-cut phase
+    index (``prompt.py:542-550``), the node bands, the prompt tables
+    (``prompt.py:412-434``), the first-entry optical panels of
+    ``prepare_optics(..., exact_response=True)``, the acceptance, OM geometry
+    and the kernel configuration."""
+    from lighthit.ballistic_interval import BallisticIntervalConfig, prepare_optics
+    from lighthit.prompt import _spectral_tables
+    k = route.kernel
+    fold = tables["fold"]
+    wl = np.asarray(k.wavelength.wavelength_nm, float)
+    sample = k.medium.sample(wl)
+    low, high = k.config.wavelength_range_nm or k.medium.wavelength_range_nm
+    native = k.medium.wavelength_nm
+    critical = np.r_[low, native[(native > low) & (native < high)], high]
+    prompt = _spectral_tables(k)
+    optics = prepare_optics(k, BallisticIntervalConfig(), exact_response=True)
+    d = k.detector
+    n_om = len(d)
+    return dict(
+        wavelength_nm=wl, weight_nm=np.asarray(k.wavelength.weight_nm, float),
+        phase_index=np.asarray(sample["phase_index"], float),
+        group_index=np.asarray(sample["group_index"], float),
+        absorption_per_m=np.asarray(sample["absorption_per_m"], float),
+        scattering_per_m=np.asarray(sample["scattering_per_m"], float),
+        efficiency=np.asarray(d.spectral_weight(wl), float),
+        threshold_phase=float(np.max(k.medium.sample(critical)["phase_index"])),
+        g=float(k.medium.g), fold_bands=np.asarray(fold.bands, np.int64),
+        fold_scale=np.asarray(fold.scale, float), fold_phase=np.asarray(fold.phase_index, float),
+        mus=prompt["mus"], mut=prompt["mut"], speed=prompt["speed"], s0w=prompt["s0w"],
+        s2w=prompt["s2w"], **{f"optics_{key}": optics[key] for key in (
+            "panel_edges", "phase_nodes", "group_nodes", "extinction_nodes",
+            "efficiency_coefficients")},
+        alpha=np.asarray(k.acceptance()["alpha"], float),
+        peak_acceptance=float(np.max(np.abs(np.asarray(
+            d.angular_acceptance(np.linspace(-1, 1, 257)), float)))),
+        positions_m=np.asarray(d.positions_m, float),
+        looks=np.asarray(-d.orientations, float),
+        areas_m2=np.broadcast_to(np.asarray(d.effective_area_m2, float), (n_om,)).copy(),
+        radii_m=np.broadcast_to(np.asarray(d.receiver_surface.radii(n_om), float), (n_om,)).copy(),
+        omega_per_ns=np.asarray(k.config.omega_per_ns, float),
+        readout_omega_per_ns=np.asarray(k.config.readout_omega_per_ns, float),
+        edges_ns=np.asarray(k.config.relative_time_edges_ns, float),
+        radial_range_m=np.asarray(k.config.radial_range_m, float),
+        threshold_pe=float(k.config.threshold_pe), source_degree=int(k.config.source_degree),
+        azimuthal_degree=int(k.config.azimuthal_degree))
 
 
 def main(name, near_only=False):
@@ -87,9 +158,7 @@ def main(name, near_only=False):
     os.environ.setdefault("NUMBA_CACHE_DIR", str(work / "numba-cache"))
     sys.path.insert(0, str(src))
     import lighthit as lh
-    from lighthit.ballistic_interval import BallisticIntervalConfig, prepare_optics
     from lighthit.examples.synthetic import baikal_like_detector, synthetic_medium_model
-    from lighthit.prompt import _spectral_tables
     from lighthit.shower import ShowerData, ShowerTransport
 
     c = CONFIGS[name]
@@ -117,62 +186,15 @@ def main(name, near_only=False):
         kernel.ge2_kernel_store().save(str(cache / "ge2-pack"))
     route = ShowerTransport(kernel, ShowerData.of(str(cache), str(cache / "ge2-pack")))
     tables = route.tables()
-    write_near(name, route, tables)
+    np.savez_compressed(HERE / f"near_{name}.npz", **near_interval(route, tables))
+    print("wrote", f"near_{name}.npz")
     if near_only:
         return
-    folded, fold = tables["folded"], tables["fold"]
-    k = route.kernel
     lo, hi = c["radial_range_m"]
-    n_om = len(detector)
-    np.savez_compressed(
-        HERE / f"ge2_fold_{n_om}om_{lo:g}-{hi:g}m.npz",
-        coefficients=np.asarray(folded["coefficients"], np.complex64),
-        log_r=np.asarray(folded["log_r"], float), omega=np.asarray(folded["omega"], float),
-        absorption=np.asarray(folded["absorption"], float), speed=np.asarray(folded["speed"], float),
-        degree=int(folded["degree"]), acceptance_degree=int(folded["acceptance_degree"]),
-        pair_lambda=np.asarray(folded["pair_lambda"], np.int64),
-        pair_mu=np.asarray(folded["pair_mu"], np.int64), phase=str(folded["phase"]),
-        bands=np.asarray(fold.bands, np.int64), scale=np.asarray(fold.scale, float),
-        provenance=json.dumps({"built_by": "lighthit ShowerTransport.tables() (BandFold rank 3)",
-                               "kernel": {"radial_range_m": [lo, hi],
-                                          "radial_nodes": c["radial_nodes"],
-                                          "k_panel_per_m": float(c["k_panel_per_m"])}}))
-    wl = np.asarray(k.wavelength.wavelength_nm, float)
-    sample = k.medium.sample(wl)
-    low, high = k.config.wavelength_range_nm or k.medium.wavelength_range_nm
-    native = k.medium.wavelength_nm
-    critical = np.r_[low, native[(native > low) & (native < high)], high]
-    prompt = _spectral_tables(k)
-    optics = prepare_optics(k, BallisticIntervalConfig(), exact_response=True)
-    d = k.detector
-    np.savez_compressed(
-        HERE / f"route_{name}.npz",
-        wavelength_nm=wl, weight_nm=np.asarray(k.wavelength.weight_nm, float),
-        phase_index=np.asarray(sample["phase_index"], float),
-        group_index=np.asarray(sample["group_index"], float),
-        absorption_per_m=np.asarray(sample["absorption_per_m"], float),
-        scattering_per_m=np.asarray(sample["scattering_per_m"], float),
-        efficiency=np.asarray(d.spectral_weight(wl), float),
-        threshold_phase=float(np.max(k.medium.sample(critical)["phase_index"])),
-        g=float(k.medium.g), fold_bands=np.asarray(fold.bands, np.int64),
-        fold_scale=np.asarray(fold.scale, float), fold_phase=np.asarray(fold.phase_index, float),
-        mus=prompt["mus"], mut=prompt["mut"], speed=prompt["speed"], s0w=prompt["s0w"],
-        s2w=prompt["s2w"], **{f"optics_{key}": optics[key] for key in (
-            "panel_edges", "phase_nodes", "group_nodes", "extinction_nodes",
-            "efficiency_coefficients")},
-        alpha=np.asarray(k.acceptance()["alpha"], float),
-        peak_acceptance=float(np.max(np.abs(np.asarray(
-            d.angular_acceptance(np.linspace(-1, 1, 257)), float)))),
-        positions_m=np.asarray(d.positions_m, float),
-        looks=np.asarray(-d.orientations, float),
-        areas_m2=np.broadcast_to(np.asarray(d.effective_area_m2, float), (n_om,)).copy(),
-        radii_m=np.broadcast_to(np.asarray(d.receiver_surface.radii(n_om), float), (n_om,)).copy(),
-        omega_per_ns=omega, readout_omega_per_ns=np.asarray(k.config.readout_omega_per_ns, float),
-        edges_ns=np.asarray(k.config.relative_time_edges_ns, float),
-        radial_range_m=np.asarray(k.config.radial_range_m, float),
-        threshold_pe=float(k.config.threshold_pe), source_degree=int(k.config.source_degree),
-        azimuthal_degree=int(k.config.azimuthal_degree))
-    print("wrote", name, "fold", fold.bands, fold.scale)
+    np.savez_compressed(HERE / f"ge2_fold_{len(detector)}om_{lo:g}-{hi:g}m.npz",
+                        **folded_kernels(route, tables))
+    np.savez_compressed(HERE / f"route_{name}.npz", **route_constants(route, tables))
+    print("wrote", name, "fold", tables["fold"].bands, tables["fold"].scale)
 
 
 if __name__ == "__main__":

@@ -56,7 +56,7 @@ def routed(request, stream):
     from dataclasses import replace
     from lighthit_b200.shower import ShowerTransport
     tables, g, kept, sources = stream
-    route = ShowerTransport(tables, replace(tables.settings, readout_mode=request.param))
+    route = ShowerTransport(tables, config=replace(tables.settings, readout_mode=request.param))
     return request.param, route.batch(sources), g, kept, tables.threshold
 
 
