@@ -282,6 +282,7 @@ def shower_section(args, dev, world):
             _lib.kernel_timing(True)
             served_ms, _ = served_region(server, timed, stream)
             kernels = _lib.kernel_times()
+            units = _lib.kernel_units()
             _lib.kernel_timing(False)
             if world > 1:
                 torch.distributed.barrier()
@@ -326,7 +327,7 @@ def shower_section(args, dev, world):
     return dict(pool=pool, served_ms=served_ms, served_rate=served_rate, steps=steps,
                 warmup=warmup, e2e_ms=e2e_ms, e2e_steps=e2e_steps, e2e_rate=job_rate(
                     len(host), world, e2e_ms), h2d=h2d, d2h=d2h, lat=lat, clocks=clocks.summary(),
-                kernels=kernels, plain_rate=plain_rate, plain_n=len(plain_showers),
+                kernels=kernels, units=units, plain_rate=plain_rate, plain_n=len(plain_showers),
                 launches_per_step=launches)
 
 
@@ -343,15 +344,26 @@ def count_launches(server, sources):
                and e.name.startswith("lh::"))
 
 
-def roofline(kernels, peaks):
-    """The fine order-1 group stage: one pencil record read per (OM, pencil)
-    evaluation (the unit of the order-1 row of the scope table)."""
-    if "o1_group_kernel" not in kernels:
+def shower_roofline(kernels, hbm_peak, peak_source):
+    """Roofline of the order-1 group stage (``o1_group_kernel``), the row's unit
+    being one (OM, pencil) evaluation that reads one float64 pencil record
+    (``PENCIL_BYTES``): achieved = evaluations per launch x record bytes over the
+    launch's average CUDA-event duration, both measured in the timed region."""
+    group = kernels.get("o1_group_kernel")
+    if not group or not group["units"]:
         return None
-    launches, total_ms = kernels["o1_group_kernel"]
-    items = kernels.get("_o1_group_items")
-    return {"kernel": "o1_group_kernel", "launches": launches,
-            "avg_launch_ms": total_ms / launches, "items": items}
+    per_launch = group["units"] / group["launches"]
+    achieved = per_launch * PENCIL_BYTES / (group["avg_ms"] / 1e3) / 1e9
+    traffic = (None if O1_GROUP_TRAFFIC_PER_ITEM is None
+               else O1_GROUP_TRAFFIC_PER_ITEM * per_launch)
+    return {"kernel": "o1_group_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+            "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
+            "peak_source": peak_source, "algorithmic_bytes_per_unit": PENCIL_BYTES,
+            "unit_of_work": "(OM, pencil) evaluation", "units_per_launch": per_launch,
+            "avg_launch_ms": group["avg_ms"], "launches": group["launches"],
+            "note": "the pencil table (a few MB) stays in L2, so DRAM traffic is far below "
+                    "the algorithmic bytes: the kernel is bound by float64 issue and latency "
+                    "(see profiles/), not by HBM"}
 
 
 def flash_section(args, dev):
@@ -413,6 +425,29 @@ def flash_section(args, dev):
             "l2": "flushed between launches"}
 
 
+def kernel_case(args):
+    """One stage-major batch of the first ``args.kernel_case`` showers of the
+    stream through ``ShowerTransport.batch`` (after one untimed batch): the
+    small case the ncu captures of the shower kernels run on. Prints the timed
+    kernels of the second batch."""
+    import torch
+    from lighthit_b200 import _lib
+    from lighthit_b200.shower import ShowerTables, ShowerTransport
+    route = ShowerTransport(ShowerTables.synthetic("c2"))
+    pool = shower_pool(route.tables.positions.mean(axis=0), args.kernel_case)
+    route.batch(pool)
+    torch.cuda.synchronize()
+    _lib.kernel_timing(True)
+    route.batch(pool)
+    torch.cuda.synchronize()
+    times = _lib.kernel_times()
+    units = _lib.kernel_units()
+    _lib.kernel_timing(False)
+    print(json.dumps({"case": f"first {len(pool)} showers of the config-2 stream, one batch",
+                      "kernels": {k: {"launches": n, "total_ms": ms, "units": units.get(k)}
+                                  for k, (n, ms) in times.items()}}), flush=True)
+
+
 def ours(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
@@ -434,18 +469,10 @@ def ours(args, rank, world, local_rank):
                "sample": f"the first {done} showers of the stream ({secs:.1f} s); {ORACLE_SAMPLE}"}
     if rank != 0:
         return
-    kernels = {k: {"launches": n, "total_ms": ms, "avg_ms": ms / n}
+    kernels = {k: {"launches": n, "total_ms": ms, "avg_ms": ms / n, "units": s["units"].get(k)}
                for k, (n, ms) in s["kernels"].items()}
     top = max(kernels.items(), key=lambda kv: kv[1]["total_ms"])[0] if kernels else None
-    group = kernels.get("o1_group_kernel")
-    roof = None
-    if group is not None:
-        # algorithmic bytes: one pencil record per (OM, pencil) evaluation; the
-        # evaluations of the timed region come from the route's own counters
-        items = s["kernels"].get("__o1_items__")
-        roof = {"kernel": "o1_group_kernel", "bound": "hbm", "achieved": None, "peak": hbm_peak,
-                "unit": "GB/s", "frac": None, "traffic": None, "peak_source": peak_source,
-                "avg_launch_ms": group["avg_ms"], "launches": group["launches"]}
+    roof = shower_roofline(kernels, hbm_peak, peak_source)
     line = {
         "metric": METRIC, "value": s["served_rate"], "unit": "showers/s", "n_gpus": world,
         "steps": s["steps"], "warmup": s["warmup"],
@@ -484,7 +511,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-flash", action="store_true", help="skip the flash-stream section")
+    ap.add_argument("--kernel-case", type=int, default=0, metavar="N",
+                    help="run only one batch of N showers (the case of the ncu captures)")
     args = ap.parse_args()
+    if args.kernel_case:
+        kernel_case(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

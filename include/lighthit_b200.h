@@ -246,9 +246,16 @@ typedef struct {
   const double* extinction;    /* [n_panel_edges] mu_a + mu_s 1/m                      */
   int32_t eff_cols;            /* 4 (cubic) or 6 (cubic x exp(linear))                 */
   const double* efficiency;    /* [n_panel_edges - 1][eff_cols]                        */
-  int32_t order;               /* Gauss-Legendre order of every quadrature (<= 32)     */
+  int32_t order;               /* Gauss-Legendre order of every quadrature (<= 64)     */
   const double* gauss_x;       /* [order] nodes on (-1, 1)                             */
   const double* gauss_w;       /* [order] weights                                      */
+  /* A second, lower Gauss order evaluated in the same launch when the batch asks
+   * for it (charge_check): the per-OM difference of the two charges is the
+   * quadrature's error estimate (the reference doubles its order until
+   * successive charges agree, _surface_ballistic.py:149-168). 0: none. */
+  int32_t check_order;         /* < order                                              */
+  const double* check_x;       /* [check_order] nodes                                  */
+  const double* check_w;       /* [check_order] weights                                */
 } lh_order0_optics;
 
 typedef struct {
@@ -271,6 +278,8 @@ typedef struct {
   int32_t* status;               /* [1] LH_STATUS_* flags (or-ed in)                      */
   void* workspace;               /* lh_order0_workspace_bytes bytes of device memory      */
   size_t workspace_bytes;
+  double* charge_check;          /* [n_events][n_om] charge at optics->check_order
+                                    (overwritten), or NULL: no check                      */
 } lh_order0_batch;
 
 /* Device scratch for one call: candidate-pair lists (4 bytes per (OM, element)). */
@@ -574,6 +583,12 @@ enum {
 };
 int lh_kernel_timing(int enable);
 int lh_kernel_timing_read(int32_t n_kernels, int64_t* launches, double* total_ms);
+/* Algorithmic work units of the timed kernels, counted on the device by every
+ * launch since the last lh_kernel_timing(1) (after a device synchronisation):
+ * (OM, pencil) evaluations for o1_group_kernel, float32 integrand
+ * evaluations (one wavelength x along-track x azimuth node of a piece) for
+ * order0_kernel, 0 for the kernels that do not count. */
+int lh_kernel_units_read(int32_t n_kernels, int64_t* units);
 
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory

@@ -86,7 +86,8 @@ class Order0Optics(C.Structure):
                 ("om_radius", P), ("n_alpha", C.c_int32), ("alpha", P),
                 ("n_panel_edges", C.c_int32), ("panel_edges", P), ("phase", P), ("group", P),
                 ("extinction", P), ("eff_cols", C.c_int32), ("efficiency", P),
-                ("order", C.c_int32), ("gauss_x", P), ("gauss_w", P)]
+                ("order", C.c_int32), ("gauss_x", P), ("gauss_w", P),
+                ("check_order", C.c_int32), ("check_x", P), ("check_w", P)]
 
 
 class Order0Batch(C.Structure):
@@ -94,7 +95,8 @@ class Order0Batch(C.Structure):
                 ("start", P), ("direction", P), ("length", P),
                 ("c0", P), ("c2", P), ("beta", P), ("t0", P), ("t1", P), ("origins", P),
                 ("n_edges", C.c_int32), ("edges", P), ("charge", P), ("bins", P),
-                ("status", P), ("workspace", P), ("workspace_bytes", C.c_size_t)]
+                ("status", P), ("workspace", P), ("workspace_bytes", C.c_size_t),
+                ("charge_check", P)]
 
 
 class Order1Config(C.Structure):
@@ -188,6 +190,7 @@ SIGNATURES = {
                                              C.POINTER(FlashBatch), P]),
     "lh_kernel_timing": (C.c_int, [C.c_int]),
     "lh_kernel_timing_read": (C.c_int, [C.c_int32, P, P]),
+    "lh_kernel_units_read": (C.c_int, [C.c_int32, P]),
     "lh_flash_combine": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(FlashNodes),
                                    C.POINTER(FlashBatch), P]),
     "lh_ge2_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem)]),
@@ -320,3 +323,14 @@ def kernel_times():
           "lh_kernel_timing_read")
     return {name: (int(launches[k]), float(total[k])) for k, name in enumerate(TIMED_KERNELS)
             if launches[k]}
+
+
+def kernel_units():
+    """``{kernel: units}`` of algorithmic work counted on the device since the
+    timing was last started ((OM, pencil) evaluations of ``o1_group_kernel``,
+    integrand nodes of ``order0_kernel``)."""
+    import numpy as np
+    n = len(TIMED_KERNELS)
+    units = np.zeros(n, np.int64)
+    check(load().lh_kernel_units_read(n, units.ctypes.data), "lh_kernel_units_read")
+    return {name: int(units[k]) for k, name in enumerate(TIMED_KERNELS) if units[k]}

@@ -41,7 +41,7 @@ namespace lh {
 
 constexpr int kO0Chunk = 32;
 constexpr int kO0Threads = 256;
-constexpr int kO0MaxOrder = 32;
+constexpr int kO0MaxOrder = 64;
 constexpr int kO0MaxPanels = 128;
 constexpr int kO0MaxSCuts = 64;
 constexpr int kO0MaxPhiCuts = 32;
@@ -351,19 +351,26 @@ __global__ void __launch_bounds__(1024) order0_scan_kernel(int32_t n_keys, O0Wor
   if (threadIdx.x == 0) *W.n_chunks = carry_chunks;
 }
 
+// One Gauss rule: nodes, weights and the s-node map sin/cos(pi/2 x).
+struct O0Rule {
+  double x[kO0MaxOrder], w[kO0MaxOrder];
+  double sin_psi[kO0MaxOrder], cos_psi[kO0MaxOrder];
+};
+
 struct O0Shared {
-  double gx[kO0MaxOrder], gw[kO0MaxOrder];
-  double sin_psi[kO0MaxOrder], cos_psi[kO0MaxOrder];  // sin/cos(pi/2 gx): s-node map
+  O0Rule rule[2];  // the quadrature order and the lower check order
   float alpha[kO0MaxAlpha];
   O0Pair pair[kO0Chunk];
   double warp_charge[kO0Threads / 32];
+  double warp_check[kO0Threads / 32];
   int n_pairs;
   int n_combos;
   int next_item;  // phase-2 work counter (warps take 32 items at a time)
 };
 
-__global__ void __launch_bounds__(kO0Threads, 3)
-order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W) {
+__global__ void __launch_bounds__(kO0Threads, 4)
+order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W,
+              unsigned long long* units) {
   extern __shared__ __align__(16) unsigned char o0_smem[];
   O0Shared& S = *reinterpret_cast<O0Shared*>(o0_smem);
   const int n_panels = O.n_panel_edges - 1;
@@ -373,15 +380,24 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
   uint32_t* combos = reinterpret_cast<uint32_t*>(sbins + (want_bins ? nb : 0));
   const int tid = threadIdx.x;
   const int order = O.order;
+  // the check rule's items follow the main rule's in each (pair, panel, piece)
+  const int check = (B.charge_check && O.check_order > 0) ? O.check_order : 0;
+  const int rules = order + check;
   for (int k = tid; k < order; k += blockDim.x) {
-    S.gx[k] = O.gauss_x[k];
-    S.gw[k] = O.gauss_w[k];
-    sincospi(0.5 * O.gauss_x[k], &S.sin_psi[k], &S.cos_psi[k]);
+    S.rule[0].x[k] = O.gauss_x[k];
+    S.rule[0].w[k] = O.gauss_w[k];
+    sincospi(0.5 * O.gauss_x[k], &S.rule[0].sin_psi[k], &S.rule[0].cos_psi[k]);
+  }
+  for (int k = tid; k < check; k += blockDim.x) {
+    S.rule[1].x[k] = O.check_x[k];
+    S.rule[1].w[k] = O.check_w[k];
+    sincospi(0.5 * O.check_x[k], &S.rule[1].sin_psi[k], &S.rule[1].cos_psi[k]);
   }
   for (int k = tid; k < O.n_alpha; k += blockDim.x) S.alpha[k] = (float)O.alpha[k];
   double pmin, pmax;
   o0_phase_range(O, pmin, pmax);
   const int total_chunks = min(*W.n_chunks, (int)W.chunk_capacity);
+  unsigned long long evaluations = 0;  // float32 integrand nodes of this thread
   for (int chunk = blockIdx.x; chunk < total_chunks; chunk += gridDim.x) {
   __syncthreads();
   const int2 entry = W.chunks[chunk];
@@ -501,13 +517,13 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
   for (int k = 0; k < O.n_alpha; ++k) alpha_abs += fabsf(S.alpha[k]);
   alpha_abs = fmaxf(alpha_abs, 1.0f);
   bool bad_acceptance = false;
-  double charge = 0.0;
+  double charge = 0.0, charge_check = 0.0;
   double scuts[kO0MaxSCuts];
   double phicuts[kO0MaxPhiCuts];
 
   // warps take 32 consecutive items at a time from a shared counter, so a warp
   // that drew cheap pieces goes back for more instead of idling at the barrier
-  const int n_items = n_combos * order;
+  const int n_items = n_combos * rules;
   const int lane = tid & 31;
   for (int item_base = 0;;) {
     if (lane == 0) item_base = atomicAdd(&S.next_item, 32);
@@ -515,7 +531,11 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
     if (item_base >= n_items) break;
     const int item = item_base + lane;
     if (item >= n_items) continue;
-    const int ci = item / order, ilam = item - ci * order;
+    const int ci = item / rules, r_item = item - ci * rules;
+    const bool is_check = r_item >= order;
+    const int ilam = is_check ? r_item - order : r_item;
+    const int ord = is_check ? check : order;
+    const O0Rule& R = S.rule[is_check ? 1 : 0];
     const uint32_t code = combos[ci];
     const int p = code & 0xff, panel = (code >> 8) & 0xffff, piece = code >> 24;
     const O0Pair& P = S.pair[p];
@@ -541,7 +561,7 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
     }
     const double low = cuts[piece], high = cuts[piece + 1];
     const double beta = B.beta[i], L = B.length[i];
-    const double lam = (low + high) / 2 + (high - low) / 2 * S.gx[ilam];
+    const double lam = (low + high) / 2 + (high - low) / 2 * R.x[ilam];
     const double q = (lam - left) / width, n = n0 + dn * q, bn = beta * n;
     if (bn <= 1.0) continue;
     const double cosine = 1 / bn, sine = sqrt(1 - cosine * cosine);
@@ -556,7 +576,7 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
     double eta = ((ef[3] * q + ef[2]) * q + ef[1]) * q + ef[0];
     if (O.eff_cols > 4) eta *= exp(ef[4] + q * ef[5]);
     const double spectral = (B.c0[i] + B.c2[i] / (n * n)) / L / (lam * lam) * eta;
-    const double scale = (high - low) / 2 * S.gw[ilam] * spectral * area_scale;
+    const double scale = (high - low) / 2 * R.w[ilam] * spectral * area_scale;
     const double t0 = B.t0[i], tau = P.tau;
 
     // s cuts where a cone ray's entry time crosses a bin edge (_surface_ballistic_rays.py:96-118)
@@ -597,10 +617,10 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
     for (int sp = 0; sp < ns - 1; ++sp) {
       const double sa = scuts[sp], sb = scuts[sp + 1];
       if (sa >= sb) continue;
-      for (int j = 0; j < order; ++j) {
-        const double sin_psi = S.sin_psi[j], cos_psi = S.cos_psi[j];
+      for (int j = 0; j < ord; ++j) {
+        const double sin_psi = R.sin_psi[j], cos_psi = R.cos_psi[j];
         const double s = (sa + sb) / 2 + (sb - sa) / 2 * sin_psi;
-        const double ds = (sb - sa) / 2 * cos_psi * kPi / 2 * S.gw[j];
+        const double ds = (sb - sa) / 2 * cos_psi * kPi / 2 * R.w[j];
         const double along = z - s, W2 = rho * rho + along * along, Bq = W2 - radius * radius;
         double half;
         if (rho > 0.0) {
@@ -642,14 +662,15 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
           const double pa = phicuts[pp], pb = phicuts[pp + 1];
           if (pa >= pb) continue;
           const float mid = (float)((pa + pb) / 2), hw = (float)((pb - pa) / 2);
+          evaluations += ord;
           float integral = 0.0f;
-          for (int jp = 0; jp < order; ++jp) {
+          for (int jp = 0; jp < ord; ++jp) {
             // arguments lie in [0, pi]: the hardware approximations (absolute error
             // near 2^-21) are well inside the float32 integrand's budget
             float s_eta, c_eta;
-            __sincosf(mid + hw * (float)S.gx[jp], &s_eta, &c_eta);
+            __sincosf(mid + hw * (float)R.x[jp], &s_eta, &c_eta);
             const float phi = half_f * s_eta;
-            const float dphi = half_f * c_eta * hw * (float)S.gw[jp];
+            const float dphi = half_f * c_eta * hw * (float)R.w[jp];
             // sin(phi), cos(phi) from the half angle: 2 sin^2(phi/2) = 1 - cos(phi)
             // without cancellation near phi = 0
             float sh, chh;
@@ -666,6 +687,10 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
             integral += dphi * accept * __expf(-absorption_f * distance);
           }
           const double value = scale * ds * (double)integral * (1.0 / (2 * kPi));
+          if (is_check) {  // the check rule: charge only
+            charge_check += value;
+            continue;
+          }
           charge += value;
           if (want_bins) {
             const double phi_mid = half * sin((pa + pb) / 2);
@@ -681,13 +706,24 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
   if (bad_acceptance) flags |= LH_STATUS_NEGATIVE_ACCEPTANCE;
 
   // ---- charge: warp shuffles, then one add per CTA; bins: one add per nonzero bin
-  for (int off = 16; off > 0; off >>= 1) charge += __shfl_xor_sync(0xffffffffu, charge, off);
-  if ((tid & 31) == 0) S.warp_charge[tid >> 5] = charge;
+  for (int off = 16; off > 0; off >>= 1) {
+    charge += __shfl_xor_sync(0xffffffffu, charge, off);
+    charge_check += __shfl_xor_sync(0xffffffffu, charge_check, off);
+  }
+  if ((tid & 31) == 0) {
+    S.warp_charge[tid >> 5] = charge;
+    S.warp_check[tid >> 5] = charge_check;
+  }
   __syncthreads();
   if (tid == 0) {
-    double total = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += S.warp_charge[w];
+    double total = 0.0, total_check = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      total += S.warp_charge[w];
+      total_check += S.warp_check[w];
+    }
     if (total != 0.0) atomicAdd(&B.charge[(int64_t)ev * O.n_om + om], total);
+    if (check && total_check != 0.0)
+      atomicAdd(&B.charge_check[(int64_t)ev * O.n_om + om], total_check);
   }
   if (want_bins) {
     double* out = B.bins + ((int64_t)ev * O.n_om + om) * nb;
@@ -696,6 +732,11 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W)
   }
   if (flags) atomicOr(reinterpret_cast<unsigned*>(B.status), flags);
   }  // chunks
+  if (units) {
+    for (int off = 16; off > 0; off >>= 1)
+      evaluations += __shfl_xor_sync(0xffffffffu, evaluations, off);
+    if ((tid & 31) == 0 && evaluations) atomicAdd(units, evaluations);
+  }
 }
 
 size_t order0_shared_bytes(const lh_order0_optics& O, const lh_order0_batch& B) {
@@ -743,6 +784,8 @@ int order0_launch(const lh_order0_optics& O, const lh_order0_batch& B, cudaStrea
     return LH_ECUDA;
   const int64_t keys = (int64_t)B.n_events * O.n_om;
   cudaMemsetAsync(B.charge, 0, sizeof(double) * (size_t)keys, s);
+  if (B.charge_check && O.check_order > 0)
+    cudaMemsetAsync(B.charge_check, 0, sizeof(double) * (size_t)keys, s);
   if (B.bins) cudaMemsetAsync(B.bins, 0, sizeof(double) * (size_t)keys * (B.n_edges - 1), s);
   if (B.n_elements == 0) return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
   cudaMemsetAsync(W.counts, 0, sizeof(int32_t) * keys, s);
@@ -753,7 +796,8 @@ int order0_launch(const lh_order0_optics& O, const lh_order0_batch& B, cudaStrea
   order0_candidates_kernel<true><<<blocks, 256, 0, s>>>(O, B, W);
   {
     lh::TimedLaunch timed_launch(LH_KT_ORDER0, s);
-    order0_kernel<<<148 * 8, kO0Threads, smem, s>>>(O, B, W);
+    order0_kernel<<<148 * 8, kO0Threads, smem, s>>>(
+        O, B, W, lh::kernel_units() ? lh::kernel_units() + LH_KT_ORDER0 : nullptr);
   }
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }
@@ -768,6 +812,9 @@ bool order0_valid(const lh_order0_optics* O, const lh_order0_batch* B) {
     return false;
   if (O->eff_cols != 4 && O->eff_cols != 6) return false;
   if (O->order < 1 || O->order > kO0MaxOrder || !O->gauss_x || !O->gauss_w) return false;
+  if (O->check_order < 0 || O->check_order >= O->order ||
+      (O->check_order > 0 && (!O->check_x || !O->check_w)))
+    return false;
   if (B->n_events < 1 || !B->element_offset || B->n_elements < 0) return false;
   // pair indices, counts and offsets are 32-bit
   if (B->n_elements * (int64_t)O->n_om >= (1ll << 31)) return false;

@@ -50,24 +50,53 @@ LH_DEVICE uint64_t o1_mix(uint64_t v) {
   return v ^ (v >> 31);
 }
 
+// A slot whose claiming thread is still zeroing its row holds its key with
+// this bit set (keys stay below 2^62).
+constexpr long long kO1Busy = 1ll << 62;
+constexpr long long kO1ClaimWaitNs = 100000000ll;  // a wait for a claimed row gives up after 0.1 s
+
 // Insert `key` (>= 0) into an open-addressing table of `capacity` (power of
-// two) slots holding -1 when free. Returns the slot, or -1 when full; `fresh`
-// tells whether this call claimed it.
-LH_DEVICE int64_t o1_insert(long long* keys, int64_t capacity, long long key, bool& fresh,
-                            bool ordered = false) {
+// two) slots holding -1 when free, whose rows of `n` doubles at `rows` are
+// not cleared beforehand: the thread that claims a free slot marks it busy,
+// zeroes the slot's row, then publishes the key; a thread that finds its key
+// still busy waits for the publication (bounded: past kO1ClaimWaitNs it sets
+// LH_STATUS_TIMEOUT and returns -1). Returns the slot, or -1 when the table
+// is full (LH_STATUS_OVERFLOW); `fresh` tells whether this call claimed it.
+// Only the rows of published slots are ever read.
+LH_DEVICE int64_t o1_insert(long long* keys, int64_t capacity, long long key, double* rows,
+                            int n, bool& fresh, int32_t* status, bool ordered = false) {
   const uint64_t mask = (uint64_t)capacity - 1;
   uint64_t slot = (ordered ? (uint64_t)key : o1_mix((uint64_t)key)) & mask;
   fresh = false;
+  unsigned long long* word = reinterpret_cast<unsigned long long*>(keys);
   for (int64_t probe = 0; probe < capacity; ++probe) {
-    long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(keys + slot),
-                               (unsigned long long)(-1ll), (unsigned long long)key);
+    const long long prev = (long long)atomicCAS(word + slot, (unsigned long long)(-1ll),
+                                                (unsigned long long)(key | kO1Busy));
     if (prev == -1ll) {
+      double* row = rows + (int64_t)slot * n;
+      for (int k = 0; k < n; ++k) row[k] = 0.0;
+      __threadfence();  // the zeros reach the device before the key does
+      atomicExch(word + slot, (unsigned long long)key);
       fresh = true;
       return (int64_t)slot;
     }
     if (prev == key) return (int64_t)slot;
+    if (prev == (key | kO1Busy)) {
+      const unsigned long long began = global_ns();
+      for (int poll = 0;; ++poll) {
+        if ((long long)atomicAdd(word + slot, 0ull) == key) {
+          __threadfence();  // the row's zeros before this thread's additions
+          return (int64_t)slot;
+        }
+        if ((poll & 63) == 63 && (long long)(global_ns() - began) > kO1ClaimWaitNs) {
+          atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_TIMEOUT);
+          return -1;
+        }
+      }
+    }
     slot = (slot + 1) & mask;
   }
+  atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
   return -1;
 }
 
@@ -107,15 +136,34 @@ LH_DEVICE O1Subseg o1_subseg(const lh_order1_elements& E, int64_t i, int64_t ia,
   return s;
 }
 
+constexpr int kO1CoopGroups = 8;  // at most this many groups per warp: summed by the whole warp
+
 // Warp-level sums by key: every lane writes its n values to its row of the
-// warp's staging area (`stage`, 32 rows of n doubles in shared memory); the
-// lowest lane of each group of equal keys (`group`, a __match_any_sync mask)
-// adds its members' rows in lane order and issues one atomic per value to
-// `row`. The loads are independent, so a group of g lanes costs about g x n
-// issue slots in its leader instead of g dependent round trips.
+// warp's staging area (`stage`, 32 rows of n doubles in shared memory), and
+// each group of lanes with equal keys (`group`, a __match_any_sync mask; its
+// lowest lane the `leader`, holding the group's `row`) adds its members' rows
+// in lane order with one atomic per value. With few groups the whole warp
+// takes one group at a time (lane k sums value k); with many, each leader
+// sums its own group's values one after another. Both sum in the same order.
 LH_DEVICE void o1_warp_group_add(double* stage, int n, unsigned group, bool leader, double* row) {
   __syncwarp();
-  if (leader && row) {
+  const unsigned full = 0xffffffffu;
+  unsigned leaders = __ballot_sync(full, leader && row != nullptr);
+  if (__popc(leaders) <= kO1CoopGroups) {
+    const int lane = threadIdx.x & 31;
+    while (leaders) {
+      const int src = __ffs(leaders) - 1;
+      leaders &= leaders - 1;
+      const unsigned members = __shfl_sync(full, group, src);
+      double* target = reinterpret_cast<double*>(
+          __shfl_sync(full, reinterpret_cast<unsigned long long>(row), src));
+      for (int k = lane; k < n; k += 32) {
+        double sum = 0.0;
+        for (unsigned g = members; g; g &= g - 1) sum += stage[(__ffs(g) - 1) * n + k];
+        atomicAdd(target + k, sum);
+      }
+    }
+  } else if (leader && row) {
     for (int k = 0; k < n; ++k) {
       double sum = 0.0;
       for (unsigned g = group; g; g &= g - 1) sum += stage[(__ffs(g) - 1) * n + k];
@@ -207,9 +255,8 @@ o1_ring_kernel(const lh_order1_config C, const lh_order1_elements E,
         bool fresh;
         // slots in key order (keys of one cell are contiguous) so that the
         // compacted pencils come out spatially ordered
-        const int64_t slot = o1_insert(keys, capacity, key, fresh, true);
-        if (slot < 0) atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
-        else row = rows + slot * kO1Moments;
+        const int64_t slot = o1_insert(keys, capacity, key, rows, kO1Moments, fresh, status, true);
+        if (slot >= 0) row = rows + slot * kO1Moments;
       }
       const double tx = -sp * e1x + cp * e2x, ty = -sp * e1y + cp * e2y, tz = -sp * e1z + cp * e2z;
       const double m[kO1Moments] = {
@@ -300,11 +347,9 @@ o1_parent_kernel(const long long* keys, const double* rows, int64_t capacity, in
     if (key == -1ll) continue;
     bool fresh;
     const int64_t ps = o1_insert(parent_keys, parent_capacity,
-                                 o1_parent_key(key, face, parent_face), fresh, true);
-    if (ps < 0) {
-      atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
-      continue;
-    }
+                                 o1_parent_key(key, face, parent_face), parent_rows, kO1Moments,
+                                 fresh, status, true);
+    if (ps < 0) continue;
     for (int k = 0; k < kO1Moments; ++k)
       atomicAdd(parent_rows + ps * kO1Moments + k, rows[slot * kO1Moments + k]);
   }
@@ -444,19 +489,80 @@ LH_DEVICE void o1_write_pencil(const double* a, lh_order1_pencil_table& Pn, int 
 
 // ------------------------------------------------------------------ stage B
 
-// gauss_inverse_mean_prepared (_prompt_numba.py:115-129)
-LH_DEVICE double o1_gauss_inverse_mean(double u, double v, double var_u, double var_v,
-                                       const double* tangent, const double* wsec2, int n) {
-  const double scale = 2.0 * (var_u + var_v) + u * u + v * v;
-  if (scale <= 0.0) return 1e300;
-  const double s0 = 1.0 / sqrt(scale);
-  double total = 0.0;
-  for (int k = 0; k < n; ++k) {
-    const double s = s0 * tangent[k], s2 = s * s;
-    const double a = 1.0 + 2.0 * s2 * var_u, b = 1.0 + 2.0 * s2 * var_v;
-    total += wsec2[k] * exp(-s2 * (u * u / a + v * v / b)) / sqrt(a * b);
+// Node sums of the Gaussian inverse-radius measure shared by
+// gauss_inverse_mean_prepared (_prompt_numba.py:115-129) and
+// inverse_radius_rule (_prompt_screen.py:101-140), for every lane of `need`
+// (arguments u, v, var_u, var_v): the warp evaluates one lane's nodes at a
+// time, lane j taking nodes j, j + 32, ..., and a butterfly reduction adds
+// them, so a lane that needs the 48-node sum does not run it alone while the
+// rest of its warp waits. Each lane of `need` receives s0 = 1 / sqrt(scale),
+// scale = 2 (var_u + var_v) + u^2 + v^2 (its sums stay 0 when scale <= 0),
+// the sum of the node masses and of mass x the radial second moment. Call
+// with the whole warp.
+LH_DEVICE void o1_node_sums(unsigned need, double u, double v, double var_u, double var_v,
+                            const double* tangent, const double* wsec2, int n, double& s0_out,
+                            double& mass_out, double& radial_out) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  s0_out = mass_out = radial_out = 0.0;
+  while (need) {
+    const int src = __ffs(need) - 1;
+    need &= need - 1;
+    const double bu = __shfl_sync(full, u, src), bv = __shfl_sync(full, v, src);
+    const double bvu = __shfl_sync(full, var_u, src), bvv = __shfl_sync(full, var_v, src);
+    const double scale = 2.0 * (bvu + bvv) + bu * bu + bv * bv;
+    if (scale <= 0.0) continue;  // the same for the whole warp
+    const double s0 = 1.0 / sqrt(scale);
+    double mass = 0.0, radial = 0.0;
+    for (int k = lane; k < n; k += 32) {
+      const double t = s0 * tangent[k];
+      const double a = 1.0 + 2.0 * t * t * bvu, b = 1.0 + 2.0 * t * t * bvv;
+      const double m = wsec2[k] * exp(-t * t * (bu * bu / a + bv * bv / b)) / sqrt(a * b);
+      mass += m;
+      radial += m * (bvu / a + bvv / b + bu * bu / (a * a) + bv * bv / (b * b));
+    }
+    for (int off = 16; off; off >>= 1) {
+      mass += __shfl_xor_sync(full, mass, off);
+      radial += __shfl_xor_sync(full, radial, off);
+    }
+    if (lane == src) {
+      s0_out = s0;
+      mass_out = mass;
+      radial_out = radial;
+    }
   }
-  return 2.0 / sqrt(kPi) * s0 * total;
+}
+
+// gauss_inverse_mean_prepared from its node sums.
+LH_DEVICE double o1_gauss_inverse_mean(double u, double v, double var_u, double var_v, double s0,
+                                       double mass) {
+  if (2.0 * (var_u + var_v) + u * u + v * v <= 0.0) return 1e300;
+  return 2.0 / sqrt(kPi) * s0 * mass;
+}
+
+// inverse_radius_rule from its node sums: a positive two-node rule for the
+// Gaussian measure over the radius (w0, t0, w1, t1).
+LH_DEVICE void o1_inverse_radius_rule(double u, double v, double var_u, double var_v, double s0,
+                                      double mass, double radial, double& w0, double& t0,
+                                      double& w1, double& t1) {
+  w0 = t0 = w1 = t1 = 0.0;
+  if (2.0 * (var_u + var_v) + u * u + v * v <= 0.0) return;
+  const double multiplier = 2.0 / sqrt(kPi) * s0;
+  const double inverse = mass * multiplier;
+  radial *= multiplier;
+  if (inverse <= 0.0) return;
+  const double mean = 1.0 / inverse, second = radial / inverse;
+  const double variance = second - mean * mean;
+  if (variance <= 0.0) {
+    w0 = inverse; t0 = mean; t1 = mean;
+    return;
+  }
+  const double third = (u * u + v * v + var_u + var_v) / inverse;
+  const double other = (third - 2.0 * mean * second + mean * mean * mean) / variance;
+  const double disc = sqrt((mean - other) * (mean - other) + 4.0 * variance);
+  const double low = 0.5 * (mean + other - disc), high = 0.5 * (mean + other + disc);
+  const double low_weight = inverse * (high - mean) / (high - low);
+  w0 = low_weight; t0 = low; w1 = inverse - low_weight; t1 = high;
 }
 
 // The coarse screen's refinement test (_prompt_screen.py:233-240): the OM
@@ -477,41 +583,6 @@ LH_DEVICE bool o1_refined(const lh_order1_config& C, const lh_order1_pencil_tabl
   return theta < 0.5 * kPi && theta * theta < sf * sf * extent2;
 }
 
-// inverse_radius_rule (_prompt_screen.py:101-140): a positive two-node rule
-// for the Gaussian measure over the radius (w0, t0, w1, t1).
-LH_DEVICE void o1_inverse_radius_rule(double u, double v, double var_u, double var_v,
-                                      const double* tangent, const double* wsec2, int n,
-                                      double& w0, double& t0, double& w1, double& t1) {
-  w0 = t0 = w1 = t1 = 0.0;
-  const double scale = 2.0 * (var_u + var_v) + u * u + v * v;
-  if (scale <= 0.0) return;
-  const double s0 = 1.0 / sqrt(scale);
-  double inverse = 0.0, radial = 0.0;
-  for (int k = 0; k < n; ++k) {
-    const double t = s0 * tangent[k];
-    const double a = 1.0 + 2.0 * t * t * var_u, b = 1.0 + 2.0 * t * t * var_v;
-    const double mass = wsec2[k] * exp(-t * t * (u * u / a + v * v / b)) / sqrt(a * b);
-    inverse += mass;
-    radial += mass * (var_u / a + var_v / b + u * u / (a * a) + v * v / (b * b));
-  }
-  const double multiplier = 2.0 / sqrt(kPi) * s0;
-  inverse *= multiplier;
-  radial *= multiplier;
-  if (inverse <= 0.0) return;
-  const double mean = 1.0 / inverse, second = radial / inverse;
-  const double variance = second - mean * mean;
-  if (variance <= 0.0) {
-    w0 = inverse; t0 = mean; t1 = mean;
-    return;
-  }
-  const double third = (u * u + v * v + var_u + var_v) / inverse;
-  const double other = (third - 2.0 * mean * second + mean * mean * mean) / variance;
-  const double disc = sqrt((mean - other) * (mean - other) + 4.0 * variance);
-  const double low = 0.5 * (mean + other - disc), high = 0.5 * (mean + other + disc);
-  const double low_weight = inverse * (high - mean) / (high - low);
-  w0 = low_weight; t0 = low; w1 = inverse - low_weight; t1 = high;
-}
-
 struct O1GroupShared {
   double tangent[kO1MaxGauss], wsec2[kO1MaxGauss];
   double coef[kO1MaxMono];
@@ -520,11 +591,12 @@ struct O1GroupShared {
 
 // One thread per (work OM, pencil): _grouped_pencils_order1_block's pencil
 // loop (_prompt_numba.py:1827-1921) with the generic moment layout.
-__global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
+__global__ void __launch_bounds__(256, 3)
+o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
                                 int32_t n_pencils_bound, const int32_t* n_pencils_device,
                                 const int32_t* work, int32_t n_work,
                                 const double* origins, long long* gkeys, double* grows,
-                                int32_t* gcount, int32_t* status) {
+                                int32_t* gcount, int32_t* status, unsigned long long* units) {
   __shared__ O1GroupShared S;
   for (int k = threadIdx.x; k < C.n_gauss; k += blockDim.x) {
     const double t = tan(C.gauss_tau[k]);
@@ -545,6 +617,7 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
   const int32_t n_pencils =
       n_pencils_device ? min(*n_pencils_device, n_pencils_bound) : n_pencils_bound;
   const int64_t total = (int64_t)n_work * n_pencils;
+  if (units && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(units, (unsigned long long)total);
   const int lane = threadIdx.x & 31;
   extern __shared__ double o1g_stage[];  // [warp][32][n_values]
   double* stage = o1g_stage + (threadIdx.x >> 5) * 32 * n_values;
@@ -589,13 +662,22 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
     const double c3 = sine > 1e-300 ? (qx * nx + qy * ny + qz * nz) / sine : 0.0;
     double theta = atan2(sine, cosine);
     const bool backward = theta > 0.5 * kPi;
-    double weight, weight2 = 0.0, theta2 = theta;
+    double weight = 0.0, weight2 = 0.0, theta2 = theta;
     bool averaged = false;
     const double ax = Pn.major[3 * p], ay = Pn.major[3 * p + 1], az = Pn.major[3 * p + 2];
     const double* cov = Pn.pos_cov + 6 * p;
     // _prepare_pencil_shape (_prompt_numba.py:1347-1370)
     const double bx = sy * az - sz * ay, by = sz * ax - sx * az, bz = sx * ay - sy * ax;
     const double trace = cov[0] + cov[1] + cov[2];
+    const double sf = C.smoothing_factor;
+    // How this lane's weight is formed: 0 done; 1 the screen's two-node radial
+    // rule; 2 the Gauss inverse mean; 3 the far-field expansion. Modes 1 and 2
+    // need a 48-node sum, which the whole warp evaluates for each such lane.
+    int mode = 0;
+    bool far = true;
+    double m11 = 0.0, m22 = 0.0, m12 = 0.0, mu1 = 0.0, mu2 = 0.0, extent = 0.0;
+    double u_ = 0.0, v_ = 0.0, r_extent = 0.0;
+    double arg_u = 0.0, arg_v = 0.0, arg_var_u = 0.0, arg_var_v = 0.0;  // of the node sums
     if (backward) {
       weight = 1.0 / r;
     } else {
@@ -614,14 +696,12 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
                            ay * (cov[3] * bx + cov[1] * by + cov[5] * bz) +
                            az * (cov[4] * bx + cov[5] * by + cov[2] * bz);
         const double inv_r2 = 1.0 / (r * r);
-        const double m11 = Pn.var_major[p] + caa * inv_r2;
-        const double m22 = Pn.var_minor[p] + cbb * inv_r2;
-        const double m12 = cab * inv_r2;
+        m11 = Pn.var_major[p] + caa * inv_r2;
+        m22 = Pn.var_minor[p] + cbb * inv_r2;
+        m12 = cab * inv_r2;
         const double upper = fmax(m11, m22) + fabs(m12);
-        const double sf = C.smoothing_factor;
-        const bool far = fmax(fmax(fabs(m11), fabs(m22)), fabs(m12)) < 1e150 &&
-                         theta * theta > sf * sf * fmax(upper, 0.0) * (1.0 + 1e-12);
-        double mu1 = 0.0, mu2 = 0.0, extent = 0.0;
+        far = fmax(fmax(fabs(m11), fabs(m22)), fabs(m12)) < 1e150 &&
+              theta * theta > sf * sf * fmax(upper, 0.0) * (1.0 + 1e-12);
         if (!far) {
           const double half_tr = 0.5 * (m11 + m22);
           const double disc = sqrt(fmax(0.25 * (m11 - m22) * (m11 - m22) + m12 * m12, 0.0));
@@ -629,9 +709,9 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
           mu2 = fmax(half_tr - disc, 1e-16 * mu1 + 1e-300);
           extent = sqrt(fmax(mu1, 0.0));
         }
-        const double u_ = hx * ax + hy * ay + hz * az, v_ = hx * bx + hy * by + hz * bz;
-        double factor;
-        bool done = false;
+        u_ = hx * ax + hy * ay + hz * az;
+        v_ = hx * bx + hy * by + hz * bz;
+        mode = (!far && extent > 0.0 && theta < sf * extent) ? 2 : 3;
         if (C.screen) {
           // pencil_radial_rule (_prompt_screen.py:143-169): two radial nodes where the
           // OM lies within the pencil's angular smoothing extent
@@ -639,46 +719,73 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
           const double disc = sqrt(fmax(0.25 * (m11 - m22) * (m11 - m22) + m12 * m12, 0.0));
           const double r_mu1 = half_tr + disc;
           const double r_mu2 = fmax(half_tr - disc, 1e-16 * r_mu1 + 1e-300);
-          const double r_extent = sqrt(fmax(r_mu1, 0.0));
+          r_extent = sqrt(fmax(r_mu1, 0.0));
           if (r_extent > 0.0 && theta < sf * r_extent) {
             const double st = sine > 0.0 ? theta / sine : 1.0;
             const double uu = u_ * st, vv = v_ * st;
             double sa, ca;
             sincos(0.5 * atan2(2.0 * m12, m11 - m22), &sa, &ca);
-            double w0r, t0r, w1r, t1r;
-            o1_inverse_radius_rule(ca * uu + sa * vv, -sa * uu + ca * vv, r_mu1, r_mu2, S.tangent,
-                                   S.wsec2, C.n_gauss, w0r, t0r, w1r, t1r);
-            if (t0r > 0.0 && t1r < 0.5 * kPi && w0r > 0.0 && w1r >= 0.0) {
-              averaged = theta < r_extent;
-              factor = w0r * t0r / sin(t0r);
-              weight2 = (w1r * t1r / sin(t1r)) / r;
-              theta = t0r;
-              theta2 = t1r;
-              done = true;
-            }
+            arg_u = ca * uu + sa * vv;
+            arg_v = -sa * uu + ca * vv;
+            arg_var_u = r_mu1;
+            arg_var_v = r_mu2;
+            mode = 1;
           }
         }
-        if (done) {
-        } else if (!far && extent > 0.0 && theta < sf * extent) {
-          double sa, ca;
-          sincos(0.5 * atan2(2.0 * m12, m11 - m22), &sa, &ca);
-          const double mean = o1_gauss_inverse_mean(ca * u_ + sa * v_, -sa * u_ + ca * v_, mu1,
-                                                    mu2, S.tangent, S.wsec2, C.n_gauss);
-          factor = mean * (sine > 1e-300 ? theta / sine : 1.0);
-          const bool avg = theta < extent;
-          theta = factor > 1.0 ? asin(fmin(1.0, 1.0 / factor)) : theta;
-          averaged = avg;
+      }
+    }
+    if (!live) mode = 0;  // nothing of this lane is added
+    const unsigned full = 0xffffffffu;
+    double s0n, mass, radial;
+    const unsigned need_rule = __ballot_sync(full, mode == 1);
+    if (need_rule) {
+      o1_node_sums(need_rule, arg_u, arg_v, arg_var_u, arg_var_v, S.tangent, S.wsec2, C.n_gauss,
+                   s0n, mass, radial);
+      if (mode == 1) {
+        double w0r, t0r, w1r, t1r;
+        o1_inverse_radius_rule(arg_u, arg_v, arg_var_u, arg_var_v, s0n, mass, radial, w0r, t0r,
+                               w1r, t1r);
+        if (t0r > 0.0 && t1r < 0.5 * kPi && w0r > 0.0 && w1r >= 0.0) {
+          averaged = theta < r_extent;
+          weight = (w0r * t0r / sin(t0r)) / r;
+          weight2 = (w1r * t1r / sin(t1r)) / r;
+          theta = t0r;
+          theta2 = t1r;
+          mode = 0;
         } else {
-          if (sine <= 1e-300) live = false;
-          const double d2 = u_ * u_ + v_ * v_;
-          factor = 1.0 / sine;
-          if (d2 > 0.0) {
-            const double qf = m11 * u_ * u_ + 2.0 * m12 * u_ * v_ + m22 * v_ * v_;
-            factor *= 1.0 + 0.5 * (3.0 * qf / d2 - (m11 + m22)) / d2;
-          }
+          mode = (!far && extent > 0.0 && theta < sf * extent) ? 2 : 3;
         }
+      }
+    }
+    if (mode == 2) {
+      double sa, ca;
+      sincos(0.5 * atan2(2.0 * m12, m11 - m22), &sa, &ca);
+      arg_u = ca * u_ + sa * v_;
+      arg_v = -sa * u_ + ca * v_;
+      arg_var_u = mu1;
+      arg_var_v = mu2;
+    }
+    const unsigned need_mean = __ballot_sync(full, mode == 2);
+    if (need_mean) {
+      o1_node_sums(need_mean, arg_u, arg_v, arg_var_u, arg_var_v, S.tangent, S.wsec2, C.n_gauss,
+                   s0n, mass, radial);
+      if (mode == 2) {
+        const double mean = o1_gauss_inverse_mean(arg_u, arg_v, arg_var_u, arg_var_v, s0n, mass);
+        const double factor = mean * (sine > 1e-300 ? theta / sine : 1.0);
+        averaged = theta < extent;
+        theta = factor > 1.0 ? asin(fmin(1.0, 1.0 / factor)) : theta;
         weight = factor / r;
       }
+    }
+    if (mode == 3) {
+      if (sine <= 1e-300) live = false;
+      const double d2 = u_ * u_ + v_ * v_;
+      double factor = 1.0 / sine;
+      if (d2 > 0.0) {
+        const double qf = m11 * u_ * u_ + 2.0 * m12 * u_ * v_ + m22 * v_ * v_;
+        factor *= 1.0 + 0.5 * (3.0 * qf / d2 - (m11 + m22)) / d2;
+      }
+      weight = factor / r;
     }
     // _fill_moments_averaged_pair (_prompt_numba.py:1260-1277): the angular powers
     double cpw[5], spw[5];
@@ -712,10 +819,9 @@ __global__ void o1_group_kernel(const lh_order1_config C, const lh_order1_pencil
       if (leader) {
         bool fresh;
         long long* keys = gkeys + (int64_t)w * cap;
-        const int64_t slot = o1_insert(keys, cap, key, fresh);
-        if (slot < 0) {
-          atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
-        } else {
+        const int64_t slot = o1_insert(keys, cap, key, grows + (int64_t)w * cap * kO1MaxValues,
+                                       kO1MaxValues, fresh, status);
+        if (slot >= 0) {
           if (fresh) atomicAdd(gcount + w, 1);
           row = grows + ((int64_t)w * cap + slot) * kO1MaxValues;
         }
@@ -1436,8 +1542,7 @@ extern "C" int lh_order1_pencils(const lh_order1_config* C, const lh_order1_elem
   if (!workspace || workspace_bytes < W.bytes) return LH_ENOMEM;
   cudaMemsetAsync(n_pencils_device, 0, sizeof(int32_t), s);
   if (E->n_el == 0 || E->n_subseg == 0) return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
-  cudaMemsetAsync(W.pkeys, 0xff, sizeof(long long) * ring_cap, s);
-  cudaMemsetAsync(W.prows, 0, sizeof(double) * lh::kO1Moments * ring_cap, s);
+  cudaMemsetAsync(W.pkeys, 0xff, sizeof(long long) * ring_cap, s);  // rows: zeroed on claim
   const int64_t ring_threads = ((E->n_subseg + 31) / 32) * 32 *
                                ((C->ring_nodes + lh::kO1RingBlock - 1) / lh::kO1RingBlock);
   {
@@ -1458,7 +1563,6 @@ extern "C" int lh_order1_pencils(const lh_order1_config* C, const lh_order1_elem
   // the coarse screen: parents (sums of their children) take rows [0, n_parents),
   // children follow with their parent's row
   cudaMemsetAsync(W.parent_keys, 0xff, sizeof(long long) * ring_cap, s);
-  cudaMemsetAsync(W.parent_rows, 0, sizeof(double) * lh::kO1Moments * ring_cap, s);
   cudaMemsetAsync(W.parent_row, 0xff, sizeof(int32_t) * ring_cap, s);
   lh::o1_parent_kernel<<<lh::grid_for(ring_cap, lh::kO1FinishThreads), lh::kO1FinishThreads, 0, s>>>(
       W.pkeys, W.prows, ring_cap, C->pixel_face, C->parent_face, W.parent_keys, W.parent_rows,
@@ -1498,8 +1602,7 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
   if (C->compute_bins) cudaMemsetAsync(bins, 0, sizeof(double) * (size_t)C->n_om * nb, s);
   if (n_work == 0 || n_pencils == 0) return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
   const int64_t cap = C->group_capacity;
-  cudaMemsetAsync(W.gkeys, 0xff, sizeof(long long) * (size_t)n_work * cap, s);
-  cudaMemsetAsync(W.grows, 0, sizeof(double) * lh::kO1MaxValues * (size_t)n_work * cap, s);
+  cudaMemsetAsync(W.gkeys, 0xff, sizeof(long long) * (size_t)n_work * cap, s);  // rows: zeroed on claim
   cudaMemsetAsync(W.gcount, 0, sizeof(int32_t) * (size_t)n_work, s);
   cudaMemsetAsync(W.batch_total, 0, sizeof(int32_t) * 4, s);
   cudaMemsetAsync(W.accum, 0, sizeof(double) * (size_t)n_work * C->n_bands * (3 + 4 * nb + 1), s);
@@ -1512,7 +1615,7 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
     lh::TimedLaunch timed_launch(LH_KT_O1_GROUP, s);
     lh::o1_group_kernel<<<lh::grid_for((int64_t)n_work * n_pencils, 256), 256, group_smem, s>>>(
         *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows, W.gcount,
-        status);
+        status, lh::kernel_units() ? lh::kernel_units() + LH_KT_O1_GROUP : nullptr);
   }
   const size_t sort_smem =
       cap <= lh::kO1SmemSort ? sizeof(unsigned long long) * (size_t)cap : 0;

@@ -19,6 +19,8 @@ struct Pending {
   cudaEvent_t start, stop;
 };
 
+__device__ unsigned long long g_units[LH_KT_COUNT];
+
 std::mutex g_timing_lock;
 bool g_timing_on = false;
 std::vector<Pending> g_pending;
@@ -38,6 +40,16 @@ cudaEvent_t take_event() {
 }  // namespace
 
 namespace lh {
+
+unsigned long long* kernel_units() {
+  static unsigned long long* address = nullptr;
+  if (!address) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_units) != cudaSuccess) return nullptr;
+    address = static_cast<unsigned long long*>(p);
+  }
+  return address;
+}
 
 TimedLaunch::TimedLaunch(int kernel, cudaStream_t stream) : kernel_(kernel), stream_(stream) {
   std::lock_guard<std::mutex> guard(g_timing_lock);
@@ -70,6 +82,24 @@ extern "C" int lh_kernel_timing(int enable) {
   }
   g_pending.clear();
   g_timing_on = enable != 0;
+  if (enable) {  // the unit counters start from zero with the record
+    unsigned long long* units = lh::kernel_units();
+    if (!units || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemset(units, 0, sizeof(unsigned long long) * LH_KT_COUNT) != cudaSuccess ||
+        cudaDeviceSynchronize() != cudaSuccess)
+      return LH_ECUDA;
+  }
+  return LH_OK;
+}
+
+extern "C" int lh_kernel_units_read(int32_t n_kernels, int64_t* units) {
+  if (n_kernels < 0 || (n_kernels && !units)) return LH_EINVAL;
+  unsigned long long host[LH_KT_COUNT];
+  unsigned long long* device = lh::kernel_units();
+  if (!device || cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpy(host, device, sizeof(host), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return LH_ECUDA;
+  for (int k = 0; k < n_kernels; ++k) units[k] = k < LH_KT_COUNT ? (int64_t)host[k] : 0;
   return LH_OK;
 }
 

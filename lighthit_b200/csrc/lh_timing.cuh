@@ -22,4 +22,8 @@ class TimedLaunch {
   bool armed_ = false;
 };
 
+// Device counters of algorithmic work units, one per timed kernel id
+// (LH_KT_*): a kernel adds its units to kernel_units()[id].
+unsigned long long* kernel_units();
+
 }  // namespace lh

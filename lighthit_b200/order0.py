@@ -45,13 +45,17 @@ class Order0Optics:
     """Optical panels, acceptance and OM spheres resident on the device."""
 
     def __init__(self, optics, positions_m, looks, areas_m2, radii_m, alpha, *, order=8,
-                 device="cuda"):
+                 check_order=0, device="cuda"):
+        """``check_order``: a lower Gauss order evaluated beside ``order`` when a
+        call asks for an error estimate (0: none)."""
         import torch
         self.device = torch.device(device)
         positions = np.ascontiguousarray(np.atleast_2d(positions_m), float)
         n = len(positions)
         self.n_om = n
         self.order = int(order)
+        self.check_order = int(check_order)
+        self._source = (optics, positions, looks, areas_m2, radii_m, alpha)
         radii = np.broadcast_to(np.asarray(radii_m, float), (n,))
         if np.any(radii <= 0):
             raise ValueError("the first-entry order 0 needs OM sphere radii > 0")
@@ -63,7 +67,9 @@ class Order0Optics:
             group=optics["group_nodes"], extinction=optics["extinction_nodes"],
             efficiency=optics["efficiency_coefficients"])
         gx, gw = np.polynomial.legendre.leggauss(self.order)
-        arrays.update(gauss_x=gx, gauss_w=gw)
+        cx, cw = (np.polynomial.legendre.leggauss(self.check_order) if self.check_order
+                  else (np.zeros(1), np.zeros(1)))
+        arrays.update(gauss_x=gx, gauss_w=gw, check_x=cx, check_w=cw)
         self._t = {k: torch.tensor(np.ascontiguousarray(v, float), dtype=torch.float64,
                                    device=self.device) for k, v in arrays.items()}
         eff = np.asarray(optics["efficiency_coefficients"], float)
@@ -74,7 +80,18 @@ class Order0Optics:
             len(optics["panel_edges"]), t["panel_edges"].data_ptr(), t["phase"].data_ptr(),
             t["group"].data_ptr(), t["extinction"].data_ptr(), eff.shape[1],
             t["efficiency"].data_ptr(), self.order, t["gauss_x"].data_ptr(),
-            t["gauss_w"].data_ptr())
+            t["gauss_w"].data_ptr(), self.check_order, t["check_x"].data_ptr(),
+            t["check_w"].data_ptr())
+
+    def subset(self, ids, *, order):
+        """These optics for the OMs ``ids`` at Gauss ``order`` (no check order)."""
+        optics, positions, looks, areas, radii, alpha = self._source
+        n = len(positions)
+        ids = np.asarray(ids, np.int64)
+        return Order0Optics(optics, positions[ids], np.atleast_2d(looks)[ids],
+                            np.broadcast_to(np.asarray(areas, float), (n,))[ids],
+                            np.broadcast_to(np.asarray(radii, float), (n,))[ids], alpha,
+                            order=order, device=self.device)
 
     def workspace(self, nbytes):
         """Device scratch of at least ``nbytes`` (kept and grown across calls)."""
@@ -163,7 +180,7 @@ class ElementBatch:
 
 
 def order0(optics: Order0Optics, events, origins=None, edges=None, *, stream=None,
-           check=True):
+           check=True, estimate=False):
     """Order-0 charge (events, OMs) and bins (events, OMs, bins) on the device.
 
     ``events``: element sets (reference ``SpectralLightElements`` or dicts with
@@ -171,6 +188,7 @@ def order0(optics: Order0Optics, events, origins=None, edges=None, *, stream=Non
     (``prompt.py:542-562``). ``edges`` None gives the charge only
     (``PreparedBallistic.charge``); otherwise ``origins`` (events, OMs) are the
     per-OM clocks and the bins are ``PreparedBallistic.bins`` for every OM.
+    ``estimate``: also the charge at the optics' check order (``charge_check``).
     """
     import torch
     dev = optics.device
@@ -194,11 +212,14 @@ def order0(optics: Order0Optics, events, origins=None, edges=None, *, stream=Non
     bins = (torch.empty((E, n, len(edges_np) - 1), dtype=torch.float64, device=dev)
             if want_bins else None)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
+    charge_check = (torch.empty((E, n), dtype=torch.float64, device=dev)
+                    if estimate and optics.check_order > 0 else None)
     t = batch._t
     b = _lib.Order0Batch(E, t["offsets"].data_ptr(), batch.n_elements, *batch.pointers(),
                          origins_t.data_ptr(), len(edges_np), edges_t.data_ptr(),
                          charge.data_ptr(), bins.data_ptr() if bins is not None else None,
-                         status.data_ptr(), None, 0)
+                         status.data_ptr(), None, 0,
+                         charge_check.data_ptr() if charge_check is not None else None)
     lib = _lib.load()
     need = int(lib.lh_order0_workspace_bytes(optics.struct, b))
     if need == 0:
@@ -207,7 +228,7 @@ def order0(optics: Order0Optics, events, origins=None, edges=None, *, stream=Non
     b.workspace, b.workspace_bytes = workspace.data_ptr(), workspace.numel()
     s = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
     _lib.check(lib.lh_order0(optics.struct, b, s), "lh_order0")
-    result = dict(charge=charge, bins=bins, status=status,
+    result = dict(charge=charge, bins=bins, status=status, charge_check=charge_check,
                   _keep=(batch, origins_t, edges_t, workspace))
     if check:
         raise_status(int(status.item()))

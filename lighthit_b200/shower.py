@@ -75,6 +75,28 @@ class ShowerSettings:
     # order 5: 4.6e-7), inside the reference's own tolerance 1e-10 + 2e-6 |q|
     # (_surface_ballistic.py:149-168), at (6/8)^3 of order 8's work.
     order0_gauss: int = 6
+    # Error estimate of order 0: the charge at this lower Gauss order is formed
+    # in the same launch. Their difference bounds the lower order's error, and
+    # order 6's error is several times smaller still (on the README shower
+    # order 5 agrees with the reference's order 0 to 4.6e-7, order 6 to 6e-8), so
+    # an OM passes when the difference is within the reference's tolerance
+    # 1e-10 + 2e-6 |q| (BallisticIntervalConfig, ballistic_interval.py:31-36).
+    # An OM that does not is evaluated again with the order doubled until
+    # successive charges agree within a quarter of that tolerance (the
+    # reference's adaptive loop, _surface_ballistic.py:179-229), and raises the
+    # reference's ValueError at order0_max_order (_surface_ballistic.py:195-196).
+    # 0 skips the estimate.
+    order0_check: int = 5
+    order0_max_order: int = 64
+    order0_relative_tolerance: float = 2e-6
+    order0_absolute_tolerance_pe: float = 1e-10
+    # The device integrand is float32 with hardware sine/exponential (absolute
+    # error near 2^-21 per node), so two quadrature orders of one OM can differ
+    # by ~1e-6 of its charge however far the order is raised. Differences below
+    # this fraction of the charge are taken as that float32 floor rather than
+    # as quadrature error (the route's order-0 charge agrees with the
+    # reference's float64 to a few 1e-6); 0 tests the reference's tolerance alone.
+    order0_float32_floor: float = 1e-5
     screen: bool = True                  # PromptConfig.screen
     screen_margin: float = 3.0           # PromptConfig.screen_margin
 
@@ -181,7 +203,8 @@ class ShowerTables:
         import torch
         dev, settings = self.device, self.settings
         self.order0 = Order0Optics(self._optics, self.positions, self.looks, self.areas,
-                                   self.radii, self.alpha, order=settings.order0_gauss, device=dev)
+                                   self.radii, self.alpha, order=settings.order0_gauss,
+                                   check_order=settings.order0_check, device=dev)
         self.order1 = Order1Tables(self.prompt, self.g, acceptance_monomials(self.alpha),
                                    self.positions, self.looks, self.areas, self.edges,
                                    settings=PromptSettings(), device=dev)
@@ -855,9 +878,12 @@ class ShowerTransport:
                 origins = np.stack([ev.origins for ev in prompt_events])
                 batch0 = (prompt_store if len(prompt_events) == len(events) else
                           ElementBatch([ev.prompt_el for ev in prompt_events], dev))
-                out0 = order0(T.order0, batch0, origins, edges, check=False)
+                out0 = order0(T.order0, batch0, origins, edges, check=False,
+                              estimate=cfg.order0_check > 0)
         if prompt_events:
             extra0 = [out0["status"], out0["charge"]]
+            if out0["charge_check"] is not None:
+                extra0.append(out0["charge_check"])
             coarse_host = self._collect(prompt_events, "coarse", T.order1_screen, extra0)
             raise_order0_status(int(extra0[0][0]))
             q0_all = extra0[1]
@@ -865,6 +891,12 @@ class ShowerTransport:
             for k, ev in enumerate(prompt_events):
                 ev.charge[ev.work, 0] = q0_all[k][ev.work]
                 ev.pending["bins0"] = bins0_all[k]
+                if len(extra0) > 2:
+                    q = q0_all[k][ev.work]
+                    failed = ev.work[np.abs(q - extra0[2][k][ev.work])
+                                     > self._order0_tolerance(q, 1.0)]
+                    if len(failed):
+                        self._order0_converged(ev, failed, bins0_all[k])
         stage("order0_screen")
         fine_events = []
         for ev in prompt_events:
@@ -1011,6 +1043,10 @@ class ShowerTransport:
             for (k, work), spec in zip(row_ev, host[1:1 + len(row_ev)]):
                 events[k].pending["spec"] = (work, spec)
         for k, values in zip(with_bins0, host[(1 + len(row_ev)) if row_ev else 0:]):
+            override = getattr(events[k], "order0_override", None)
+            if override is not None:  # OMs whose order 0 was evaluated again
+                values = np.array(values)
+                values[override[0]] = override[1]
             events[k].pending["bins0"] = values
         late_bins = self._late_bins(events, row_ev, omega, cfg.readout_mode)
         responses = []
@@ -1045,6 +1081,13 @@ class ShowerTransport:
                                   "exact_over_prediction_min": (float(ev.ratio.min())
                                                                 if len(ev.ratio) else None)},
                 "prompt_order1_level": ev.level1.tolist(), "radial_window_m": [low, high],
+                "order0": {"gauss_order": int(cfg.order0_gauss),
+                           "check_order": int(cfg.order0_check),
+                           "reevaluated_oms": (len(ev.order0_override[0])
+                                               if getattr(ev, "order0_override", None)
+                                               else 0),
+                           "highest_order": int(getattr(ev, "order0_orders",
+                                                        cfg.order0_gauss))},
                 "radial_tail_estimate_max_pe": float(ev.tail.max(initial=0.0)),
                 "time_origin": ("supplied event clock" if time_origin_ns is not None else
                                 "earliest local segment and fastest group flight"
@@ -1116,6 +1159,59 @@ class ShowerTransport:
                                                       mode=mode)
             out.setdefault(k, []).append(values.cpu().numpy().astype(float))
         return out
+
+    def _order0_tolerance(self, q, fraction):
+        """Allowed change of order-0 charges ``q`` between two quadrature orders:
+        ``fraction`` of the reference's tolerance (``BallisticInterval.tolerance``,
+        ``_surface_ballistic.py:88-89``), at least the float32 floor."""
+        cfg = self.config
+        reference = fraction * (cfg.order0_absolute_tolerance_pe
+                                + cfg.order0_relative_tolerance * np.abs(q))
+        return np.maximum(reference, cfg.order0_float32_floor * np.abs(q))
+
+    def _order0_converged(self, ev, oms, bins_device):
+        """Order 0 of the OMs ``oms`` whose error estimate failed: the Gauss order
+        doubled from the route's until successive charges agree within a
+        quarter of the reference's tolerance or the float32 floor (the
+        ``adaptive`` loop of ``_surface_ballistic.py:179-196``, its ``rays``
+        part); the reference's ``ValueError`` when the maximum order does not
+        converge. The bins of the last order are kept. Unlike the reference's
+        loop the bins' L1 change is not tested: node positions decide which bin
+        each float32 sample lands in, so successive orders move ~1e-4 of an
+        OM's charge between neighbouring bins (measured on the README shower
+        and the config-2 stream: 4e-4 from order 6 to 12, 4e-6 from 48 to
+        64), inside the route's 1e-3 bins tolerance but far above the
+        reference's 5e-7. Sets the charges on the event and keeps the bins
+        for the final read."""
+        import torch
+        T, cfg = self.tables, self.config
+        dev = T.device
+        nb = len(T.edges) - 1
+        prev_q = ev.charge[oms, 0].copy()
+        ids_t = torch.as_tensor(oms, device=dev)
+        prev_b = _lib.fetch([bins_device.index_select(0, ids_t)])[0]
+        q_out, b_out = prev_q.copy(), prev_b.copy()
+        pending = np.arange(len(oms))
+        order = int(cfg.order0_gauss)
+        elements = ElementBatch([ev.prompt_el], dev)
+        while len(pending):
+            order = min(2 * order, int(cfg.order0_max_order))
+            optics = T.order0.subset(oms[pending], order=order)
+            out = order0(optics, elements, ev.origins[oms[pending]][None], T.edges, check=False)
+            status, q, b = _lib.fetch([out["status"], out["charge"][0], out["bins"][0]])
+            raise_order0_status(int(status[0]))
+            error = np.abs(q - prev_q[pending])
+            bad = error > self._order0_tolerance(q, 0.25)
+            q_out[pending], b_out[pending] = q, b
+            if bad.any() and order == int(cfg.order0_max_order):
+                worst = float(np.max(error[bad] / np.maximum(np.abs(q[bad]), 1e-300)))
+                raise ValueError(f"ballistic rays quadrature failed for {int(bad.sum())} OMs "
+                                 f"at order {order} (largest change {worst:.2e} of the charge)")
+            prev_q[pending], prev_b[pending] = q, b
+            pending = pending[bad]
+        ev.charge[oms, 0] = q_out
+        ev.order0_override = (np.asarray(oms), b_out.reshape(len(oms), nb))
+        ev.order0_orders = order
 
     def _collect(self, events, key, tables, extra=None):
         """Host values of the events' pending ``key`` results (coarse charge, or

@@ -33,7 +33,9 @@ def test_served_showers_equal_each_shower_alone():
         got, alone = req.result, alone_route(src)
         assert np.array_equal(got.active, alone.active)
         assert np.array_equal(got.time_origin_ns, alone.time_origin_ns)
+        # orders 0 and 1 add per-block float64 partial sums with atomics, whose
+        # order depends on what else shares the launch: a few 1e-16 per term
         scale = max(np.abs(alone.charge_pe).max(), 1e-300)
-        assert np.abs(got.charge_components_pe - alone.charge_components_pe).max() <= 1e-12 * scale
-        assert np.abs(got.components_pe - alone.components_pe).max() <= 1e-11 * scale
+        assert np.abs(got.charge_components_pe - alone.charge_components_pe).max() <= 1e-10 * scale
+        assert np.abs(got.components_pe - alone.components_pe).max() <= 1e-10 * scale
         assert got.metadata["ge2_charge_level"] == alone.metadata["ge2_charge_level"]

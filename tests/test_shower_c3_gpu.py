@@ -5,9 +5,13 @@ reference's float64 ``ShowerTransport`` with each readout precision (``-m gpu``)
 node bands, scattering/source degree 16, azimuthal degree 4 (133 source
 channels), 1025 readout nodes, 1 ns bins from -60 to 2000 ns (2060 bins).
 Fixture: ``tests/golden/shower_c3.npz`` (``make_shower_c3_golden.py``): the
-first 12 showers of the seeded config-3 stream (20000 elements each); a shower
-the reference rejects (its order-0 disk quadrature failing to converge) is
-skipped. The showers of a mode run as one stage-major batch.
+first 12 showers of the seeded config-3 stream (20000 elements each). Shower 11
+makes the reference's control-variate order 0 raise (its disk quadrature does
+not converge); the reference's direct ray form, which the device evaluates,
+converges there, so that shower is checked against the CPU oracle's whole route
+(``shower_c3_oracle.npz``, ``make_shower_c3_oracle.py``: the ray form with the
+reference's adaptive order doubling). The showers of a mode run as one
+stage-major batch.
 
 Charges do not depend on the readout precision; bins and the per-order error
 against the reference are reported for FP32, split-BF16 (hi + lo, three
@@ -43,12 +47,23 @@ def stream():
                              charged_track_length_m=s["charged_track_length_m"],
                              elements=s["elements"], seed=s["seed"])
         assert float(el["start_m"].sum() + el["start_ns"].sum()) == float(g[f"s{k}_checksum"])
-        if f"s{k}_raises" in g.files:
-            continue
         kept.append(k)
         sources.append(el)
-    assert len(kept) >= N_SHOWERS - 2
-    return tables, g, kept, sources
+    return tables, merged(g), kept, sources
+
+
+def merged(g):
+    """The reference's fixture with the oracle's response for the shower the
+    reference rejects."""
+    out = dict(g)
+    oracle = np.load(GOLDEN / "shower_c3_oracle.npz")
+    for k in range(N_SHOWERS):
+        if f"s{k}_raises" in g.files:
+            assert float(oracle[f"s{k}_checksum"]) == float(g[f"s{k}_checksum"])
+            for key in ("charge", "active", "origin", "active_ids", "components", "level",
+                        "spectrum"):
+                out[f"s{k}_{key}"] = oracle[f"s{k}_{key}"]
+    return out
 
 
 @pytest.fixture(scope="module", params=["split-bf16", "fp32", "bf16"])

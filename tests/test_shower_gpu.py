@@ -155,3 +155,54 @@ def test_radial_window_counts_bit_exact():
             ref = np.bincount(om, weights=photons[pt] * factor, minlength=T.n_om)
             assert np.abs(far_sum[k, b] - ref).max() <= 2e-7 * max(ref.max(), 1e-300)
     assert n_near.sum() > 0 and n_far.sum() > 0
+
+
+def _readme_shower():
+    el = np.load(GOLDEN / "order0_c0.npz")
+    return {k: np.array(el[k]) for k in ("start_m", "direction", "length_m", "coefficient0",
+                                         "coefficient2", "beta", "start_ns", "end_ns")}
+
+
+def test_order0_error_estimate_raises_like_the_reference():
+    """With a zero tolerance (and no float32 floor) no OM converges: the route
+    doubles the Gauss order of every OM up to its maximum and raises the
+    reference's ValueError (_surface_ballistic.py:195-196)."""
+    from dataclasses import replace
+    from lighthit_b200.shower import ShowerTables, ShowerTransport
+    tables = ShowerTables.synthetic("c0")
+    cfg = replace(tables.settings, order0_relative_tolerance=0.0,
+                  order0_absolute_tolerance_pe=0.0, order0_float32_floor=0.0,
+                  order0_max_order=12)
+    with pytest.raises(ValueError, match="ballistic rays quadrature failed for [0-9]+ OMs at order 12"):
+        ShowerTransport(tables, config=cfg)(_readme_shower())
+
+
+def test_order0_reevaluated_oms_converge_to_the_oracle():
+    """A check rule too coarse for some OMs (Gauss order 2 beside the route's
+    6): those OMs are evaluated again at doubled orders until they converge,
+    and their charges and bins equal the oracle's converged ray quadrature
+    (Gauss order 16)."""
+    from dataclasses import replace
+    from lighthit_b200.shower import ShowerTables, ShowerTransport
+    from oracle import order0 as oracle
+    tables = ShowerTables.synthetic("c0")
+    el = _readme_shower()
+    base = ShowerTransport(tables)(el)
+    cfg = replace(tables.settings, order0_check=2)
+    got = ShowerTransport(ShowerTables.synthetic("c0", settings=cfg))(el)
+    meta = got.metadata["order0"]
+    assert meta["reevaluated_oms"] > 0 and meta["highest_order"] >= 12
+    g = np.load(GOLDEN / "order0_c0.npz")
+    det = dict(positions_m=g["positions_m"], looks=g["looks"], areas_m2=g["areas_m2"],
+               radii_m=g["radii_m"], alpha=g["alpha"])
+    optics = {k: g[k] for k in ("panel_edges", "phase_nodes", "group_nodes", "extinction_nodes",
+                                "efficiency_coefficients")}
+    po, pe = oracle.candidates(g["positions_m"], g["radii_m"], el["start_m"], el["direction"],
+                               el["length_m"], el["coefficient0"], el["beta"], g["phase_nodes"])
+    q16, b16 = oracle.rays(po, pe, det, el, optics, got.time_origin_ns, tables.edges, 16)
+    big = q16 > 1e-6
+    for r in (base, got):
+        assert (np.abs(r.charge_components_pe[big, 0] - q16[big]) / q16[big]).max() < 2e-5
+    on = got.active & big
+    l1 = np.abs(got.components_pe[on, :, 0] - b16[on]).sum(axis=1) / q16[on]
+    assert l1.max() < BINS_L1
