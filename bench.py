@@ -106,7 +106,9 @@ def config_json(pool, steps):
                                     "max": int(max(sizes))},
             "n_om": 384, "omega_nodes": 65, "readout_nodes": 321, "bins": 160,
             "served": {"workers": WORKERS, "max_batch": MAX_BATCH,
-                       "readout": "split-bf16 (fp32 accumulate)"},
+                       "readout": "split-bf16 tcgen05 (fp32 accumulate)",
+                       ">=2 contraction": "split-bf16 tcgen05 (fp32 accumulate)"},
+            "plain": "fp32 CUDA cores, readout and >=2 contraction",
             "l2": "inputs and tables larger than L2 (126 MB): every step streams new showers",
             "parallelism": "replicas"}
 
@@ -264,8 +266,8 @@ def shower_section(args, dev, world):
     from lighthit_b200.serve_shower import ShowerServer
     from lighthit_b200.shower import ShowerSettings, ShowerTables, ShowerTransport
     stream = torch.cuda.current_stream(dev)
-    plain = ShowerTransport(ShowerTables.synthetic("c2", device=dev,
-                                                   settings=ShowerSettings(readout_mode="fp32")))
+    plain = ShowerTransport(ShowerTables.synthetic(
+        "c2", device=dev, settings=ShowerSettings(readout_mode="fp32", contraction_mode="fp32")))
     pool = shower_pool(plain.tables.positions.mean(axis=0))
     resident = [ResidentElements(el, dev) for el in pool]
     server = ShowerServer(lambda: ShowerTransport(ShowerTables.synthetic("c2", device=dev)),
@@ -478,8 +480,8 @@ def ours(args, rank, world, local_rank):
         "steps": s["steps"], "warmup": s["warmup"],
         "ms_per_step": s["served_ms"] / s["steps"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64 geometry and clocks, f64 order 1, f32 order 0 and >=2, "
-                 "split-bf16 readout (f32 accumulate)",
+        "dtype": "f64 geometry and clocks, f64 order 1, f32 order 0, split-bf16 >=2 "
+                 "contraction and readout on the tensor cores (f32 accumulate)",
         "data": "synthetic", "config": config_json(s["pool"], s["steps"]),
         "latency": {"p50_ms": float(np.percentile(s["lat"], 50)),
                     "p99_ms": float(np.percentile(s["lat"], 99)), "requests": len(s["lat"]),

@@ -213,6 +213,24 @@ size_t lh_ge2_batch_slot_bytes(int32_t n);
 int lh_ge2_apply_batch(const lh_ge2_table* t, const lh_ge2_problem* p, int32_t n,
                        void* workspace, size_t workspace_bytes, void* host_slots, void* stream);
 
+/* The same batch contraction on the tensor cores (tcgen05, BF16 operands with
+ * FP32 accumulation in TMEM; mode LH_MODE_SPLIT_BF16 splits every operand into
+ * three BF16 parts, hi + mid + lo, and accumulates the six products down to
+ * float32 rounding, LH_MODE_BF16 multiplies the hi parts alone). The
+ * folded kernels are first packed into the tensor-core operand layout, once per
+ * table: lh_ge2_tc_pack_bytes(t) bytes (0: the table's shape is not supported:
+ * bands x frequencies > 256, pairs > 8 or rows x 8 too wide), filled by
+ * lh_ge2_tc_pack on `stream`. Every problem must compute the table's full
+ * spectrum (n_omega == t->n_omega). `status` (device int32) receives
+ * LH_STATUS_TIMEOUT if a tensor-core pipeline wait gave up. */
+size_t lh_ge2_tc_pack_bytes(const lh_ge2_table* t);
+int lh_ge2_tc_pack(const lh_ge2_table* t, void* packed, size_t packed_bytes, void* stream);
+size_t lh_ge2_tc_workspace_bytes(const lh_ge2_table* t, const lh_ge2_problem* p, int32_t n);
+int lh_ge2_apply_batch_tc(const lh_ge2_table* t, const lh_ge2_problem* p, int32_t n,
+                          int32_t mode, const void* packed, void* workspace,
+                          size_t workspace_bytes, void* host_slots, int32_t* status,
+                          void* stream);
+
 /* ------------------------------------------------------------------ order 0
  * Replaces PreparedBallistic.charge() / .bins(ids, origins, edges)
  * (_surface_ballistic.py:95-118, the first-entry order 0 of transport_prompt,
@@ -574,7 +592,7 @@ enum {
   LH_KT_O1_RING = 1,     /* o1_ring_kernel (lh_order1_pencils)       */
   LH_KT_O1_GROUP = 2,    /* o1_group_kernel (lh_order1_grouped)      */
   LH_KT_O1_BATCH = 3,    /* o1_batch_kernel (lh_order1_grouped)      */
-  LH_KT_GE2_APPLY = 4,   /* ge2_apply_batch_kernel (lh_ge2_apply_batch) */
+  LH_KT_GE2_APPLY = 4,   /* ge2_apply_batch_kernel or ge2_tc_kernel (lh_ge2_apply_batch[_tc]) */
   LH_KT_SRC_GROUP = 5,   /* src_group_kernel (lh_source_compile)     */
   LH_KT_SRC_TRANSFORM = 6, /* src_transform_kernel (lh_source_compile) */
   LH_KT_READOUT = 7,     /* readout_tc_kernel (lh_readout_rows)      */

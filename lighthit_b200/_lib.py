@@ -203,6 +203,12 @@ SIGNATURES = {
     "lh_ge2_batch_slot_bytes": (C.c_size_t, [C.c_int32]),
     "lh_ge2_apply_batch": (C.c_int, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem), C.c_int32, P,
                                      C.c_size_t, P, P]),
+    "lh_ge2_tc_pack_bytes": (C.c_size_t, [C.POINTER(Ge2Table)]),
+    "lh_ge2_tc_pack": (C.c_int, [C.POINTER(Ge2Table), P, C.c_size_t, P]),
+    "lh_ge2_tc_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem),
+                                               C.c_int32]),
+    "lh_ge2_apply_batch_tc": (C.c_int, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem), C.c_int32,
+                                        C.c_int32, P, P, C.c_size_t, P, P, P]),
     "lh_order0_workspace_bytes": (C.c_size_t, [C.POINTER(Order0Optics), C.POINTER(Order0Batch)]),
     "lh_order0": (C.c_int, [C.POINTER(Order0Optics), C.POINTER(Order0Batch), P]),
     "lh_order1_workspace_bytes": (C.c_size_t, [C.POINTER(Order1Config), C.c_int64, C.c_int32]),

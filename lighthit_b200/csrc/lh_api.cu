@@ -254,3 +254,52 @@ extern "C" int lh_ge2_apply_batch(const lh_ge2_table* t, const lh_ge2_problem* p
   if (!workspace || workspace_bytes < lh::ge2_batch_workspace(*t, p, n)) return LH_ENOMEM;
   return lh::ge2_batch_launch(*t, p, n, workspace, host_slots, static_cast<cudaStream_t>(stream));
 }
+
+namespace lh {
+bool ge2_tc_supported(const lh_ge2_table& T, int& halves, int& n_pad_max);
+size_t ge2_tc_pack_bytes(const lh_ge2_table& T);
+int ge2_tc_pack(const lh_ge2_table& T, void* packed, cudaStream_t s);
+size_t ge2_tc_workspace(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n);
+int ge2_tc_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n, int passes,
+                        const void* packed, void* ws, void* host_slots, int32_t* status,
+                        cudaStream_t s);
+}  // namespace lh
+
+extern "C" size_t lh_ge2_tc_pack_bytes(const lh_ge2_table* t) {
+  if (!t || t->n_bands < 1 || t->n_intervals < 1 || t->degree < 0 || t->degree > 16 ||
+      t->n_pairs < 1 || t->n_pairs > 8 || t->n_omega < 1 || !t->coef)
+    return 0;
+  return lh::ge2_tc_pack_bytes(*t);
+}
+
+extern "C" int lh_ge2_tc_pack(const lh_ge2_table* t, void* packed, size_t packed_bytes,
+                              void* stream) {
+  const size_t need = lh_ge2_tc_pack_bytes(t);
+  if (need == 0) return LH_EUNSUPPORTED;
+  if (!packed || packed_bytes < need) return LH_ENOMEM;
+  if (reinterpret_cast<uintptr_t>(packed) % 16) return LH_EINVAL;  // bulk copies start there
+  return lh::ge2_tc_pack(*t, packed, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" size_t lh_ge2_tc_workspace_bytes(const lh_ge2_table* t, const lh_ge2_problem* p,
+                                            int32_t n) {
+  if (!t || !p || n < 1 || n > 65535 || lh_ge2_tc_pack_bytes(t) == 0) return 0;
+  for (int i = 0; i < n; ++i)
+    if (!ge2_valid(t, p + i) || p[i].n_omega != t->n_omega) return 0;
+  return lh::ge2_tc_workspace(*t, p, n);
+}
+
+extern "C" int lh_ge2_apply_batch_tc(const lh_ge2_table* t, const lh_ge2_problem* p, int32_t n,
+                                     int32_t mode, const void* packed, void* workspace,
+                                     size_t workspace_bytes, void* host_slots, int32_t* status,
+                                     void* stream) {
+  if (!t || !p || n < 1 || n > 65535 || !host_slots || !packed || !status) return LH_EINVAL;
+  if (mode != LH_MODE_SPLIT_BF16 && mode != LH_MODE_BF16) return LH_EINVAL;
+  if (lh_ge2_tc_pack_bytes(t) == 0) return LH_EUNSUPPORTED;
+  if (reinterpret_cast<uintptr_t>(packed) % 16) return LH_EINVAL;
+  for (int i = 0; i < n; ++i)
+    if (!ge2_valid(t, p + i) || p[i].n_omega != t->n_omega) return LH_EINVAL;
+  if (!workspace || workspace_bytes < lh::ge2_tc_workspace(*t, p, n)) return LH_ENOMEM;
+  return lh::ge2_tc_batch_launch(*t, p, n, mode == LH_MODE_SPLIT_BF16 ? 6 : 1, packed, workspace,
+                                 host_slots, status, static_cast<cudaStream_t>(stream));
+}

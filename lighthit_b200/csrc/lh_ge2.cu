@@ -469,4 +469,533 @@ int ge2_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n, 
   return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
 }
 
+
+// ------------------------------------------------------------------ tensor cores
+// The contraction on tcgen05 (BF16 operands, FP32 accumulation in TMEM). In
+// the split mode every operand is the sum of three BF16 parts (hi + mid + lo,
+// 24 significant bits, as float32) and six products are accumulated: hi hi,
+// hi mid, mid hi, hi lo, lo hi, mid mid (the rest lie below float32's
+// rounding); the single mode multiplies the hi parts.
+//
+// For interval j and kernel degree l the band-folded coefficients form a real
+// matrix A_jl[(band, w, part)][(pair p, power q)] (part: real or imaginary
+// coefficient; K = 4 x pairs <= 32), and a (OM, point) pair of interval j
+// forms B[(channel row r of degree l)][(p, q)] = F[r][p] t^(3 - q). The
+// product X = A_jl B^T holds, for every source channel row of the pair and
+// every (band, w), the row's F contracted with the cubic radial kernels. The
+// epilogue multiplies each X entry by the row's source channel (complex, per
+// band and frequency) and sums rows and degrees in registers; then the pair's
+// band scale and flight phase give its spectrum, written per pair and summed
+// over points by ge2_tc_reduce_kernel in a fixed order.
+//
+// Layout: M = (band, w) rows in H <= 2 halves of 128 TMEM lanes, each half as
+// a real and an imaginary accumulator; N = channel row x pair columns
+// (column r * kTcSub + i for pair i of a sub-tile). Pairs are bucketed by
+// interval (counting sort); a CTA takes up to kTcPairs pairs of one interval,
+// streams A_jl with one bulk copy per degree (double-buffered) and keeps the
+// pairs' accumulators in registers across degrees.
+constexpr int kTcSub = 8;                   // pairs per MMA sub-tile
+constexpr int kTcSubs = 4;                  // sub-tiles per CTA tile
+constexpr int kTcPairs = kTcSub * kTcSubs;  // pairs per CTA tile
+constexpr int kTcThreads = 256;
+constexpr int kTcK = 32;                                  // K columns (pairs x 4 <= 32)
+constexpr uint32_t kTcTileBytes = 128u * kTcK * 2u;       // one 128 x 32 BF16 operand tile
+constexpr int kTcParts = 3;                               // BF16 parts of a split operand
+
+struct Ge2TcArgs {
+  const Ge2Slot* slots;
+  Ge2Arrays A;
+  const uint8_t* packed;        // [interval][degree] blocks: [hi, lo][half][re, im] tiles
+  const int32_t* sorted;        // global pair ids bucketed by interval
+  const int32_t* sorted_slot;   // their problems
+  const int32_t* bucket_start;  // [n_intervals + 1]
+  const int32_t* tile_start;    // [n_intervals + 1]
+  float2* partial;              // [global pair][band * n_omega + w]
+  int32_t* status;
+  int passes;                   // 6 split-BF16, 1 BF16
+  int halves;                   // H: ceil(bands x omega / 128)
+  int n_pad_max;                // widest sub-tile (16-column multiple)
+  int tmem_cols;                // 256 (two CTAs per SM) or 512
+  int a_buffers;                // 1 with two CTAs per SM, 2 (prefetch) with one
+};
+
+// (A part, B part) of each product of the split mode, largest first.
+__constant__ int kTcPassA[6] = {0, 0, 1, 0, 2, 1};
+__constant__ int kTcPassB[6] = {0, 1, 0, 2, 0, 1};
+
+struct Ge2TcPair {
+  const float2* channels;  // the point's channel block, band 0, channel row 0, w 0
+  int64_t band_stride;     // float2 elements between bands
+  int64_t scale_at;        // g_scale index of band 0
+  int64_t scale_stride;    // between bands
+  int32_t pair;            // global pair id, -1 for an empty place
+  int32_t omega_stride;    // float2 elements between channel rows
+  float t;
+  float pad;
+};
+
+// Whether a table takes the tensor-core path, and its widest sub-tile.
+bool ge2_tc_supported(const lh_ge2_table& T, int& halves, int& n_pad_max) {
+  const int M = T.n_bands * T.n_omega;
+  const int rows_max = 2 * std::min(T.degree, T.max_m) + 1;
+  halves = (M + 127) / 128;
+  n_pad_max = (rows_max * kTcSub + 15) & ~15;
+  return M <= 256 && 4 * T.n_pairs <= kTcK && 2 * halves * n_pad_max <= 512;
+}
+
+size_t ge2_tc_block_bytes(const lh_ge2_table& T, int halves) {
+  (void)T;
+  return (size_t)kTcParts * halves * 2 * kTcTileBytes;
+}
+
+// x = hi + mid + lo, each BF16 (24 significant bits together).
+LH_DEVICE void split3_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& mid, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(x);
+  const float r = x - __bfloat162float(hi);
+  mid = __float2bfloat16_rn(r);
+  lo = __float2bfloat16_rn(r - __bfloat162float(mid));
+}
+
+// Packs the folded coefficients into the operand tiles (no swizzle, K-major
+// 8 x 16-byte core matrices), hi, mid and lo parts.
+__global__ void ge2_tc_pack_kernel(const lh_ge2_table T, int halves, __nv_bfloat16* out) {
+  const int L1 = T.degree + 1, W = T.n_omega, M = T.n_bands * W;
+  const int64_t per_block = (int64_t)halves * 2 * 128 * kTcK;
+  const int64_t total = (int64_t)T.n_intervals * L1 * per_block;
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const int k = (int)(idx % kTcK);
+  const int m = (int)((idx / kTcK) % 128);
+  const int part = (int)((idx / (kTcK * 128)) % 2);
+  const int h = (int)((idx / (kTcK * 256)) % halves);
+  const int64_t jl = idx / per_block;
+  const int l = (int)(jl % L1), j = (int)(jl / L1);
+  const int flat = h * 128 + m;
+  float v = 0.f;
+  if (flat < M && k < 4 * T.n_pairs) {
+    const int lam = flat / W, w = flat % W, pp = k >> 2, q = k & 3;
+    const float2 c = reinterpret_cast<const float2*>(T.coef)
+        [((((int64_t)lam * T.n_intervals + j) * L1 + l) * T.n_pairs * 4 + pp * 4 + q) * W + w];
+    v = part ? c.y : c.x;
+  }
+  __nv_bfloat16 hi, mid, lo;
+  split3_bf16(v, hi, mid, lo);
+  const int64_t tile = (int64_t)(h * 2 + part) * 128 * kTcK;
+  const int64_t at = jl * kTcParts * per_block + tile + tile_offset(m, k);
+  out[at] = hi;
+  out[at + per_block] = mid;
+  out[at + 2 * per_block] = lo;
+}
+
+// Bucket pass 1 and 3 over every pair of every problem, points outermost so
+// that a bucket lists the OMs of one point together: count per interval, then
+// place (warp-aggregated atomics).
+__global__ void ge2_tc_bucket_kernel(const Ge2Slot* slots, Ge2Arrays A, int32_t* counts,
+                                     int32_t* sorted, int32_t* sorted_slot, int fill) {
+  const Ge2Slot& S = slots[blockIdx.y];
+  const int64_t total = (int64_t)S.P.n_om * S.P.n_points;
+  const int64_t rounded = (total + 31) & ~(int64_t)31;
+  const int lane = threadIdx.x & 31;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < rounded;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int j = -1;
+    int64_t idx = 0;
+    if (t < total) {
+      const int64_t c = t / S.P.n_om, d = t % S.P.n_om;
+      idx = d * S.P.n_points + c;
+      j = A.g_j[S.pair_offset + idx];
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, j);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader && j >= 0) base = atomicAdd(counts + j, __popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (fill && j >= 0) {
+      const int pos = base + __popc(peers & ((1u << lane) - 1u));
+      sorted[pos] = (int32_t)(S.pair_offset + idx);
+      sorted_slot[pos] = (int32_t)blockIdx.y;
+    }
+  }
+}
+
+// Bucket starts, tile starts (kTcPairs pairs per tile) and the fill cursors.
+__global__ void ge2_tc_scan_kernel(int n_intervals, int32_t* counts, int32_t* bucket_start,
+                                   int32_t* tile_start) {
+  if (threadIdx.x != 0) return;
+  int32_t at = 0, tiles = 0;
+  for (int j = 0; j < n_intervals; ++j) {
+    const int32_t c = counts[j];
+    bucket_start[j] = at;
+    tile_start[j] = tiles;
+    counts[j] = at;  // the fill pass counts from the bucket's start
+    at += c;
+    tiles += (c + kTcPairs - 1) / kTcPairs;
+  }
+  bucket_start[n_intervals] = at;
+  tile_start[n_intervals] = tiles;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 2)
+ge2_tc_kernel(const lh_ge2_table T, const Ge2TcArgs G) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int H = G.halves;
+  const int parts = G.passes > 1 ? kTcParts : 1;
+  const uint32_t block_bytes = (uint32_t)kTcParts * H * 2u * kTcTileBytes;
+  const uint32_t load_bytes = (uint32_t)parts * H * 2u * kTcTileBytes;
+  uint8_t* s_a0 = smem;
+  uint8_t* s_a1 = smem + (G.a_buffers > 1 ? load_bytes : 0);
+  __nv_bfloat16* s_b = reinterpret_cast<__nv_bfloat16*>(smem + G.a_buffers * load_bytes);
+  const int b_elems = G.n_pad_max * kTcK;
+  Ge2TcPair* s_pair = reinterpret_cast<Ge2TcPair*>(smem + G.a_buffers * load_bytes +
+                                                   (size_t)parts * b_elems * 2);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(s_pair + kTcPairs);  // load[2], mma
+  uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + 3);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    mbar_init(bars + 0, 1);
+    mbar_init(bars + 1, 1);
+    mbar_init(bars + 2, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(s_tmem, (uint32_t)G.tmem_cols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  const int L1 = T.degree + 1, W = T.n_omega, M = T.n_bands * W;
+  const int h = warp >> 2, quarter = warp & 3;
+  const int m = h * 128 + quarter * 32 + lane;
+  const bool m_ok = m < M;
+  const int lam = m_ok ? m / W : 0, wq = m_ok ? m % W : 0;
+  const bool reads = h < H;  // warps of a missing half read no TMEM
+  const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+  const int k_used = 4 * T.n_pairs;
+  const double omega = T.omega[wq];
+  const double inv_speed = 1.0 / T.speed[lam];
+  uint32_t ph_load[2] = {0u, 0u}, ph_mma = 0u;
+  bool failed = false, mma_pending = false;
+  const int n_tiles = G.tile_start[T.n_intervals];
+
+  for (int tile = blockIdx.x; tile < n_tiles && !failed; tile += gridDim.x) {
+    int lo = 0, hi = T.n_intervals;  // the bucket: last j with tile_start[j] <= tile
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (G.tile_start[mid] <= tile) lo = mid; else hi = mid;
+    }
+    const int j = lo;
+    const int first = G.bucket_start[j] + (tile - G.tile_start[j]) * kTcPairs;
+    const int count = min(kTcPairs, G.bucket_start[j + 1] - first);
+    if (tid < kTcPairs) {
+      Ge2TcPair e{};
+      e.pair = -1;
+      if (tid < count) {
+        const int g = G.sorted[first + tid];
+        const Ge2Slot& S = G.slots[G.sorted_slot[first + tid]];
+        const int64_t idx = g - S.pair_offset;
+        const int c = (int)(idx % S.P.n_points);
+        const int64_t pairs = (int64_t)S.P.n_om * S.P.n_points;
+        e.pair = g;
+        e.t = G.A.g_t[g];
+        e.omega_stride = S.P.n_omega_channels;
+        e.band_stride = (int64_t)S.P.n_points * T.nch * S.P.n_omega_channels;
+        e.channels = reinterpret_cast<const float2*>(S.P.channels) +
+                     (int64_t)c * T.nch * S.P.n_omega_channels;
+        e.scale_at = S.pair_offset * T.n_bands + idx;
+        e.scale_stride = pairs;
+      }
+      s_pair[tid] = e;
+    }
+    if (tid == 0) {  // degree 0 of this interval
+      mbar_expect_tx(bars + 0, load_bytes);
+      bulk_g2s(s_a0, G.packed + (size_t)j * L1 * block_bytes, load_bytes, bars + 0);
+    }
+    __syncthreads();
+    float acc_re[kTcSubs][kTcSub], acc_im[kTcSubs][kTcSub];
+#pragma unroll
+    for (int s = 0; s < kTcSubs; ++s)
+#pragma unroll
+      for (int i = 0; i < kTcSub; ++i) acc_re[s][i] = acc_im[s][i] = 0.f;
+
+    for (int l = 0; l < L1 && !failed; ++l) {
+      const int buf = G.a_buffers > 1 ? (l & 1) : 0;
+      uint8_t* s_a = buf ? s_a1 : s_a0;
+      const int keep = min(l, T.max_m), nr = 2 * keep + 1, row0 = T.starts[l];
+      const int n_cols = nr * kTcSub, n_pad = (n_cols + 15) & ~15;
+      if (G.a_buffers > 1 && tid == 0 && l + 1 < L1) {
+        // the next degree into the other buffer (its MMAs are done)
+        mbar_expect_tx(bars + (buf ^ 1), load_bytes);
+        bulk_g2s(buf ? s_a0 : s_a1, G.packed + ((size_t)j * L1 + l + 1) * block_bytes,
+                 load_bytes, bars + (buf ^ 1));
+      }
+      bool ok = mbar_wait(bars + buf, ph_load[buf]);
+      ph_load[buf] ^= 1u;
+      if (__syncthreads_or(!ok)) { failed = true; break; }
+#pragma unroll
+      for (int s = 0; s < kTcSubs; ++s) {
+        if (failed) continue;
+        if (s * kTcSub >= count) continue;  // the same for the whole CTA
+        // B of sub-tile s: column n = r * kTcSub + i, K index k = 4 p + q
+        for (int e = tid; e < n_pad * kTcK; e += kTcThreads) {
+          const int n = e / kTcK, k = e % kTcK;
+          float v = 0.f;
+          if (n < n_cols && k < k_used) {
+            const Ge2TcPair& P = s_pair[s * kTcSub + n % kTcSub];
+            if (P.pair >= 0) {
+              const int r = n / kTcSub, pp = k >> 2, q = k & 3;
+              float power = 1.f;
+              for (int u = q; u < 3; ++u) power *= P.t;
+              v = G.A.g_F[((int64_t)P.pair * T.nch + row0 + r) * T.n_pairs + pp] * power;
+            }
+          }
+          __nv_bfloat16 bh, bm, bl;
+          split3_bf16(v, bh, bm, bl);
+          const int off = ((k >> 3) * n_pad + n) * 8 + (k & 7);
+          s_b[off] = bh;
+          if (parts > 1) {
+            s_b[b_elems + off] = bm;
+            s_b[2 * b_elems + off] = bl;
+          }
+        }
+        fence_proxy_async();  // generic-proxy smem writes -> visible to the tensor core
+        __syncthreads();
+        tc_fence_after();
+        if (tid == 0) {
+          const uint32_t idesc = instr_desc_bf16_f32(128, n_pad);
+          const uint32_t lbo_a = 128u * 16u, lbo_b = (uint32_t)n_pad * 16u;
+          for (int hh = 0; hh < H; ++hh)
+            for (int part = 0; part < 2; ++part) {
+              const uint32_t d = tmem + (uint32_t)((hh * 2 + part) * n_pad);
+              int first_mma = 1;
+              for (int pass = 0; pass < G.passes; ++pass) {
+                const uint8_t* pa =
+                    s_a + (size_t)((kTcPassA[pass] * H + hh) * 2 + part) * kTcTileBytes;
+                const uint8_t* pb =
+                    reinterpret_cast<const uint8_t*>(s_b + kTcPassB[pass] * b_elems);
+                for (int kk = 0; kk < kTcK / 16; ++kk) {
+                  const uint64_t da = smem_desc_kmajor(pa + kk * 2 * lbo_a, lbo_a, 128);
+                  const uint64_t db = smem_desc_kmajor(pb + kk * 2 * lbo_b, lbo_b, 128);
+                  tc_mma_bf16(d, da, db, idesc, first_mma ? 0u : 1u);
+                  first_mma = 0;
+                }
+              }
+            }
+          tc_commit(bars + 2);
+        }
+        mma_pending = true;
+        ok = mbar_wait(bars + 2, ph_mma);
+        ph_mma ^= 1u;
+        if (__syncthreads_or(!ok)) { failed = true; continue; }
+        mma_pending = false;
+        tc_fence_after();
+        if (reads) {
+          for (int r = 0; r < nr; ++r) {
+            float xr[kTcSub], xi[kTcSub];
+            tmem_ld8(lane_base + (uint32_t)((h * 2) * n_pad + r * kTcSub), xr);
+            tmem_ld8(lane_base + (uint32_t)((h * 2 + 1) * n_pad + r * kTcSub), xi);
+            if (m_ok) {
+#pragma unroll
+              for (int i = 0; i < kTcSub; ++i) {
+                const Ge2TcPair& P = s_pair[s * kTcSub + i];
+                if (P.pair < 0) continue;
+                const float2 ch =
+                    P.channels[lam * P.band_stride + (int64_t)(row0 + r) * P.omega_stride + wq];
+                acc_re[s][i] += ch.x * xr[i] - ch.y * xi[i];
+                acc_im[s][i] += ch.x * xi[i] + ch.y * xr[i];
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        __syncthreads();  // TMEM and the B tile are free for the next sub-tile
+      }
+      if (G.a_buffers == 1 && tid == 0 && l + 1 < L1 && !failed) {
+        // one buffer: the next degree once this degree's MMAs are done
+        mbar_expect_tx(bars + 0, load_bytes);
+        bulk_g2s(s_a0, G.packed + ((size_t)j * L1 + l + 1) * block_bytes, load_bytes, bars + 0);
+      }
+    }
+    // the pairs' spectra: band scale and flight phase e^{i w r / v}
+    if (!failed && m_ok) {
+#pragma unroll
+      for (int s = 0; s < kTcSubs; ++s)
+#pragma unroll
+        for (int i = 0; i < kTcSub; ++i) {
+          const Ge2TcPair& P = s_pair[s * kTcSub + i];
+          if (P.pair < 0) continue;
+          const float sc = G.A.g_scale[P.scale_at + lam * P.scale_stride];
+          float sv = 0.f, cv = 1.f;
+          if (T.flight) {
+            const double turns = omega * G.A.g_r[P.pair] * inv_speed * (1.0 / (2 * kPi));
+            sincospif(2.f * (float)(turns - rint(turns)), &sv, &cv);
+          }
+          G.partial[(int64_t)P.pair * M + m] =
+              make_float2(sc * (acc_re[s][i] * cv - acc_im[s][i] * sv),
+                          sc * (acc_re[s][i] * sv + acc_im[s][i] * cv));
+        }
+    }
+    __syncthreads();  // the pair table is rewritten by the next tile
+  }
+  if (failed && tid == 0) atomicOr(reinterpret_cast<unsigned*>(G.status), LH_STATUS_TIMEOUT);
+  // nothing in flight may outlive the TMEM allocation (bounded waits)
+  if (mma_pending) mbar_wait(bars + 2, ph_mma);
+  for (int b = 0; b < G.a_buffers; ++b)  // a prefetched degree that was never waited for
+    if (failed) mbar_wait(bars + b, ph_load[b]);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, (uint32_t)G.tmem_cols);
+}
+
+// result[d][w] = e^{i w ref} * sum over points (in order) and bands of the pairs' spectra.
+__global__ void ge2_tc_reduce_kernel(const lh_ge2_table T, const Ge2Slot* slots, Ge2Arrays A,
+                                     const float2* partial) {
+  const Ge2Slot& S = slots[blockIdx.y];
+  const int W = S.P.n_omega, M = T.n_bands * T.n_omega;
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)S.P.n_om * W) return;
+  const int d = (int)(idx / W), w = (int)(idx % W);
+  double re = 0.0, im = 0.0;
+  for (int c = 0; c < S.P.n_points; ++c) {
+    const int64_t g = S.pair_offset + (int64_t)d * S.P.n_points + c;
+    if (A.g_j[g] < 0) continue;
+    for (int lam = 0; lam < T.n_bands; ++lam) {
+      const float2 v = partial[g * M + lam * T.n_omega + w];
+      re += v.x;
+      im += v.y;
+    }
+  }
+  const double ang = T.omega[w] * S.P.reference_ns;
+  const double c = cos(ang), s = sin(ang);
+  S.P.result[2 * idx] = re * c - im * s;
+  S.P.result[2 * idx + 1] = re * s + im * c;
+}
+
+size_t ge2_tc_smem_bytes(int halves, int n_pad_max, int parts, int a_buffers) {
+  return (size_t)a_buffers * parts * halves * 2 * kTcTileBytes +
+         (size_t)parts * n_pad_max * kTcK * 2 + sizeof(Ge2TcPair) * kTcPairs +
+         3 * sizeof(uint64_t) + 16;
+}
+
+size_t ge2_tc_pack_bytes(const lh_ge2_table& T) {
+  int halves, n_pad_max;
+  if (!ge2_tc_supported(T, halves, n_pad_max)) return 0;
+  return (size_t)T.n_intervals * (T.degree + 1) * ge2_tc_block_bytes(T, halves);
+}
+
+int ge2_tc_pack(const lh_ge2_table& T, void* packed, cudaStream_t s) {
+  int halves, n_pad_max;
+  if (!ge2_tc_supported(T, halves, n_pad_max)) return LH_EUNSUPPORTED;
+  const int64_t total = (int64_t)T.n_intervals * (T.degree + 1) * halves * 2 * 128 * kTcK;
+  ge2_tc_pack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(
+      T, halves, static_cast<__nv_bfloat16*>(packed));
+  return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+}
+
+// Workspace of the tensor-core batch: the batch layout of ge2_batch_workspace,
+// then the bucket arrays, the sorted pairs and the per-pair spectra.
+size_t ge2_tc_workspace(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n) {
+  size_t pairs = 0;
+  for (int i = 0; i < n; ++i) pairs += (size_t)P[i].n_om * P[i].n_points;
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  return ge2_batch_workspace(T, P, n) + 3 * up(sizeof(int32_t) * (T.n_intervals + 1)) +
+         2 * up(sizeof(int32_t) * pairs) + up(sizeof(float2) * pairs * T.n_bands * T.n_omega);
+}
+
+int ge2_tc_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t n, int passes,
+                        const void* packed, void* ws, void* host_slots, int32_t* status,
+                        cudaStream_t s) {
+  int halves, n_pad_max;
+  if (!ge2_tc_supported(T, halves, n_pad_max)) return LH_EUNSUPPORTED;
+  auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
+  Ge2Slot* hs = static_cast<Ge2Slot*>(host_slots);
+  size_t pairs = 0;
+  int64_t max_pairs = 0, max_outs = 0;
+  for (int i = 0; i < n; ++i) {
+    if (P[i].n_omega != T.n_omega) return LH_EINVAL;  // full spectra only
+    hs[i].P = P[i];
+    hs[i].pair_offset = (int64_t)pairs;
+    hs[i].partial_offset = 0;
+    hs[i].chunks = 0;
+    const int64_t pp = (int64_t)P[i].n_om * P[i].n_points;
+    pairs += pp;
+    max_pairs = std::max(max_pairs, pp);
+    max_outs = std::max(max_outs, (int64_t)P[i].n_om * P[i].n_omega);
+  }
+  uint8_t* p = static_cast<uint8_t*>(ws);
+  Ge2Slot* slots = reinterpret_cast<Ge2Slot*>(p); p += up(sizeof(Ge2Slot) * (size_t)n);
+  Ge2Arrays A;
+  A.g_j = reinterpret_cast<int*>(p); p += up(pairs * 4);
+  A.g_t = reinterpret_cast<float*>(p); p += up(pairs * 4);
+  A.g_r = reinterpret_cast<double*>(p); p += up(pairs * 8);
+  A.g_scale = reinterpret_cast<float*>(p); p += up(pairs * T.n_bands * 4);
+  A.g_F = reinterpret_cast<float*>(p); p += up(pairs * T.nch * T.n_pairs * 4);
+  A.partial = nullptr;
+  // the CUDA-core path's chunk partials are not used here
+  p = static_cast<uint8_t*>(ws) + ge2_batch_workspace(T, P, n);
+  int32_t* counts = reinterpret_cast<int32_t*>(p); p += up(sizeof(int32_t) * (T.n_intervals + 1));
+  int32_t* bucket_start = reinterpret_cast<int32_t*>(p); p += up(sizeof(int32_t) * (T.n_intervals + 1));
+  int32_t* tile_start = reinterpret_cast<int32_t*>(p); p += up(sizeof(int32_t) * (T.n_intervals + 1));
+  int32_t* sorted = reinterpret_cast<int32_t*>(p); p += up(sizeof(int32_t) * pairs);
+  int32_t* sorted_slot = reinterpret_cast<int32_t*>(p); p += up(sizeof(int32_t) * pairs);
+  float2* partial = reinterpret_cast<float2*>(p);
+  if (cudaMemcpyAsync(slots, hs, sizeof(Ge2Slot) * (size_t)n, cudaMemcpyHostToDevice, s) !=
+      cudaSuccess)
+    return LH_ECUDA;
+  if (max_outs == 0) return LH_OK;
+  if (max_pairs == 0) {  // no points anywhere: every result is zero
+    for (int i = 0; i < n; ++i)
+      cudaMemsetAsync(P[i].result, 0, sizeof(double) * 2 * (size_t)P[i].n_om * P[i].n_omega, s);
+    return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+  }
+  ge2_geometry_batch_kernel<<<dim3((unsigned)((max_pairs + 127) / 128), n), 128, 0, s>>>(T, slots,
+                                                                                      A);
+  cudaMemsetAsync(counts, 0, sizeof(int32_t) * (T.n_intervals + 1), s);
+  const unsigned bucket_blocks = (unsigned)std::min<int64_t>((max_pairs + 255) / 256, 148 * 4);
+  ge2_tc_bucket_kernel<<<dim3(bucket_blocks, n), 256, 0, s>>>(slots, A, counts, sorted,
+                                                              sorted_slot, 0);
+  ge2_tc_scan_kernel<<<1, 32, 0, s>>>(T.n_intervals, counts, bucket_start, tile_start);
+  ge2_tc_bucket_kernel<<<dim3(bucket_blocks, n), 256, 0, s>>>(slots, A, counts, sorted,
+                                                              sorted_slot, 1);
+  Ge2TcArgs G;
+  G.slots = slots;
+  G.A = A;
+  G.packed = static_cast<const uint8_t*>(packed);
+  G.sorted = sorted;
+  G.sorted_slot = sorted_slot;
+  G.bucket_start = bucket_start;
+  G.tile_start = tile_start;
+  G.partial = partial;
+  G.status = status;
+  G.passes = passes;
+  G.halves = halves;
+  G.n_pad_max = n_pad_max;
+  // Two CTAs per SM (one overlapping the other's waits) when the accumulators
+  // fit 256 TMEM columns and one coefficient buffer each fits half the shared
+  // memory; otherwise one CTA per SM with 512 columns and a prefetch buffer.
+  const int parts = passes > 1 ? kTcParts : 1;
+  const bool two = 2 * halves * n_pad_max <= 256 &&
+                   ge2_tc_smem_bytes(halves, n_pad_max, parts, 1) <= 110 * 1024;
+  G.tmem_cols = two ? 256 : 512;
+  G.a_buffers = two ? 1 : 2;
+  const size_t smem = ge2_tc_smem_bytes(halves, n_pad_max, parts, G.a_buffers);
+  if (smem > 227 * 1024) return LH_EUNSUPPORTED;
+  if (cudaFuncSetAttribute(ge2_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return LH_ECUDA;
+  // persistent CTAs (one or two per SM); tiles beyond the grid are taken in turn
+  const int64_t tile_bound = (int64_t)(pairs + kTcPairs - 1) / kTcPairs + T.n_intervals;
+  const unsigned grid =
+      (unsigned)std::max<int64_t>(1, std::min<int64_t>(tile_bound, two ? 2 * 148 : 148));
+  {
+    lh::TimedLaunch timed_launch(LH_KT_GE2_APPLY, s);
+    ge2_tc_kernel<<<grid, kTcThreads, smem, s>>>(T, G);
+  }
+  ge2_tc_reduce_kernel<<<dim3((unsigned)((max_outs + 255) / 256), n), 256, 0, s>>>(T, slots, A,
+                                                                                   partial);
+  return cudaGetLastError() == cudaSuccess ? LH_OK : LH_ECUDA;
+}
+
 }  // namespace lh

@@ -583,6 +583,9 @@ LH_DEVICE bool o1_refined(const lh_order1_config& C, const lh_order1_pencil_tabl
   return theta < 0.5 * kPi && theta * theta < sf * sf * extent2;
 }
 
+constexpr int kO1GroupOms = 8;       // work OMs per warp chunk of the group stage
+constexpr int kO1PencilFields = 20;  // float64 fields of a pencil read by the group stage
+
 struct O1GroupShared {
   double tangent[kO1MaxGauss], wsec2[kO1MaxGauss];
   double coef[kO1MaxMono];
@@ -591,7 +594,7 @@ struct O1GroupShared {
 
 // One thread per (work OM, pencil): _grouped_pencils_order1_block's pencil
 // loop (_prompt_numba.py:1827-1921) with the generic moment layout.
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 2)
 o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
                                 int32_t n_pencils_bound, const int32_t* n_pencils_device,
                                 const int32_t* work, int32_t n_work,
@@ -618,27 +621,46 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
       n_pencils_device ? min(*n_pencils_device, n_pencils_bound) : n_pencils_bound;
   const int64_t total = (int64_t)n_work * n_pencils;
   if (units && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(units, (unsigned long long)total);
-  const int lane = threadIdx.x & 31;
-  extern __shared__ double o1g_stage[];  // [warp][32][n_values]
-  double* stage = o1g_stage + (threadIdx.x >> 5) * 32 * n_values;
-  // whole warps iterate together: lanes past the end compute on pencil 0 of OM
-  // 0 and take no part in any group
-  for (int64_t item0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x - lane; item0 < total;
-       item0 += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t item = item0 + lane;
-    bool live = item < total;
-    const int w = live ? (int)(item / n_pencils) : 0;
-    const int p = live ? (int)(item - (int64_t)w * n_pencils) : 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // [warp][32][n_values] group staging, then [warp][field][32] pencil fields
+  extern __shared__ double o1g_stage[];
+  double* stage = o1g_stage + warp * 32 * n_values;
+  double* pen = o1g_stage + (blockDim.x >> 5) * 32 * n_values + warp * 32 * kO1PencilFields + lane;
+  // A warp takes 32 consecutive pencils and kO1GroupOms consecutive work OMs:
+  // each lane reads its pencil once (into shared memory) and evaluates it
+  // against every OM of the chunk in turn. Lanes past the last pencil compute
+  // on pencil 0 and take no part in any group.
+  const int64_t pblocks = ((int64_t)n_pencils + 31) / 32;
+  const int64_t chunks = pblocks * ((n_work + kO1GroupOms - 1) / kO1GroupOms);
+  const int64_t warps_total = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t chunk = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp; chunk < chunks;
+       chunk += warps_total) {
+    const int64_t p_raw = (chunk % pblocks) * 32 + lane;
+    const int w_first = (int)(chunk / pblocks) * kO1GroupOms;
+    const bool p_ok = p_raw < n_pencils;
+    const int p = p_ok ? (int)p_raw : 0;
+    pen[0] = Pn.position[3 * p]; pen[32] = Pn.position[3 * p + 1]; pen[64] = Pn.position[3 * p + 2];
+    pen[96] = Pn.time[p];
+    pen[128] = Pn.direction[3 * p]; pen[160] = Pn.direction[3 * p + 1];
+    pen[192] = Pn.direction[3 * p + 2];
+    pen[224] = Pn.major[3 * p]; pen[256] = Pn.major[3 * p + 1]; pen[288] = Pn.major[3 * p + 2];
+    pen[320] = Pn.var_major[p]; pen[352] = Pn.var_minor[p];
+    for (int f = 0; f < 6; ++f) pen[(12 + f) * 32] = Pn.pos_cov[6 * p + f];
+    pen[576] = Pn.w0[p]; pen[608] = Pn.w2[p];
+    const int parent = C.screen ? Pn.parent[p] : -1;
+    for (int k = 0; k < kO1GroupOms; ++k) {
+    const int w = w_first + k;
+    if (w >= n_work) break;  // the same for the whole warp
+    bool live = p_ok;
     const int d = work[w];
     const double rx = C.om_pos[3 * d], ry = C.om_pos[3 * d + 1], rz = C.om_pos[3 * d + 2];
     const double nx = C.om_look[3 * d], ny = C.om_look[3 * d + 1], nz = C.om_look[3 * d + 2];
     // _prepare_receiver_geometry (_prompt_numba.py:1590-1612)
-    const double dx = rx - Pn.position[3 * p], dy = ry - Pn.position[3 * p + 1],
-                 dz = rz - Pn.position[3 * p + 2];
+    const double dx = rx - pen[0], dy = ry - pen[32], dz = rz - pen[64];
     const double r = sqrt(dx * dx + dy * dy + dz * dz);
     const double hx = dx / r, hy = dy / r, hz = dz / r;
     // the screen's charge batches ignore emission time (_prompt_screen.py:220-229)
-    const double t_emit = C.screen ? 0.0 : Pn.time[p] - origins[d];
+    const double t_emit = C.screen ? 0.0 : pen[96] - origins[d];
     const double tau = C.screen ? 0.0 : t_emit + r / C.speed_ref;
     const double log_r = log(r);
     const long long key0 = (long long)floor(log_r / C.log_r_step) + (1ll << 20);
@@ -646,15 +668,17 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
         min(max((long long)floor(tau / C.tau_step) + (1ll << 20), 0ll), (1ll << 21) - 1);
     const long long base = C.screen ? key0 * 2 * theta_bins : ((key1 << 21) + key0) * 2 * theta_bins;
     if (C.screen && live) {  // a parent unless the OM looks into it, else its children
-      const int parent = Pn.parent[p];
       // rows of a table whose stage A overflowed are not written (the caller
       // redoes it): an index outside the table is never followed
       if (parent >= n_pencils || parent < -1) live = false;
       else live = parent < 0 ? !o1_refined(C, Pn, p, rx, ry, rz)
                              : o1_refined(C, Pn, parent, rx, ry, rz);
     }
+    // children stand in for their parent only where the OM looks into it, so
+    // most screen warps over children have nothing to add
+    if (C.screen && !__any_sync(0xffffffffu, live)) continue;
     // _pencil_frame_from_ray_cached_look (_prompt_numba.py:594-606)
-    const double sx = Pn.direction[3 * p], sy = Pn.direction[3 * p + 1], sz = Pn.direction[3 * p + 2];
+    const double sx = pen[128], sy = pen[160], sz = pen[192];
     const double c1 = sx * nx + sy * ny + sz * nz;
     const double cosine = hx * sx + hy * sy + hz * sz;
     const double qx = hx - cosine * sx, qy = hy - cosine * sy, qz = hz - cosine * sz;
@@ -664,8 +688,8 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
     const bool backward = theta > 0.5 * kPi;
     double weight = 0.0, weight2 = 0.0, theta2 = theta;
     bool averaged = false;
-    const double ax = Pn.major[3 * p], ay = Pn.major[3 * p + 1], az = Pn.major[3 * p + 2];
-    const double* cov = Pn.pos_cov + 6 * p;
+    const double ax = pen[224], ay = pen[256], az = pen[288];
+    const double cov[6] = {pen[384], pen[416], pen[448], pen[480], pen[512], pen[544]};
     // _prepare_pencil_shape (_prompt_numba.py:1347-1370)
     const double bx = sy * az - sz * ay, by = sz * ax - sx * az, bz = sx * ay - sy * ax;
     const double trace = cov[0] + cov[1] + cov[2];
@@ -681,7 +705,7 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
     if (backward) {
       weight = 1.0 / r;
     } else {
-      const double bound = Pn.var_major[p] + Pn.var_minor[p] + trace / (r * r);
+      const double bound = pen[320] + pen[352] + trace / (r * r);
       if (sine > 1e-300 && bound < 1e-4 * sine * sine) {
         weight = (1.0 / sine) / r;
       } else {
@@ -696,8 +720,8 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
                            ay * (cov[3] * bx + cov[1] * by + cov[5] * bz) +
                            az * (cov[4] * bx + cov[5] * by + cov[2] * bz);
         const double inv_r2 = 1.0 / (r * r);
-        m11 = Pn.var_major[p] + caa * inv_r2;
-        m22 = Pn.var_minor[p] + cbb * inv_r2;
+        m11 = pen[320] + caa * inv_r2;
+        m22 = pen[352] + cbb * inv_r2;
         m12 = cab * inv_r2;
         const double upper = fmax(m11, m22) + fabs(m12);
         far = fmax(fmax(fabs(m11), fabs(m22)), fabs(m12)) < 1e150 &&
@@ -826,7 +850,7 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
           row = grows + ((int64_t)w * cap + slot) * kO1MaxValues;
         }
       }
-      const double field0 = wn * Pn.w0[p], field2 = wn * Pn.w2[p];
+      const double field0 = wn * pen[576], field2 = wn * pen[608];
       double omega = 0.0;
       double* mine = stage + lane * n_values;
       for (int m = 0; m < nm; ++m) {
@@ -844,6 +868,7 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
       mine[2 * nm + 5] = omega * tau * tau;
       o1_warp_group_add(stage, n_values, group, leader, row);
     }
+    }  // OMs of the chunk
   }
 }
 
@@ -1606,14 +1631,19 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
   cudaMemsetAsync(W.gcount, 0, sizeof(int32_t) * (size_t)n_work, s);
   cudaMemsetAsync(W.batch_total, 0, sizeof(int32_t) * 4, s);
   cudaMemsetAsync(W.accum, 0, sizeof(double) * (size_t)n_work * C->n_bands * (3 + 4 * nb + 1), s);
-  const size_t group_smem = sizeof(double) * 32 * (256 / 32) * (2 * C->n_mono + 6);
+  const size_t group_smem =
+      sizeof(double) * 32 * (256 / 32) * (2 * C->n_mono + 6 + lh::kO1PencilFields);
   if (group_smem > 48 * 1024 &&
       cudaFuncSetAttribute(lh::o1_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)group_smem) != cudaSuccess)
     return LH_ECUDA;
   {
     lh::TimedLaunch timed_launch(LH_KT_O1_GROUP, s);
-    lh::o1_group_kernel<<<lh::grid_for((int64_t)n_work * n_pencils, 256), 256, group_smem, s>>>(
+    // persistent: two resident CTAs per SM take the warp chunks in turn (the
+    // host's pencil count is the table's capacity, far above the pencils a
+    // shower makes, so a grid sized from it would mostly launch idle CTAs)
+    const int group_grid = std::min(lh::grid_for((int64_t)n_work * n_pencils, 256), 148 * 2);
+    lh::o1_group_kernel<<<group_grid, 256, group_smem, s>>>(
         *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows, W.gcount,
         status, lh::kernel_units() ? lh::kernel_units() + LH_KT_O1_GROUP : nullptr);
   }

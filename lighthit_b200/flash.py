@@ -47,6 +47,13 @@ class FlashTable:
                    np.asarray(z["moments"]), medium, str(z["radial_phase"]), int(z["degree"]))
 
     @classmethod
+    def from_cache_file(cls, path):
+        """From the reference's ``transport-<key>.npz`` (``ResponseCache.save``,
+        ``cache.py:485-507``), read without the reference."""
+        from .formats import load_response_cache
+        return load_response_cache(path)
+
+    @classmethod
     def from_cache(cls, cache):
         """From a reference ``ResponseCache`` object (attributes read by name)."""
         m = cache.medium

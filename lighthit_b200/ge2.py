@@ -9,7 +9,12 @@ The band-folded kernels (``ShowerTransport.tables()['folded']``,
 read-only as complex64 ``[band][interval][l][pair][power][omega]``. Per call
 the host only rotates the points and OMs into the source's axis frame
 (float64, O(points + OMs)); the phase alignment of the band sources, the
-geometry (float64) and the contraction (float32) run in ``liblh_b200.so``.
+geometry (float64) and the contraction run in ``liblh_b200.so``: float32 on
+the CUDA cores (``mode="fp32"``, and every zero-frequency apply), or on the
+tensor cores with BF16 operands and float32 accumulation (``"split-bf16"``:
+hi + mid + lo parts, six products, float32 accuracy; ``"bf16"``: one
+product), for which the folded kernels are packed once into the tcgen05
+operand layout.
 """
 from __future__ import annotations
 
@@ -113,15 +118,38 @@ class Ge2Table:
             self._alpha.data_ptr(), self._starts.data_ptr(), self._norm.data_ptr(), self.jmax,
             int(self.flight))
         self._workspace = None
+        self._tc_packed = None
+
+    def tc_packed(self):
+        """The folded kernels in the tensor-core operand layout (packed on the
+        device once), or None when the table's shape does not fit that path."""
+        import torch
+        if self._tc_packed is None:
+            lib = _lib.load()
+            need = int(lib.lh_ge2_tc_pack_bytes(self.struct))
+            if need == 0:
+                self._tc_packed = False
+            else:
+                packed = torch.empty(need, dtype=torch.uint8, device=self.device)
+                _lib.check(lib.lh_ge2_tc_pack(self.struct, packed.data_ptr(), need,
+                                              _lib.stream_ptr(torch.cuda.current_stream(
+                                                  self.device))), "lh_ge2_tc_pack")
+                self._tc_packed = packed
+        return self._tc_packed if self._tc_packed is not False else None
 
     @classmethod
     def load(cls, path, alpha, **kw):
         return cls(dict(np.load(path)), alpha, **kw)
 
     def band(self, b):
-        """A view of node band ``b`` alone (for bands whose point sets differ)."""
+        """A view of node band ``b`` alone (for bands whose point sets differ),
+        made once per band and kept with its own workspace and packed kernels."""
         import copy
+        views = self.__dict__.setdefault("_band_views", {})
+        if b in views:
+            return views[b]
         view = copy.copy(self)
+        view._band_views = {}
         per_band = self._coef[0].numel() * self._coef.element_size()
         st = _lib.Ge2Table()
         C.pointer(st)[0] = self.struct
@@ -132,6 +160,8 @@ class Ge2Table:
         view.struct = st
         view.n_bands = 1
         view._workspace = None
+        view._tc_packed = None
+        views[b] = view
         return view
 
     def radial_limits(self):
@@ -220,10 +250,14 @@ class Ge2Table:
         return self.apply_batch([(sources, positions, looks, out_scale, window)],
                                 zero_frequency=zero_frequency, stream=stream)[0]
 
-    def apply_batch(self, items, *, zero_frequency=False, stream=None):
+    def apply_batch(self, items, *, zero_frequency=False, stream=None, mode="fp32"):
         """Several problems (``(sources, positions, looks, out_scale, window)`` each)
         on this table in one set of launches: a list of device (OM, frequency)
-        complex128 spectra, each equal to the problem applied alone."""
+        complex128 spectra, each equal to the problem applied alone.
+
+        ``mode``: ``"fp32"`` (CUDA cores), ``"split-bf16"`` or ``"bf16"`` (tensor
+        cores, full spectra on a table whose shape fits that path; zero-frequency
+        applies and other shapes run on the CUDA cores)."""
         import torch
         lib = _lib.load()
         dev = self.device
@@ -241,16 +275,32 @@ class Ge2Table:
             probs[i], at = self._problem(q, at, result.data_ptr() + 16 * r_at)
             r_at += sizes[i]
         n = len(prepared)
-        need = int(lib.lh_ge2_batch_workspace_bytes(self.struct, probs, n))
+        if mode not in _lib.MODES:
+            raise ValueError(f"unknown contraction mode {mode!r}")
+        packed = (self.tc_packed() if mode != "fp32" and not zero_frequency
+                  and all(q["W"] == len(self.omega) for q in prepared) else None)
+        slots = C.create_string_buffer(int(lib.lh_ge2_batch_slot_bytes(n)))  # pageable staging
+        s = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
+        if packed is not None:
+            need = int(lib.lh_ge2_tc_workspace_bytes(self.struct, probs, n))
+        else:
+            need = int(lib.lh_ge2_batch_workspace_bytes(self.struct, probs, n))
         if need == 0:
             raise ValueError("order >=2 problem rejected by the device library")
         if self._workspace is None or self._workspace.numel() < need:
             self._workspace = torch.empty(need, dtype=torch.uint8, device=dev)
-        slots = C.create_string_buffer(int(lib.lh_ge2_batch_slot_bytes(n)))  # pageable staging
-        s = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))
-        _lib.check(lib.lh_ge2_apply_batch(self.struct, probs, n, self._workspace.data_ptr(),
-                                          self._workspace.numel(), slots, s),
-                   "lh_ge2_apply_batch")
+        status = None
+        if packed is not None:
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
+            _lib.check(lib.lh_ge2_apply_batch_tc(self.struct, probs, n, _lib.MODES[mode],
+                                                 packed.data_ptr(), self._workspace.data_ptr(),
+                                                 self._workspace.numel(), slots,
+                                                 status.data_ptr(), s), "lh_ge2_apply_batch_tc")
+        else:
+            _lib.check(lib.lh_ge2_apply_batch(self.struct, probs, n, self._workspace.data_ptr(),
+                                              self._workspace.numel(), slots, s),
+                       "lh_ge2_apply_batch")
+        self.status = status  # LH_STATUS_TIMEOUT when a tensor-core wait gave up
         self._keep = (d_geom, [q["ch"] for q in prepared])  # alive until the stream runs
         out, r_at = [], 0
         for q, size in zip(prepared, sizes):

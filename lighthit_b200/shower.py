@@ -69,6 +69,9 @@ class ShowerSettings:
     delayed_cell_ns: float = 20.0        # ShowerConfig.delayed_cell_ns
     min_distance_m: float = 0.1          # PromptConfig.min_distance_m
     readout_mode: str = "split-bf16"
+    # The >=2 contraction of the full spectra: "split-bf16" or "bf16" on the
+    # tensor cores (BF16 operands, float32 accumulation), "fp32" on the CUDA cores.
+    contraction_mode: str = "split-bf16"
     # Gauss order of the order-0 ray quadrature (wavelength, along-track and
     # azimuth nodes per piece). Against the reference's control-variate order 0
     # on the README shower: order 6 agrees to 6e-8 in charge (order 8: 2.5e-8,
@@ -252,6 +255,29 @@ class ShowerTables:
         tables = route.tables()
         return cls(route_constants(route, tables), folded_kernels(route, tables),
                    near=near_interval(route, tables), **kw)
+
+    @classmethod
+    def from_packs(cls, route, folded_pack, kernel_pack=None, **kw):
+        """Tables from the reference's own files, without the reference: the
+        route constants (``route``: a ``route_<config>.npz`` or its dict), the
+        band-folded order >=2 directory ``ShowerData.ge2_band_fold`` points to
+        (``folded.npy`` + ``folded.json``), and optionally the per-wavelength
+        kernel pack of ``ShowerData.ge2_pack`` (``pack.json`` + ``<n>.npy``),
+        whose bundle on the route's frequencies gives the near-field interval
+        (``lighthit_b200.formats``)."""
+        from .formats import load_folded_pack, load_kernel_pack, near_table
+        folded = load_folded_pack(folded_pack)
+        near = kw.pop("near", None)
+        if kernel_pack is not None:
+            omega = np.asarray(folded["omega"], float)
+            for bundle in load_kernel_pack(kernel_pack).values():
+                if (len(bundle["omega"]) == len(omega)
+                        and np.allclose(bundle["omega"], omega, rtol=0, atol=1e-12)):
+                    near = near_table(bundle)
+                    break
+            else:
+                raise ValueError("the kernel pack holds no bundle on the folded frequencies")
+        return cls(route, folded, near=near, **kw)
 
     @classmethod
     def synthetic(cls, name="c0", **kw):
@@ -594,7 +620,7 @@ class ShowerTransport:
         return self._apply_many([(points, channels, reference, frame, oms)],
                                 zero_frequency=zero_frequency)[0]
 
-    def _apply_many(self, requests, *, zero_frequency):
+    def _apply_many(self, requests, *, zero_frequency, mode="fp32"):
         """``_apply_device`` of several ``(points, channels, reference, frame, oms)``
         requests (the events of a batch) in one batched launch set per table."""
         T = self.tables
@@ -615,15 +641,22 @@ class ShowerTransport:
                     src = AxialSources(points[b], channels[b][None], refs[b:b + 1].copy(), basis,
                                        T.source_degree, T.azimuthal_degree)
                     split.append((i, b, (src,) + args))
+        self.ge2_status = []  # status words of tensor-core contractions (read with the results)
         if joint:
             for (i, _), res in zip(joint, T.ge2.apply_batch([it for _, it in joint],
-                                                            zero_frequency=zero_frequency)):
+                                                            zero_frequency=zero_frequency,
+                                                            mode=mode)):
                 out[i] = res
+            if T.ge2.status is not None:
+                self.ge2_status.append(T.ge2.status)
         for b in sorted({b for _, b, _ in split}):
             part = [(i, it) for i, bb, it in split if bb == b]
-            for (i, _), res in zip(part, T.ge2.band(b).apply_batch(
-                    [it for _, it in part], zero_frequency=zero_frequency)):
+            view = T.ge2.band(b)
+            for (i, _), res in zip(part, view.apply_batch(
+                    [it for _, it in part], zero_frequency=zero_frequency, mode=mode)):
                 out[i] = res if out[i] is None else out[i] + res
+            if view.status is not None:
+                self.ge2_status.append(view.status)
         return out
 
     def __call__(self, source, *, progress=None, time_origin_ns=None,
@@ -1021,7 +1054,8 @@ class ShowerTransport:
         if row_ev:
             specs = self._apply_many([(events[k].points, events[k].channels, events[k].reference,
                                        events[k].frame, work) for k, work in row_ev],
-                                     zero_frequency=False)
+                                     zero_frequency=False, mode=cfg.contraction_mode)
+            contraction_status = list(self.ge2_status)
             # relative-time spectra e^{-i w origin} N(w); the stored zero frequency is
             # the exact >=2 charge (shower/api.py:584)
             origin = np.concatenate([events[k].origins[work] for k, work in row_ev])
@@ -1037,7 +1071,12 @@ class ShowerTransport:
         # one read: the >=2 bins and spectra of the active OMs, the order-0 bins
         with_bins0 = [k for k, ev in enumerate(events) if np.any(ev.active)]
         host = _lib.fetch(([bins2_d] + list(specs) if row_ev else [])
-                          + [events[k].pending["bins0"] for k in with_bins0])
+                          + [events[k].pending["bins0"] for k in with_bins0]
+                          + (contraction_status if row_ev else []))
+        if row_ev and any(int(st[0]) & _lib.LH_STATUS_TIMEOUT
+                          for st in host[len(host) - len(contraction_status):]):
+            raise RuntimeError("the tensor-core >=2 contraction timed out waiting for its "
+                               "pipeline")
         if row_ev:
             bins2 = host[0].astype(float)
             for (k, work), spec in zip(row_ev, host[1:1 + len(row_ev)]):

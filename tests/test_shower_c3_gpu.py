@@ -13,13 +13,21 @@ converges there, so that shower is checked against the CPU oracle's whole route
 reference's adaptive order doubling). The showers of a mode run as one
 stage-major batch.
 
-Charges do not depend on the readout precision; bins and the per-order error
-against the reference are reported for FP32, split-BF16 (hi + lo, three
-products, FP32 accumulate) and BF16 (one product) readouts. Bars: charge as for
-the other configs; bins L1 per order BINS_L1[mode] of the OM's charge. A single
-BF16 product (8 significant bits per operand) leaves ~5 % bins L1 on the
-order >=2 waveforms of this window (2060 bins, 130 terms per bin that largely
-cancel), outside the 1e-3 bar: that is why the route reads out in split-BF16.
+The >=2 contraction of the full spectra and the readout run in the mode
+under study: FP32 on the CUDA cores, or on the tensor cores with split-BF16
+(hi + lo, three products, FP32 accumulate) or BF16 (one product). Order 0 and
+1 charges do not depend on it (the >=2 charge is the exact zero-frequency
+contraction, always FP32); bins, spectra and the per-order errors against the
+reference are reported per mode. Bars: charge as for
+the other configs; bins L1 per order BINS_L1[mode] of the OM's charge and
+spectrum SPECTRUM[mode] of each OM's largest value. FP32 and split-BF16 (three
+BF16 parts per operand in the contraction, two in the readout) keep the >=2
+bins within 1e-3. A single BF16 product (8 significant bits per operand) in
+both the contraction and the readout leaves ~0.7 of the OM's charge as bins
+L1 and ~16 % spectrum error on the order >=2 waveforms of this window (2060
+bins, 130 terms per bin that largely cancel): the study's answer is that BF16
+alone is not usable here, which is why the route contracts and reads out in
+split-BF16; its bars only bound that measured error.
 """
 import numpy as np
 import pytest
@@ -27,7 +35,8 @@ import pytest
 from conftest import GOLDEN
 
 ORDER0, ORDER1, ORDER2 = 1e-4, 1e-5, 1e-4
-BINS_L1 = {"fp32": 1e-3, "split-bf16": 1e-3, "bf16": 0.1}
+BINS_L1 = {"fp32": 1e-3, "split-bf16": 1e-3, "bf16": 1.0}
+SPECTRUM = {"fp32": 1e-3, "split-bf16": 1e-3, "bf16": 0.25}
 N_SHOWERS = 12
 
 pytestmark = pytest.mark.gpu
@@ -71,7 +80,8 @@ def routed(request, stream):
     from dataclasses import replace
     from lighthit_b200.shower import ShowerTransport
     tables, g, kept, sources = stream
-    route = ShowerTransport(tables, config=replace(tables.settings, readout_mode=request.param))
+    route = ShowerTransport(tables, config=replace(tables.settings, readout_mode=request.param,
+                                                   contraction_mode=request.param))
     return request.param, route.batch(sources), g, kept, tables.threshold
 
 
@@ -128,4 +138,4 @@ def test_bins_and_spectrum(routed):
         spec_worst = max(spec_worst, spec.max())
     print(f"\nc3 {mode}: worst per-order bins L1 / charge {worst}, spectrum {spec_worst:.2e}")
     assert worst.max() <= BINS_L1[mode], (mode, worst)
-    assert spec_worst < 1e-3
+    assert spec_worst < SPECTRUM[mode], (mode, spec_worst)
