@@ -605,7 +605,8 @@ int lh_kernel_timing_read(int32_t n_kernels, int64_t* launches, double* total_ms
  * launch since the last lh_kernel_timing(1) (after a device synchronisation):
  * (OM, pencil) evaluations for o1_group_kernel, float32 integrand
  * evaluations (one wavelength x along-track x azimuth node of a piece) for
- * order0_kernel, 0 for the kernels that do not count. */
+ * order0_kernel, (OM, point) pairs inside the radial window for the
+ * tensor-core >=2 contraction, 0 for the kernels that do not count. */
 int lh_kernel_units_read(int32_t n_kernels, int64_t* units);
 
 /* Flash transport that allocates nothing (no counterpart in the reference).

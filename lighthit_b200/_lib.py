@@ -227,7 +227,7 @@ SIGNATURES = {
 LH_ESCRATCH = 6
 # kernel ids of lh_kernel_timing_read
 TIMED_KERNELS = ("order0_kernel", "o1_ring_kernel", "o1_group_kernel", "o1_batch_kernel",
-                 "ge2_apply_batch_kernel", "src_group_kernel", "src_transform_kernel",
+                 "ge2_contraction", "src_group_kernel", "src_transform_kernel",
                  "readout_tc_kernel", "flash_tc_kernel")
 
 _lib = None
@@ -334,7 +334,8 @@ def kernel_times():
 def kernel_units():
     """``{kernel: units}`` of algorithmic work counted on the device since the
     timing was last started ((OM, pencil) evaluations of ``o1_group_kernel``,
-    integrand nodes of ``order0_kernel``)."""
+    integrand nodes of ``order0_kernel``, in-window (OM, point) pairs of the
+    tensor-core >=2 contraction)."""
     import numpy as np
     n = len(TIMED_KERNELS)
     units = np.zeros(n, np.int64)

@@ -620,7 +620,7 @@ __global__ void ge2_tc_bucket_kernel(const Ge2Slot* slots, Ge2Arrays A, int32_t*
 
 // Bucket starts, tile starts (kTcPairs pairs per tile) and the fill cursors.
 __global__ void ge2_tc_scan_kernel(int n_intervals, int32_t* counts, int32_t* bucket_start,
-                                   int32_t* tile_start) {
+                                   int32_t* tile_start, unsigned long long* units) {
   if (threadIdx.x != 0) return;
   int32_t at = 0, tiles = 0;
   for (int j = 0; j < n_intervals; ++j) {
@@ -633,6 +633,7 @@ __global__ void ge2_tc_scan_kernel(int n_intervals, int32_t* counts, int32_t* bu
   }
   bucket_start[n_intervals] = at;
   tile_start[n_intervals] = tiles;
+  if (units) atomicAdd(units, (unsigned long long)at);  // (OM, point) pairs in range
 }
 
 __global__ void __launch_bounds__(kTcThreads, 2)
@@ -956,7 +957,8 @@ int ge2_tc_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t 
   const unsigned bucket_blocks = (unsigned)std::min<int64_t>((max_pairs + 255) / 256, 148 * 4);
   ge2_tc_bucket_kernel<<<dim3(bucket_blocks, n), 256, 0, s>>>(slots, A, counts, sorted,
                                                               sorted_slot, 0);
-  ge2_tc_scan_kernel<<<1, 32, 0, s>>>(T.n_intervals, counts, bucket_start, tile_start);
+  ge2_tc_scan_kernel<<<1, 32, 0, s>>>(T.n_intervals, counts, bucket_start, tile_start,
+                                      kernel_units() ? kernel_units() + LH_KT_GE2_APPLY : nullptr);
   ge2_tc_bucket_kernel<<<dim3(bucket_blocks, n), 256, 0, s>>>(slots, A, counts, sorted,
                                                               sorted_slot, 1);
   Ge2TcArgs G;

@@ -53,3 +53,65 @@ def test_one_rank_keeps_its_own_time():
     assert not dist.is_initialized()
     assert bench.max_over_ranks(42.0, "cpu") == 42.0
     assert bench.job_rate(10, 1, 1000.0) == pytest.approx(10.0)
+
+
+def _failing_rank(rank, world, port, results):
+    """Rank 1 leaves between steps (its replica failed), before the timing
+    collective; rank 0 must learn it from the closed connection or the short
+    process-group timeout, not wait for good."""
+    import datetime
+    import time
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=5))
+    try:
+        if rank == 1:
+            results[rank] = "left"
+            return
+        t0 = time.monotonic()
+        try:
+            bench.max_over_ranks(10.0, "cpu")
+            results[rank] = "collective completed"
+        except Exception as exc:  # gloo reports the missing peer
+            results[rank] = ("error", type(exc).__name__, time.monotonic() - t0)
+    finally:
+        if rank == 0:
+            dist.destroy_process_group()
+
+
+def test_a_failed_rank_ends_the_others_collective_with_an_error():
+    world = 2
+    with mp.Manager() as manager:
+        results = manager.dict()
+        ctx = mp.start_processes(_failing_rank, args=(world, _free_port(), results),
+                                 nprocs=world, start_method="spawn", join=False)
+        deadline = __import__("time").monotonic() + 120
+        while not ctx.join(timeout=1):
+            if __import__("time").monotonic() > deadline:
+                for p in ctx.processes:
+                    p.kill()
+                pytest.fail("ranks did not end")
+        got = dict(results)
+    assert got[1] == "left"
+    assert got[0][0] == "error" and got[0][2] < 60
+
+
+def _absent_rank(index, port, results):
+    import datetime
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    try:
+        dist.init_process_group("gloo", rank=0, world_size=2,
+                                timeout=datetime.timedelta(seconds=3))
+        results[0] = "joined"
+    except Exception as exc:
+        results[0] = ("error", type(exc).__name__)
+
+
+def test_a_rank_that_never_joins_ends_the_rendezvous_with_an_error():
+    with mp.Manager() as manager:
+        results = manager.dict()
+        mp.start_processes(_absent_rank, args=(_free_port(), results), nprocs=1,
+                           start_method="spawn", join=True)
+        got = dict(results)
+    assert got[0][0] == "error"
