@@ -105,7 +105,7 @@ def test_flash_table_from_cache_file():
 def test_route_on_tables_read_from_packs_equals_the_route(tmp_path):
     """The README shower on tables read from a full-size folded pack (in the
     format the readers above are pinned to) equals the route on the committed
-    tables, bit for bit."""
+    tables (up to the run-to-run rounding of the order-1 float64 atomics)."""
     from lighthit_b200.formats import FOLD_FORMAT
     from lighthit_b200.shower import ShowerTables, ShowerTransport
     t = dict(np.load(TABLES / "ge2_fold_48om_2-150m.npz"))
@@ -122,6 +122,8 @@ def test_route_on_tables_read_from_packs_equals_the_route(tmp_path):
     ref = ShowerTransport(ShowerTables.synthetic("c0"))(el)
     got = ShowerTransport(ShowerTables.from_packs(TABLES / "route_c0.npz", pack,
                                                   near=TABLES / "near_c0.npz"))(el)
-    np.testing.assert_array_equal(got.charge_components_pe, ref.charge_components_pe)
-    np.testing.assert_array_equal(got.components_pe, ref.components_pe)
+    scale = np.abs(ref.charge_pe).max()
+    assert np.abs(got.charge_components_pe - ref.charge_components_pe).max() <= 1e-10 * scale
+    assert np.abs(got.components_pe - ref.components_pe).max() <= 1e-10 * scale
     np.testing.assert_array_equal(got.active, ref.active)
+    np.testing.assert_array_equal(got.time_origin_ns, ref.time_origin_ns)
