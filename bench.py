@@ -373,7 +373,7 @@ def contraction_roofline(kernels, tensor_peak, peak_source):
     convention of the scope table: 2 x rows x K x N flops with rows = in-window
     (OM, point) pairs x 39 source channels, K = 6 pairs x 4 powers, N = 2 x 65
     frequencies x 3 bands, per split-BF16 product set counted once."""
-    ge2 = kernels.get("ge2_contraction")
+    ge2 = kernels.get("ge2_tc_kernel")
     if not ge2 or not ge2["units"]:
         return None
     flops = ge2["units"] * 39 * 2 * 24 * 390 / ge2["launches"]

@@ -592,12 +592,13 @@ enum {
   LH_KT_O1_RING = 1,     /* o1_ring_kernel (lh_order1_pencils)       */
   LH_KT_O1_GROUP = 2,    /* o1_group_kernel (lh_order1_grouped)      */
   LH_KT_O1_BATCH = 3,    /* o1_batch_kernel (lh_order1_grouped)      */
-  LH_KT_GE2_APPLY = 4,   /* ge2_apply_batch_kernel or ge2_tc_kernel (lh_ge2_apply_batch[_tc]) */
+  LH_KT_GE2_APPLY = 4,   /* ge2_apply_batch_kernel (lh_ge2_apply_batch)  */
   LH_KT_SRC_GROUP = 5,   /* src_group_kernel (lh_source_compile)     */
   LH_KT_SRC_TRANSFORM = 6, /* src_transform_kernel (lh_source_compile) */
   LH_KT_READOUT = 7,     /* readout_tc_kernel (lh_readout_rows)      */
   LH_KT_FLASH = 8,       /* flash_tc_kernel (lh_flash_transport)     */
-  LH_KT_COUNT = 9
+  LH_KT_GE2_TC = 9,      /* ge2_tc_kernel (lh_ge2_apply_batch_tc)    */
+  LH_KT_COUNT = 10
 };
 int lh_kernel_timing(int enable);
 int lh_kernel_timing_read(int32_t n_kernels, int64_t* launches, double* total_ms);

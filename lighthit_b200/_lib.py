@@ -227,8 +227,8 @@ SIGNATURES = {
 LH_ESCRATCH = 6
 # kernel ids of lh_kernel_timing_read
 TIMED_KERNELS = ("order0_kernel", "o1_ring_kernel", "o1_group_kernel", "o1_batch_kernel",
-                 "ge2_contraction", "src_group_kernel", "src_transform_kernel",
-                 "readout_tc_kernel", "flash_tc_kernel")
+                 "ge2_apply_batch_kernel", "src_group_kernel", "src_transform_kernel",
+                 "readout_tc_kernel", "flash_tc_kernel", "ge2_tc_kernel")
 
 _lib = None
 

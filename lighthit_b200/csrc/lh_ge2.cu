@@ -958,7 +958,7 @@ int ge2_tc_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t 
   ge2_tc_bucket_kernel<<<dim3(bucket_blocks, n), 256, 0, s>>>(slots, A, counts, sorted,
                                                               sorted_slot, 0);
   ge2_tc_scan_kernel<<<1, 32, 0, s>>>(T.n_intervals, counts, bucket_start, tile_start,
-                                      kernel_units() ? kernel_units() + LH_KT_GE2_APPLY : nullptr);
+                                      kernel_units() ? kernel_units() + LH_KT_GE2_TC : nullptr);
   ge2_tc_bucket_kernel<<<dim3(bucket_blocks, n), 256, 0, s>>>(slots, A, counts, sorted,
                                                               sorted_slot, 1);
   Ge2TcArgs G;
@@ -992,7 +992,7 @@ int ge2_tc_batch_launch(const lh_ge2_table& T, const lh_ge2_problem* P, int32_t 
   const unsigned grid =
       (unsigned)std::max<int64_t>(1, std::min<int64_t>(tile_bound, two ? 2 * 148 : 148));
   {
-    lh::TimedLaunch timed_launch(LH_KT_GE2_APPLY, s);
+    lh::TimedLaunch timed_launch(LH_KT_GE2_TC, s);
     ge2_tc_kernel<<<grid, kTcThreads, smem, s>>>(T, G);
   }
   ge2_tc_reduce_kernel<<<dim3((unsigned)((max_outs + 255) / 256), n), 256, 0, s>>>(T, slots, A,

@@ -622,16 +622,17 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W,
         const double s = (sa + sb) / 2 + (sb - sa) / 2 * sin_psi;
         const double ds = (sb - sa) / 2 * cos_psi * kPi / 2 * R.w[j];
         const double along = z - s, W2 = rho * rho + along * along, Bq = W2 - radius * radius;
-        double half;
+        double half, cos_half = 1.0;  // cos(half): the clamped argument itself (rho > 0)
         if (rho > 0.0) {
-          half = acos(o0_clamp1((sqrt(Bq) - cosine * along) / (sine * rho)));
+          cos_half = o0_clamp1((sqrt(Bq) - cosine * along) / (sine * rho));
+          half = acos(cos_half);
         } else {
           half = cosine * along >= sqrt(Bq) ? kPi : 0.0;
         }
         if (half == 0.0) continue;
         const double emission = t0 + tau * s - origin;
         const double tmin = emission + o0_entry(Bq, cosine * along + sine * rho) / velocity;
-        const double tmax = emission + o0_entry(Bq, cosine * along + sine * rho * cos(half)) / velocity;
+        const double tmax = emission + o0_entry(Bq, cosine * along + sine * rho * cos_half) / velocity;
         phicuts[0] = 0.0;
         int nphi = 1;
         if (rho > 0.0) {

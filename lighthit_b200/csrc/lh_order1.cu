@@ -423,10 +423,10 @@ o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
   for (int j = 0; j < per; ++j) {
     const int64_t slot = begin + j;
     if (slot >= capacity || !o1_slot_used(keys, rows, slot)) continue;
-    // rank q goes to row (q * 2^31-1) mod n, a fixed permutation (2^31 - 1 is
-    // prime and n < 2^31): stage B's warps then see pencils of many cells, not
-    // a run of one cell's pencils competing for the same group rows
-    const int row = (int)(base + (q * 2147483647ll) % n);
+    // rank order: a cell's pencils are neighbours in the table, so that the 32
+    // pencils of a stage-B warp share their groups (about four items per group
+    // against one for a random order) and the warp sums them before the atomics
+    const int row = (int)(base + q);
     o1_write_pencil(rows + slot * kO1Moments, Pn, row);
     if (slot_row) slot_row[slot] = row;
     if (Pn.parent) {
@@ -626,17 +626,22 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
   extern __shared__ double o1g_stage[];
   double* stage = o1g_stage + warp * 32 * n_values;
   double* pen = o1g_stage + (blockDim.x >> 5) * 32 * n_values + warp * 32 * kO1PencilFields + lane;
-  // A warp takes 32 consecutive pencils and kO1GroupOms consecutive work OMs:
-  // each lane reads its pencil once (into shared memory) and evaluates it
-  // against every OM of the chunk in turn. Lanes past the last pencil compute
-  // on pencil 0 and take no part in any group.
+  // A warp takes 32 consecutive pencils (neighbours in space) and kO1GroupOms
+  // consecutive work OMs: each lane reads its pencil once (into shared memory)
+  // and evaluates it against every OM of the chunk in turn. Chunks take the OM
+  // blocks fastest and the pencil blocks in a fixed permutation
+  // ((q (2^31 - 1)) mod blocks, 2^31 - 1 prime), so that the warps running at
+  // once work on different OMs and distant parts of the shower rather than
+  // competing for the same group rows. Lanes past the last pencil compute on
+  // pencil 0 and take no part in any group.
   const int64_t pblocks = ((int64_t)n_pencils + 31) / 32;
-  const int64_t chunks = pblocks * ((n_work + kO1GroupOms - 1) / kO1GroupOms);
+  const int64_t oblocks = (n_work + kO1GroupOms - 1) / kO1GroupOms;
+  const int64_t chunks = pblocks * oblocks;
   const int64_t warps_total = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t chunk = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp; chunk < chunks;
        chunk += warps_total) {
-    const int64_t p_raw = (chunk % pblocks) * 32 + lane;
-    const int w_first = (int)(chunk / pblocks) * kO1GroupOms;
+    const int64_t p_raw = (((chunk / oblocks) * 2147483647ll) % pblocks) * 32 + lane;
+    const int w_first = (int)(chunk % oblocks) * kO1GroupOms;
     const bool p_ok = p_raw < n_pencils;
     const int p = p_ok ? (int)p_raw : 0;
     pen[0] = Pn.position[3 * p]; pen[32] = Pn.position[3 * p + 1]; pen[64] = Pn.position[3 * p + 2];
