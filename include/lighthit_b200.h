@@ -610,6 +610,16 @@ int lh_kernel_timing_read(int32_t n_kernels, int64_t* launches, double* total_ms
  * tensor-core >=2 contraction, 0 for the kernels that do not count. */
 int lh_kernel_units_read(int32_t n_kernels, int64_t* units);
 
+/* Host function (no device work): the weighted centre and the lower triangle
+ * of the weighted covariance of the element midpoints start + length/2 *
+ * direction with weights `share` (summing to one), summed in element order
+ * with every product rounded to float64 as NumPy evaluates AxisFrame.of's
+ * expressions (axial_source.py:88-118). centre[3], covariance[3][3] (upper
+ * triangle zero). */
+int lh_axis_frame_sums(int64_t n, const double* start, const double* direction,
+                       const double* length, const double* share, double* centre,
+                       double* covariance);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

@@ -191,6 +191,7 @@ SIGNATURES = {
     "lh_kernel_timing": (C.c_int, [C.c_int]),
     "lh_kernel_timing_read": (C.c_int, [C.c_int32, P, P]),
     "lh_kernel_units_read": (C.c_int, [C.c_int32, P]),
+    "lh_axis_frame_sums": (C.c_int, [C.c_int64, P, P, P, P, P, P]),
     "lh_flash_combine": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(FlashNodes),
                                    C.POINTER(FlashBatch), P]),
     "lh_ge2_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem)]),

@@ -39,7 +39,8 @@ def build(verbose=False, force=False):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
-           "-shared", "-Xcompiler", "-fPIC", "-I", str(HERE.parent / "include"),
+           "-shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+           "-I", str(HERE.parent / "include"),
            "-o", str(tmp), *map(str, SOURCES)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

@@ -49,21 +49,20 @@ def harmonic_layout(degree, max_m):
 
 def axis_frame(start, direction, length, weights):
     """``AxisFrame.of`` (``axial_source.py:88-118``): centre, axis, first, second."""
-    start, direction = np.asarray(start, float), np.asarray(direction, float)
-    points = start + 0.5 * np.asarray(length, float)[:, None] * direction
-    share = np.asarray(weights, float) / np.sum(weights)
+    start = np.ascontiguousarray(start, float)
+    direction = np.ascontiguousarray(direction, float)
+    length = np.ascontiguousarray(length, float)
+    share = np.ascontiguousarray(np.asarray(weights, float) / np.sum(weights))
     # Bit for bit the reference's frame (one rounding apart can move a node
     # across a slice edge or a slice across the stencil threshold): its centre
-    # expression, and its einsum("i,ij,ik->jk") covariance, which adds the
-    # elements in order, as running sums of the lower triangle (eigh reads
-    # only that).
-    centre = (share[:, None] * points).sum(axis=0)
-    offset = points - centre
-    lead = share[:, None] * offset
+    # expression and its einsum("i,ij,ik->jk") covariance, which add the
+    # elements in order, summed in one host pass of the library (the lower
+    # triangle: eigh reads only that).
+    centre = np.zeros(3)
     covariance = np.zeros((3, 3))
-    for j in range(3):
-        for k in range(j + 1):
-            covariance[j, k] = np.cumsum(lead[:, j] * offset[:, k])[-1]
+    _lib.check(_lib.load().lh_axis_frame_sums(
+        len(length), start.ctypes.data, direction.ctypes.data, length.ctypes.data,
+        share.ctypes.data, centre.ctypes.data, covariance.ctypes.data), "lh_axis_frame_sums")
     values, vectors = np.linalg.eigh(covariance)
     if np.max(np.abs(values)) <= 1e-24:
         axis = np.sum(share[:, None] * direction, axis=0)
