@@ -248,7 +248,7 @@ struct O0Work {
   int32_t* cursor;    // [n_events * n_om]
   int32_t* pairs;     // [pair capacity] global element index
   int2* chunks;       // [chunk capacity] (event * n_om + om, chunk)
-  int32_t* n_chunks;  // [1]
+  int32_t* n_chunks;  // [2]: the chunk count, then the next chunk to take
   int64_t pair_capacity, chunk_capacity;
 };
 
@@ -348,7 +348,10 @@ __global__ void __launch_bounds__(1024) order0_scan_kernel(int32_t n_keys, O0Wor
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) *W.n_chunks = carry_chunks;
+  if (threadIdx.x == 0) {
+    W.n_chunks[0] = carry_chunks;
+    W.n_chunks[1] = 0;
+  }
 }
 
 // One Gauss rule: nodes, weights and the s-node map sin/cos(pi/2 x).
@@ -357,16 +360,55 @@ struct O0Rule {
   double sin_psi[kO0MaxOrder], cos_psi[kO0MaxOrder];
 };
 
+// A (piece, wavelength node) item as its s-nodes read it.
+struct O0Item {
+  double cosine, sine, velocity, scale, t0;
+  float absorption;
+  int code;  // pair | 0x100 for the check rule
+};
+
+constexpr int kO0CutPool = 1536;  // s cuts staged per batch of items
+
 struct O0Shared {
   O0Rule rule[2];  // the quadrature order and the lower check order
   float alpha[kO0MaxAlpha];
   O0Pair pair[kO0Chunk];
+  O0Item item[kO0Threads];   // the batch's items, one per thread
+  int unit_end[kO0Threads];  // inclusive prefix of the items' s-node counts
+  int cut_at[kO0Threads];    // each item's first s cut in `cuts`
+  double cuts[kO0CutPool];
   double warp_charge[kO0Threads / 32];
   double warp_check[kO0Threads / 32];
+  int scan[32];
+  int chunk;
   int n_pairs;
   int n_combos;
-  int next_item;  // phase-2 work counter (warps take 32 items at a time)
 };
+
+// Exclusive prefix sum of `v` over the CTA (blockDim a multiple of 32, at most
+// 1024) through `warp_sums` (32 ints of shared memory); `total` gets the sum.
+LH_DEVICE int o0_block_scan(int v, int& total, int* warp_sums) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+  int inclusive = v;
+  for (int off = 1; off < 32; off <<= 1) {
+    const int up = __shfl_up_sync(0xffffffffu, inclusive, off);
+    if (lane >= off) inclusive += up;
+  }
+  __syncthreads();  // warp_sums may still be read by a previous call
+  if (lane == 31) warp_sums[warp] = inclusive;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < n_warps ? warp_sums[lane] : 0;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int up = __shfl_up_sync(0xffffffffu, w, off);
+      if (lane >= off) w += up;
+    }
+    warp_sums[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  total = warp_sums[n_warps - 1];
+  return inclusive - v + (warp ? warp_sums[warp - 1] : 0);
+}
 
 __global__ void __launch_bounds__(kO0Threads, 4)
 order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W,
@@ -398,8 +440,14 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W,
   o0_phase_range(O, pmin, pmax);
   const int total_chunks = min(*W.n_chunks, (int)W.chunk_capacity);
   unsigned long long evaluations = 0;  // float32 integrand nodes of this thread
-  for (int chunk = blockIdx.x; chunk < total_chunks; chunk += gridDim.x) {
+  // CTAs take chunks from a counter: one that drew a heavy chunk does not
+  // hold back the chunks dealt to it after
+  for (;;) {
   __syncthreads();
+  if (tid == 0) S.chunk = atomicAdd(W.n_chunks + 1, 1);
+  __syncthreads();
+  const int chunk = S.chunk;
+  if (chunk >= total_chunks) break;
   const int2 entry = W.chunks[chunk];
   const int ev = entry.x / O.n_om;
   const int om = entry.x - ev * O.n_om;
@@ -407,10 +455,7 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W,
   const int p_end = min(W.offsets[entry.x] + W.counts[entry.x], p_begin + kO0Chunk);
   if (want_bins)
     for (int k = tid; k < nb; k += blockDim.x) sbins[k] = 0.0;
-  if (tid == 0) {
-    S.n_combos = 0;
-    S.next_item = 0;
-  }
+  if (tid == 0) S.n_combos = 0;
   const double ox = O.om_pos[3 * om], oy = O.om_pos[3 * om + 1], oz = O.om_pos[3 * om + 2];
   const double radius = O.om_radius[om];
   uint32_t flags = 0;
@@ -508,7 +553,11 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W,
   __syncthreads();
   const int n_combos = S.n_combos;
 
-  // ---- phase 2: (piece, wavelength node) items
+  // ---- phase 2: (piece, wavelength node) items in batches of one per thread.
+  // Each thread sets up its item (cone of the wavelength node, s window, the s
+  // cuts at the bin-edge crossings) and stages it; the batch's s-nodes (s piece
+  // x Gauss node) are then spread evenly over the CTA, so that lanes no longer
+  // wait on a neighbour whose item has more s pieces or none at all.
   const double area_scale = O.om_area[om] / (kPi * radius * radius);
   const double origin = B.origins[(int64_t)ev * O.n_om + om];
   const double* edges = B.edges;
@@ -521,188 +570,233 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W,
   double scuts[kO0MaxSCuts];
   double phicuts[kO0MaxPhiCuts];
 
-  // warps take 32 consecutive items at a time from a shared counter, so a warp
-  // that drew cheap pieces goes back for more instead of idling at the barrier
+  // main-rule items first, then the check rule's: a warp's items share a rule
+  const int main_items = n_combos * order;
   const int n_items = n_combos * rules;
-  const int lane = tid & 31;
-  for (int item_base = 0;;) {
-    if (lane == 0) item_base = atomicAdd(&S.next_item, 32);
-    item_base = __shfl_sync(0xffffffffu, item_base, 0);
-    if (item_base >= n_items) break;
-    const int item = item_base + lane;
-    if (item >= n_items) continue;
-    const int ci = item / rules, r_item = item - ci * rules;
-    const bool is_check = r_item >= order;
-    const int ilam = is_check ? r_item - order : r_item;
-    const int ord = is_check ? check : order;
-    const O0Rule& R = S.rule[is_check ? 1 : 0];
-    const uint32_t code = combos[ci];
-    const int p = code & 0xff, panel = (code >> 8) & 0xffff, piece = code >> 24;
-    const O0Pair& P = S.pair[p];
-    const int64_t i = P.el;
-    const double left = O.panel_edges[panel], width = O.panel_edges[panel + 1] - left;
-    const double n0 = O.phase[panel], dn = O.phase[panel + 1] - n0;
-    double cuts[4];
-    int count = 2;
-    if (dn == 0.0) {
-      cuts[0] = left; cuts[1] = left + width;
-    } else {
-      double x0 = (P.nmin - n0) / dn, x1 = (P.nmax - n0) / dn;
-      cuts[0] = left + width * fmax(fmin(x0, x1), 0.0);
-      cuts[1] = left + width * fmin(fmax(x0, x1), 1.0);
-      double vals[2] = {P.cut0, P.cut1};
-      const double lo_c = cuts[0], hi_c = cuts[1];
-      for (int v = 0; v < 2; ++v)
-        if (isfinite(vals[v])) {
-          double lam = left + width * (vals[v] - n0) / dn;
-          if (lo_c < lam && lam < hi_c) cuts[count++] = lam;
-        }
-      o0_sort(cuts, count);
-    }
-    const double low = cuts[piece], high = cuts[piece + 1];
-    const double beta = B.beta[i], L = B.length[i];
-    const double lam = (low + high) / 2 + (high - low) / 2 * R.x[ilam];
-    const double q = (lam - left) / width, n = n0 + dn * q, bn = beta * n;
-    if (bn <= 1.0) continue;
-    const double cosine = 1 / bn, sine = sqrt(1 - cosine * cosine);
-    const double z = P.z, rho = P.rho;
-    const double centre = z - rho * cosine / sine, spread = radius / sine;
-    const double slo = fmax(centre - spread, 0.0), shi = fmin(centre + spread, L);
-    if (slo >= shi) continue;
-    const double absorption = O.extinction[panel] + q * (O.extinction[panel + 1] - O.extinction[panel]);
-    const double group = O.group[panel] + q * (O.group[panel + 1] - O.group[panel]);
-    const double velocity = kCVacuumMPerNs / group;
-    const double* ef = O.efficiency + (int64_t)panel * O.eff_cols;
-    double eta = ((ef[3] * q + ef[2]) * q + ef[1]) * q + ef[0];
-    if (O.eff_cols > 4) eta *= exp(ef[4] + q * ef[5]);
-    const double spectral = (B.c0[i] + B.c2[i] / (n * n)) / L / (lam * lam) * eta;
-    const double scale = (high - low) / 2 * R.w[ilam] * spectral * area_scale;
-    const double t0 = B.t0[i], tau = P.tau;
+  for (int first = 0; first < n_items;) {  // the same on every thread
+    const int item = first + tid;
+    int ns = 0, units = 0;
+    O0Item it{};
+    if (item < n_items) {
+      int ci, r_item;
+      if (item < main_items) {
+        ci = item / order;
+        r_item = item - ci * order;
+      } else {
+        const int rest = item - main_items;
+        ci = rest / check;
+        r_item = order + (rest - ci * check);
+      }
+      const bool is_check = r_item >= order;
+      const int ilam = is_check ? r_item - order : r_item;
+      const O0Rule& R = S.rule[is_check ? 1 : 0];
+      const uint32_t code = combos[ci];
+      const int p = code & 0xff, panel = (code >> 8) & 0xffff, piece = code >> 24;
+      const O0Pair& P = S.pair[p];
+      const int64_t i = P.el;
+      const double left = O.panel_edges[panel], width = O.panel_edges[panel + 1] - left;
+      const double n0 = O.phase[panel], dn = O.phase[panel + 1] - n0;
+      double cuts[4];
+      int count = 2;
+      if (dn == 0.0) {
+        cuts[0] = left; cuts[1] = left + width;
+      } else {
+        double x0 = (P.nmin - n0) / dn, x1 = (P.nmax - n0) / dn;
+        cuts[0] = left + width * fmax(fmin(x0, x1), 0.0);
+        cuts[1] = left + width * fmin(fmax(x0, x1), 1.0);
+        double vals[2] = {P.cut0, P.cut1};
+        const double lo_c = cuts[0], hi_c = cuts[1];
+        for (int v = 0; v < 2; ++v)
+          if (isfinite(vals[v])) {
+            double lam = left + width * (vals[v] - n0) / dn;
+            if (lo_c < lam && lam < hi_c) cuts[count++] = lam;
+          }
+        o0_sort(cuts, count);
+      }
+      const double low = cuts[piece], high = cuts[piece + 1];
+      const double beta = B.beta[i], L = B.length[i];
+      const double lam = (low + high) / 2 + (high - low) / 2 * R.x[ilam];
+      const double q = (lam - left) / width, n = n0 + dn * q, bn = beta * n;
+      const double cosine = 1 / bn, sine = bn > 1.0 ? sqrt(1 - cosine * cosine) : 0.0;
+      const double z = P.z, rho = P.rho;
+      const double centre = z - rho * cosine / sine, spread = radius / sine;
+      const double slo = fmax(centre - spread, 0.0), shi = fmin(centre + spread, L);
+      if (bn > 1.0 && slo < shi) {
+        const double absorption =
+            O.extinction[panel] + q * (O.extinction[panel + 1] - O.extinction[panel]);
+        const double group = O.group[panel] + q * (O.group[panel + 1] - O.group[panel]);
+        const double velocity = kCVacuumMPerNs / group;
+        const double* ef = O.efficiency + (int64_t)panel * O.eff_cols;
+        double eta = ((ef[3] * q + ef[2]) * q + ef[1]) * q + ef[0];
+        if (O.eff_cols > 4) eta *= exp(ef[4] + q * ef[5]);
+        const double spectral = (B.c0[i] + B.c2[i] / (n * n)) / L / (lam * lam) * eta;
+        const double t0 = B.t0[i], tau = P.tau;
+        it.cosine = cosine;
+        it.sine = sine;
+        it.velocity = velocity;
+        it.scale = (high - low) / 2 * R.w[ilam] * spectral * area_scale;
+        it.t0 = t0;
+        it.absorption = (float)absorption;
+        it.code = p | (is_check ? 0x100 : 0);
 
-    // s cuts where a cone ray's entry time crosses a bin edge (_surface_ballistic_rays.py:96-118)
-    scuts[0] = slo;
-    scuts[1] = shi;
-    int ns = 2;
-    {
-      const double d0 = (z - slo) * (z - slo), d1 = (z - shi) * (z - shi);
-      const double rmax = sqrt(rho * rho + fmax(d0, d1));
-      const double rmin = sqrt(rho * rho + ((slo < z && z < shi) ? 0.0 : fmin(d0, d1)));
-      const double e_lo = t0 + tau * slo, e_hi = t0 + tau * shi;
-      const double earliest = fmin(e_lo, e_hi) + (rmin - radius) / velocity - origin;
-      const double latest = fmax(e_lo, e_hi) + rmax / velocity - origin;
-      const int first_edge = o0_search_right(edges, n_edges, earliest);
-      const int last_edge = o0_search_left(edges, n_edges, latest);
-      for (int edge = first_edge; edge < last_edge; ++edge) {
-        const double A = (origin + edges[edge] - t0) * velocity, Bv = tau * velocity;
-        for (int sgn = -1; sgn <= 1; sgn += 2) {
-          const double D = cosine * z + sgn * sine * rho;
-          ns = o0_quadratic_cuts(scuts, ns, 1 + Bv * Bv - 2 * Bv * cosine,
-                                 -2 * z - 2 * A * Bv + 2 * (A * cosine + Bv * D),
-                                 z * z + rho * rho - radius * radius + A * A - 2 * A * D, slo, shi);
+        // s cuts where a cone ray's entry time crosses a bin edge
+        // (_surface_ballistic_rays.py:96-118)
+        scuts[0] = slo;
+        scuts[1] = shi;
+        ns = 2;
+        const double d0 = (z - slo) * (z - slo), d1 = (z - shi) * (z - shi);
+        const double rmax = sqrt(rho * rho + fmax(d0, d1));
+        const double rmin = sqrt(rho * rho + ((slo < z && z < shi) ? 0.0 : fmin(d0, d1)));
+        const double e_lo = t0 + tau * slo, e_hi = t0 + tau * shi;
+        const double earliest = fmin(e_lo, e_hi) + (rmin - radius) / velocity - origin;
+        const double latest = fmax(e_lo, e_hi) + rmax / velocity - origin;
+        const int first_edge = o0_search_right(edges, n_edges, earliest);
+        const int last_edge = o0_search_left(edges, n_edges, latest);
+        for (int edge = first_edge; edge < last_edge; ++edge) {
+          const double A = (origin + edges[edge] - t0) * velocity, Bv = tau * velocity;
+          for (int sgn = -1; sgn <= 1; sgn += 2) {
+            const double D = cosine * z + sgn * sine * rho;
+            ns = o0_quadratic_cuts(scuts, ns, 1 + Bv * Bv - 2 * Bv * cosine,
+                                   -2 * z - 2 * A * Bv + 2 * (A * cosine + Bv * D),
+                                   z * z + rho * rho - radius * radius + A * A - 2 * A * D, slo,
+                                   shi);
+          }
+          ns = o0_quadratic_cuts(scuts, ns, Bv * Bv - 1., -2 * A * Bv + 2 * z,
+                                 A * A - z * z - rho * rho + radius * radius, slo, shi);
         }
-        ns = o0_quadratic_cuts(scuts, ns, Bv * Bv - 1., -2 * A * Bv + 2 * z,
-                               A * A - z * z - rho * rho + radius * radius, slo, shi);
+        if (ns > kO0MaxSCuts) {
+          flags |= LH_STATUS_OVERFLOW;
+          ns = 0;
+        } else {
+          o0_sort(scuts, ns);
+          units = (ns - 1) * (is_check ? check : order);
+        }
       }
     }
-    if (ns > kO0MaxSCuts) {
-      flags |= LH_STATUS_OVERFLOW;
-      continue;
-    }
-    o0_sort(scuts, ns);
+    // stage the cuts; the threads whose cuts do not fit the pool (a suffix of
+    // the CTA: the offsets only grow) set their items up again next batch
+    int cut_total;
+    const int cut_at = o0_block_scan(ns, cut_total, S.scan);
+    const bool fits = cut_at + ns <= kO0CutPool;
+    const int taken = __syncthreads_count(fits);  // at least thread 0's (ns <= kO0MaxSCuts)
+    if (!fits) units = 0;
+    else
+      for (int k = 0; k < ns; ++k) S.cuts[cut_at + k] = scuts[k];
+    int unit_total;
+    const int unit_at = o0_block_scan(units, unit_total, S.scan);
+    S.unit_end[tid] = unit_at + units;
+    S.cut_at[tid] = cut_at;
+    S.item[tid] = it;
+    __syncthreads();
 
-    const float cos_f = (float)cosine, sin_f = (float)sine;
-    const float axial = (float)P.axial, across = (float)P.across, side = (float)P.side;
+    // the batch's s-nodes, consecutive ones (one item's) on neighbouring lanes
     const float R2 = (float)(radius * radius);
-    const float absorption_f = (float)absorption;
-    for (int sp = 0; sp < ns - 1; ++sp) {
-      const double sa = scuts[sp], sb = scuts[sp + 1];
+    for (int u = tid; u < unit_total; u += blockDim.x) {
+      int owner = 0;  // the first thread whose s-nodes end past u
+      for (int hi = blockDim.x - 1; owner < hi;) {
+        const int mid = (owner + hi) >> 1;
+        if (S.unit_end[mid] > u) hi = mid; else owner = mid + 1;
+      }
+      const O0Item& c = S.item[owner];
+      const bool is_check = c.code >> 8;
+      const int ord = is_check ? check : order;
+      const O0Rule& R = S.rule[is_check ? 1 : 0];
+      const O0Pair& P = S.pair[c.code & 0xff];
+      const int local = u - (owner ? S.unit_end[owner - 1] : 0);
+      const int sp = local / ord, j = local - sp * ord;
+      const double sa = S.cuts[S.cut_at[owner] + sp], sb = S.cuts[S.cut_at[owner] + sp + 1];
       if (sa >= sb) continue;
-      for (int j = 0; j < ord; ++j) {
-        const double sin_psi = R.sin_psi[j], cos_psi = R.cos_psi[j];
-        const double s = (sa + sb) / 2 + (sb - sa) / 2 * sin_psi;
-        const double ds = (sb - sa) / 2 * cos_psi * kPi / 2 * R.w[j];
-        const double along = z - s, W2 = rho * rho + along * along, Bq = W2 - radius * radius;
-        double half, cos_half = 1.0;  // cos(half): the clamped argument itself (rho > 0)
-        if (rho > 0.0) {
-          cos_half = o0_clamp1((sqrt(Bq) - cosine * along) / (sine * rho));
-          half = acos(cos_half);
-        } else {
-          half = cosine * along >= sqrt(Bq) ? kPi : 0.0;
+      const double cosine = c.cosine, sine = c.sine, velocity = c.velocity;
+      const double z = P.z, rho = P.rho, t0 = c.t0, tau = P.tau;
+      const float cos_f = (float)cosine, sin_f = (float)sine;
+      const float axial = (float)P.axial, across = (float)P.across, side = (float)P.side;
+      const float absorption_f = c.absorption;
+      const double sin_psi = R.sin_psi[j], cos_psi = R.cos_psi[j];
+      const double s = (sa + sb) / 2 + (sb - sa) / 2 * sin_psi;
+      const double ds = (sb - sa) / 2 * cos_psi * kPi / 2 * R.w[j];
+      const double along = z - s, W2 = rho * rho + along * along, Bq = W2 - radius * radius;
+      double half, cos_half = 1.0;  // cos(half): the clamped argument itself (rho > 0)
+      if (rho > 0.0) {
+        cos_half = o0_clamp1((sqrt(Bq) - cosine * along) / (sine * rho));
+        half = acos(cos_half);
+      } else {
+        half = cosine * along >= sqrt(Bq) ? kPi : 0.0;
+      }
+      if (half == 0.0) continue;
+      const double emission = t0 + tau * s - origin;
+      const double tmin = emission + o0_entry(Bq, cosine * along + sine * rho) / velocity;
+      const double tmax = emission + o0_entry(Bq, cosine * along + sine * rho * cos_half) / velocity;
+      phicuts[0] = 0.0;
+      int nphi = 1;
+      if (rho > 0.0) {
+        const int first_cut = o0_search_right(edges, n_edges, tmin);
+        const int last_cut = o0_search_left(edges, n_edges, tmax);
+        for (int edge = first_cut; edge < last_cut; ++edge) {
+          const double distance = (edges[edge] - emission) * velocity;
+          const double dot = (Bq + distance * distance) / (2 * distance);
+          const double phi = acos(o0_clamp1((dot - cosine * along) / (sine * rho)));
+          const double r = phi / half;
+          if (nphi < kO0MaxPhiCuts - 1) phicuts[nphi] = asin(r < 1.0 ? r : 1.0);
+          ++nphi;
         }
-        if (half == 0.0) continue;
-        const double emission = t0 + tau * s - origin;
-        const double tmin = emission + o0_entry(Bq, cosine * along + sine * rho) / velocity;
-        const double tmax = emission + o0_entry(Bq, cosine * along + sine * rho * cos_half) / velocity;
-        phicuts[0] = 0.0;
-        int nphi = 1;
-        if (rho > 0.0) {
-          const int first = o0_search_right(edges, n_edges, tmin);
-          const int last = o0_search_left(edges, n_edges, tmax);
-          for (int edge = first; edge < last; ++edge) {
-            const double distance = (edges[edge] - emission) * velocity;
-            const double dot = (Bq + distance * distance) / (2 * distance);
-            const double phi = acos(o0_clamp1((dot - cosine * along) / (sine * rho)));
-            const double r = phi / half;
-            if (nphi < kO0MaxPhiCuts - 1) phicuts[nphi] = asin(r < 1.0 ? r : 1.0);
-            ++nphi;
-          }
+      }
+      if (nphi > kO0MaxPhiCuts - 1) {
+        flags |= LH_STATUS_OVERFLOW;
+        continue;
+      }
+      phicuts[nphi++] = kPi / 2;
+      // float32 azimuth integrand, entry distance without cancellation
+      const float half_f = (float)half;
+      const float W2_f = (float)W2, B_f = (float)Bq;
+      const float E0 = (float)(along * sine - rho * cosine);
+      const float Sa = (float)(along * sine);
+      const float along_cos = (float)(cosine * along), rho_sin = (float)(sine * rho);
+      const float sin2W2 = sin_f * sin_f * W2_f;
+      for (int pp = 0; pp < nphi - 1; ++pp) {
+        const double pa = phicuts[pp], pb = phicuts[pp + 1];
+        if (pa >= pb) continue;
+        const float mid = (float)((pa + pb) / 2), hw = (float)((pb - pa) / 2);
+        evaluations += ord;
+        float integral = 0.0f;
+        for (int jp = 0; jp < ord; ++jp) {
+          // arguments lie in [0, pi]: the hardware approximations (absolute error
+          // near 2^-21) are well inside the float32 integrand's budget
+          float s_eta, c_eta;
+          __sincosf(mid + hw * (float)R.x[jp], &s_eta, &c_eta);
+          const float phi = half_f * s_eta;
+          const float dphi = half_f * c_eta * hw * (float)R.w[jp];
+          // sin(phi), cos(phi) from the half angle: 2 sin^2(phi/2) = 1 - cos(phi)
+          // without cancellation near phi = 0
+          float sh, chh;
+          __sincosf(0.5f * phi, &sh, &chh);
+          const float ss = 2.0f * sh * chh, cp = 1.0f - 2.0f * sh * sh;
+          const float E = E0 - Sa * (2.0f * sh * sh);
+          const float D = R2 - (sin2W2 * ss * ss + E * E);
+          const float dot = along_cos + rho_sin * cp;
+          const float distance = __fdividef(B_f, dot + sqrtf(fmaxf(D, 0.0f)));
+          const float x1 = cos_f * axial + sin_f * (cp * across + ss * side);
+          const float x2 = cos_f * axial + sin_f * (cp * across - ss * side);
+          const float accept = o0_acceptance(S.alpha, O.n_alpha, x1, alpha_abs, bad_acceptance) +
+                               o0_acceptance(S.alpha, O.n_alpha, x2, alpha_abs, bad_acceptance);
+          integral += dphi * accept * __expf(-absorption_f * distance);
         }
-        if (nphi > kO0MaxPhiCuts - 1) {
-          flags |= LH_STATUS_OVERFLOW;
+        const double value = c.scale * ds * (double)integral * (1.0 / (2 * kPi));
+        if (is_check) {  // the check rule: charge only
+          charge_check += value;
           continue;
         }
-        phicuts[nphi++] = kPi / 2;
-        // float32 azimuth integrand, entry distance without cancellation
-        const float half_f = (float)half;
-        const float W2_f = (float)W2, B_f = (float)Bq;
-        const float E0 = (float)(along * sine - rho * cosine);
-        const float Sa = (float)(along * sine);
-        const float along_cos = (float)(cosine * along), rho_sin = (float)(sine * rho);
-        const float sin2W2 = sin_f * sin_f * W2_f;
-        for (int pp = 0; pp < nphi - 1; ++pp) {
-          const double pa = phicuts[pp], pb = phicuts[pp + 1];
-          if (pa >= pb) continue;
-          const float mid = (float)((pa + pb) / 2), hw = (float)((pb - pa) / 2);
-          evaluations += ord;
-          float integral = 0.0f;
-          for (int jp = 0; jp < ord; ++jp) {
-            // arguments lie in [0, pi]: the hardware approximations (absolute error
-            // near 2^-21) are well inside the float32 integrand's budget
-            float s_eta, c_eta;
-            __sincosf(mid + hw * (float)R.x[jp], &s_eta, &c_eta);
-            const float phi = half_f * s_eta;
-            const float dphi = half_f * c_eta * hw * (float)R.w[jp];
-            // sin(phi), cos(phi) from the half angle: 2 sin^2(phi/2) = 1 - cos(phi)
-            // without cancellation near phi = 0
-            float sh, chh;
-            __sincosf(0.5f * phi, &sh, &chh);
-            const float ss = 2.0f * sh * chh, cp = 1.0f - 2.0f * sh * sh;
-            const float E = E0 - Sa * (2.0f * sh * sh);
-            const float D = R2 - (sin2W2 * ss * ss + E * E);
-            const float dot = along_cos + rho_sin * cp;
-            const float distance = __fdividef(B_f, dot + sqrtf(fmaxf(D, 0.0f)));
-            const float x1 = cos_f * axial + sin_f * (cp * across + ss * side);
-            const float x2 = cos_f * axial + sin_f * (cp * across - ss * side);
-            const float accept = o0_acceptance(S.alpha, O.n_alpha, x1, alpha_abs, bad_acceptance) +
-                                 o0_acceptance(S.alpha, O.n_alpha, x2, alpha_abs, bad_acceptance);
-            integral += dphi * accept * __expf(-absorption_f * distance);
-          }
-          const double value = scale * ds * (double)integral * (1.0 / (2 * kPi));
-          if (is_check) {  // the check rule: charge only
-            charge_check += value;
-            continue;
-          }
-          charge += value;
-          if (want_bins) {
-            const double phi_mid = half * sin((pa + pb) / 2);
-            const double arrival =
-                emission + o0_entry(Bq, cosine * along + sine * rho * cos(phi_mid)) / velocity;
-            const int slot = o0_search_right(edges, n_edges, arrival) - 1;
-            if (slot >= 0 && slot < nb) atomicAdd(&sbins[slot], value);
-          }
+        charge += value;
+        if (want_bins) {
+          const double phi_mid = half * sin((pa + pb) / 2);
+          const double arrival =
+              emission + o0_entry(Bq, cosine * along + sine * rho * cos(phi_mid)) / velocity;
+          const int slot = o0_search_right(edges, n_edges, arrival) - 1;
+          if (slot >= 0 && slot < nb) atomicAdd(&sbins[slot], value);
         }
       }
     }
+    first += taken;
+    __syncthreads();  // the batch's staging is read before the next batch writes it
   }
   if (bad_acceptance) flags |= LH_STATUS_NEGATIVE_ACCEPTANCE;
 
