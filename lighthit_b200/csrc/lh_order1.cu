@@ -360,15 +360,19 @@ __global__ void o1_total_kernel(const int32_t* children, const int32_t* parents,
   if (threadIdx.x == 0 && blockIdx.x == 0) *total = *children + *parents;
 }
 
-// Used slots per tile of the ring table.
+// Used slots per tile of the ring table. Thread t takes slots t, t + 256, ...
+// of its tile, so that a warp's key loads are contiguous.
 __global__ void __launch_bounds__(kO1FinishThreads)
 o1_tile_count_kernel(const long long* keys, const double* rows, int64_t capacity,
                      int32_t* tile_count) {
-  const int per = kO1Tile / kO1FinishThreads;
-  const int64_t begin = blockIdx.x * (int64_t)kO1Tile + threadIdx.x * per;
+  constexpr int per = kO1Tile / kO1FinishThreads;
+  const int64_t tile0 = blockIdx.x * (int64_t)kO1Tile + threadIdx.x;
   int mine = 0;
-  for (int j = 0; j < per; ++j)
-    if (begin + j < capacity && o1_slot_used(keys, rows, begin + j)) ++mine;
+#pragma unroll
+  for (int j = 0; j < per; ++j) {
+    const int64_t slot = tile0 + (int64_t)j * kO1FinishThreads;
+    if (slot < capacity && o1_slot_used(keys, rows, slot)) ++mine;
+  }
   int total;
   o1_block_exclusive_scan(mine, total);
   if (threadIdx.x == 0) tile_count[blockIdx.x] = total;
@@ -405,8 +409,10 @@ o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
                  const int32_t* base_count, int32_t* slot_row, const long long* parent_keys,
                  int64_t parent_capacity, const int32_t* parent_row, int face, int parent_face,
                  int32_t* status) {
-  const int per = kO1Tile / kO1FinishThreads;
-  const int64_t begin = blockIdx.x * (int64_t)kO1Tile + threadIdx.x * per;
+  constexpr int per = kO1Tile / kO1FinishThreads;  // rounds of 256 consecutive slots
+  constexpr int warps = kO1FinishThreads / 32;
+  static_assert(per <= 32 && per * warps == 128, "one 32-bit mask per thread, 4 counts per lane");
+  __shared__ int before[per * warps];  // used slots ahead of each (round, warp) in the tile
   const int64_t n = *count;
   const int64_t base = base_count ? *base_count : 0;
   if (base + n > Pn.capacity) {  // the caller redoes the stage with a larger table
@@ -414,19 +420,50 @@ o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
       atomicOr(reinterpret_cast<unsigned*>(status), LH_STATUS_OVERFLOW);
     return;
   }
-  int mine = 0;
-  for (int j = 0; j < per; ++j)
-    if (begin + j < capacity && o1_slot_used(keys, rows, begin + j)) ++mine;
-  int total;
-  int64_t q = tile_offset[blockIdx.x] + o1_block_exclusive_scan(mine, total);
-  if (!mine) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t tile0 = blockIdx.x * (int64_t)kO1Tile + threadIdx.x;
+  unsigned used = 0;  // bit j: this thread's slot of round j holds a pencil
+#pragma unroll
   for (int j = 0; j < per; ++j) {
-    const int64_t slot = begin + j;
-    if (slot >= capacity || !o1_slot_used(keys, rows, slot)) continue;
-    // rank order: a cell's pencils are neighbours in the table, so that the 32
-    // pencils of a stage-B warp share their groups (about four items per group
-    // against one for a random order) and the warp sums them before the atomics
-    const int row = (int)(base + q);
+    const int64_t slot = tile0 + (int64_t)j * kO1FinishThreads;
+    if (slot < capacity && o1_slot_used(keys, rows, slot)) used |= 1u << j;
+  }
+#pragma unroll
+  for (int j = 0; j < per; ++j) {
+    const unsigned b = __ballot_sync(0xffffffffu, (used >> j) & 1u);
+    if (lane == 0) before[j * warps + warp] = __popc(b);
+  }
+  __syncthreads();
+  if (warp == 0) {  // exclusive scan of the 128 (round, warp) counts in slot order
+    int v[4], sum = 0;
+    for (int i = 0; i < 4; ++i) {
+      v[i] = before[4 * lane + i];
+      sum += v[i];
+    }
+    int inclusive = sum;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int up = __shfl_up_sync(0xffffffffu, inclusive, off);
+      if (lane >= off) inclusive += up;
+    }
+    int running = inclusive - sum;
+    for (int i = 0; i < 4; ++i) {
+      before[4 * lane + i] = running;
+      running += v[i];
+    }
+  }
+  __syncthreads();
+  if (!used) return;
+  const unsigned lower = (1u << lane) - 1u;
+  for (int j = 0; j < per; ++j) {
+    const unsigned b = __ballot_sync(__activemask(), (used >> j) & 1u);
+    if (!((used >> j) & 1u)) continue;
+    const int64_t slot = tile0 + (int64_t)j * kO1FinishThreads;
+    // rank order = slot order: a cell's pencils are neighbours in the table, so
+    // that the 32 pencils of a stage-B warp share their groups (about four items
+    // per group against one for a random order) and the warp sums them before
+    // the atomics
+    const int row = (int)(base + tile_offset[blockIdx.x] + before[j * warps + warp] +
+                          __popc(b & lower));
     o1_write_pencil(rows + slot * kO1Moments, Pn, row);
     if (slot_row) slot_row[slot] = row;
     if (Pn.parent) {
@@ -439,7 +476,6 @@ o1_finish_kernel(const long long* keys, int64_t capacity, const double* rows,
       }
       Pn.parent[row] = parent;
     }
-    ++q;
   }
 }
 
@@ -1065,10 +1101,15 @@ struct O1BandDeposit {
   bool outside;
 };
 
+// NODES: the path-grid nodes a CTA holds in shared memory (kO1SmallNodes for
+// the common short grids, kO1MaxNodes for the rest).
+constexpr int kO1SmallNodes = 512;
+
+template <int NODES>
 struct O1BatchShared {
-  double s[kO1MaxNodes];
-  double g0[kO1MaxNodes];
-  double g2[kO1MaxNodes];
+  double s[NODES];
+  double g0[NODES];
+  double g2[NODES];
   double mom[kO1MaxValues * 128];  // moments of the batch's theta groups (<= 128)
   double sin_q[128], cos_q[128];   // per group: sin, cos of its mean angle (0, 0: empty)
   double coef[kO1MaxMono];
@@ -1082,12 +1123,19 @@ struct O1BatchShared {
 // Persistent CTAs over the batch list: _grouped_pencils_order1_block's batch
 // loop (_prompt_numba.py:1934-1993) with _batch_grid, _batch_add_moments and
 // _batch_deposit (_prompt_numba.py:258-551).
+// The small-grid instance (NODES < kO1MaxNodes, 42 KB of shared memory, five
+// CTAs per SM) takes the whole list and hands each batch whose path grid needs
+// more than NODES nodes to `deferred`; the full-size instance (two CTAs per
+// SM) then takes only those.
+template <int NODES>
 __global__ void __launch_bounds__(kO1BatchThreads)
 o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* gkeys,
                 const double* grows, const int32_t* sorted_slots, const int32_t* batch_list,
-                const int32_t* batch_total, double* accum, int32_t* status) {
+                const int32_t* batch_total, int32_t* deferred, int32_t* n_deferred,
+                double* accum, int32_t* status) {
+  constexpr bool kSmall = NODES < kO1MaxNodes;
   extern __shared__ __align__(16) unsigned char o1_smem[];
-  O1BatchShared& S = *reinterpret_cast<O1BatchShared*>(o1_smem);
+  O1BatchShared<NODES>& S = *reinterpret_cast<O1BatchShared<NODES>*>(o1_smem);
   const int tid = threadIdx.x;
   const int nm = C.n_mono;
   const int nv = 2 * nm + 6;
@@ -1106,9 +1154,10 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
   }
   const double g = C.g;
   const double y_g = g != 0.0 ? (1.0 - fabs(g)) / (1.0 + fabs(g)) : 1.0;
-  const int total = *batch_total;
+  const int total = kSmall ? *batch_total : *n_deferred;
   const int64_t per_om = (int64_t)NL * (3 + 4 * nb + 1);
-  for (int b = blockIdx.x; b < total; b += gridDim.x) {
+  for (int i = blockIdx.x; i < total; i += gridDim.x) {
+    const int b = kSmall ? i : deferred[i];
     __syncthreads();
     const int w = batch_list[3 * b], start = batch_list[3 * b + 1], stop = batch_list[3 * b + 2];
     const int count = stop - start;
@@ -1175,6 +1224,11 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
           n_out = capacity - 1 - n_in;
         }
         S.n = (int)(n_in + n_out + 1);
+        if (S.n > NODES) {  // a long path grid: the full-size instance takes this batch
+          deferred[atomicAdd(n_deferred, 1)] = b;
+          S.n = 0;
+          goto stats_done;
+        }
         S.stats[0] = r_b; S.stats[1] = t_b; S.stats[2] = sqrt(12.0 * tau_var);
         S.stats[3] = sigma; S.stats[4] = u_win; S.stats[5] = u_end;
         S.stats[6] = (double)n_in; S.stats[7] = (double)n_out;
@@ -1210,7 +1264,7 @@ o1_batch_kernel(const lh_order1_config C, const int32_t* work, const long long* 
     // contiguous ranges so that every thread works: each (node, part) sum goes
     // to the unused upper part of g0/g2 and the parts are added in order.
     const double g1 = 1.0 + g * g, gg = 2.0 * g, norm = (1.0 - g * g) / (4.0 * kPi);
-    constexpr int kSplitNodes = kO1MaxNodes / 4;
+    constexpr int kSplitNodes = NODES / 4;
     const int parts = n <= kSplitNodes ? max(1, min(3, (int)blockDim.x / n)) : 1;
     for (int it = tid; it < n * parts; it += blockDim.x) {
       const int k = it % n, part = it / n;
@@ -1459,7 +1513,8 @@ struct O1Workspace {
   int32_t* gcount;
   int32_t* sorted;
   int32_t* batch_list;
-  int32_t* batch_total;
+  int32_t* batch_total;  // [4]: batches, then batches deferred to the full-size grid
+  int32_t* deferred;     // batches whose path grid exceeds kO1SmallNodes
   double* accum;
   unsigned long long* sort_keys;  // tables above kO1SmemSort only
   int32_t* sort_slots;
@@ -1495,6 +1550,7 @@ static O1Workspace o1_layout(const lh_order1_config& C, int64_t pencil_capacity,
   W.batch_list =
       reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 3 * (size_t)n_work * C.group_capacity));
   W.batch_total = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 4));
+  W.deferred = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * (size_t)n_work * C.group_capacity));
   W.accum = reinterpret_cast<double*>(take(sizeof(double) * (size_t)n_work * C.n_bands * (3 + 4 * nb + 1)));
   const size_t sort_n = C.group_capacity > kO1SmemSort ? (size_t)n_work * C.group_capacity : 0;
   W.sort_keys = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * sort_n));
@@ -1661,14 +1717,23 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
   lh::o1_batches_kernel<<<n_work, 1024, sort_smem, s>>>(*C, n_work, W.gkeys, W.sorted, W.batch_list,
                                                         W.batch_total, W.sort_keys, W.sort_slots,
                                                         status);
-  const size_t batch_smem = sizeof(lh::O1BatchShared);
-  if (cudaFuncSetAttribute(lh::o1_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)batch_smem) != cudaSuccess)
+  const size_t small_smem = sizeof(lh::O1BatchShared<lh::kO1SmallNodes>);
+  const size_t full_smem = sizeof(lh::O1BatchShared<lh::kO1MaxNodes>);
+  if (cudaFuncSetAttribute(lh::o1_batch_kernel<lh::kO1SmallNodes>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)small_smem) != cudaSuccess ||
+      cudaFuncSetAttribute(lh::o1_batch_kernel<lh::kO1MaxNodes>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)full_smem) != cudaSuccess)
     return LH_ECUDA;
   {
     lh::TimedLaunch timed_launch(LH_KT_O1_BATCH, s);
-    lh::o1_batch_kernel<<<148 * 2, lh::kO1BatchThreads, batch_smem, s>>>(
-        *C, work, W.gkeys, W.grows, W.sorted, W.batch_list, W.batch_total, W.accum, status);
+    lh::o1_batch_kernel<lh::kO1SmallNodes><<<148 * 5, lh::kO1BatchThreads, small_smem, s>>>(
+        *C, work, W.gkeys, W.grows, W.sorted, W.batch_list, W.batch_total, W.deferred,
+        W.batch_total + 1, W.accum, status);
+    lh::o1_batch_kernel<lh::kO1MaxNodes><<<148 * 2, lh::kO1BatchThreads, full_smem, s>>>(
+        *C, work, W.gkeys, W.grows, W.sorted, W.batch_list, W.batch_total, W.deferred,
+        W.batch_total + 1, W.accum, status);
   }
   const size_t fin_smem = sizeof(double) * C->n_bands * nb;
   if (fin_smem > 200 * 1024) return LH_EUNSUPPORTED;
