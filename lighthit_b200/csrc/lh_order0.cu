@@ -248,13 +248,16 @@ struct O0Work {
   int32_t* cursor;    // [n_events * n_om]
   int32_t* pairs;     // [pair capacity] global element index
   int2* chunks;       // [chunk capacity] (event * n_om + om, chunk)
+  uint32_t* mask;     // [pair capacity / 32] candidate bits of the counting pass
   int32_t* n_chunks;  // [2]: the chunk count, then the next chunk to take
   int64_t pair_capacity, chunk_capacity;
 };
 
 // Candidate pairs counted (fill = false) or listed (fill = true) per (event, OM):
 // one thread per (OM, element); a warp's elements are consecutive, so the
-// lanes of one (event, OM) add their count once (warp-aggregated atomics).
+// lanes of one (event, OM) add their count once (warp-aggregated atomics). The
+// counting pass keeps each warp's candidate mask, which the listing pass reads
+// instead of testing the pair again.
 template <bool fill>
 __global__ void order0_candidates_kernel(const lh_order0_optics O, const lh_order0_batch B,
                                          O0Work W) {
@@ -266,16 +269,19 @@ __global__ void order0_candidates_kernel(const lh_order0_optics O, const lh_orde
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < total;
        base += (int64_t)gridDim.x * blockDim.x) {
     const int64_t item = base + threadIdx.x;
+    const int64_t word = item >> 5;  // blockDim and base are multiples of 32
     bool keep = false;
     int key = -1;
     int64_t i = 0;
     if (item < total) {
       const int om = (int)(item / n_el);
       i = item - (int64_t)om * n_el;
-      keep = o0_is_candidate(O, B, om, i, pmin, pmax, flags);
-      key = o0_event_of(B, i) * O.n_om + om;
+      keep = fill ? ((W.mask[word] >> (threadIdx.x & 31)) & 1u)
+                  : o0_is_candidate(O, B, om, i, pmin, pmax, flags);
+      if (keep) key = o0_event_of(B, i) * O.n_om + om;
     }
     const unsigned active = __ballot_sync(0xffffffffu, keep);
+    if (!fill && (threadIdx.x & 31) == 0 && item < total) W.mask[word] = active;
     if (keep) {
       const unsigned peers = __match_any_sync(active, key);
       const int leader = __ffs(peers) - 1;
@@ -863,6 +869,7 @@ static O0Work o0_layout(const lh_order0_optics& O, const lh_order0_batch& B, uns
   W.cursor = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * keys));
   W.pairs = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * W.pair_capacity));
   W.chunks = reinterpret_cast<int2*>(take(sizeof(int2) * W.chunk_capacity));
+  W.mask = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * ((W.pair_capacity + 31) / 32)));
   W.n_chunks = reinterpret_cast<int32_t*>(take(sizeof(int32_t) * 4));
   if (bytes) *bytes = off;
   return W;
