@@ -274,7 +274,11 @@ def shower_section(args, dev, world):
                           workers=WORKERS, max_batch=MAX_BATCH)
     steps, warmup = args.steps, max(args.warmup, 3)
     try:
-        # warm-up: every worker's tables and workspaces sized, caching allocators filled
+        # every worker's workspaces sized for the pool's two largest showers (on
+        # each of its side-stream lanes), so no step allocates device memory
+        largest = sorted(resident, key=lambda e: len(e["length_m"]))[-2:]
+        server.prime(largest * server.routes[0].n_lanes)
+        # warm-up: caching allocators filled, every kernel loaded
         served_region(server, [s for k in range(warmup) for s in step_showers(resident, k)],
                       stream)
         if world > 1:

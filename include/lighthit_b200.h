@@ -620,6 +620,21 @@ int lh_axis_frame_sums(int64_t n, const double* start, const double* direction,
                        const double* length, const double* share, double* centre,
                        double* covariance);
 
+/* Host function (no device work): low[3], high[3] = the per-coordinate minima
+ * and maxima over the element starts and ends start + length * direction, the
+ * box of compress's cell grid (prompt.py:1317-1402). NaN coordinates give NaN
+ * bounds. */
+int lh_element_box(int64_t n, const double* start, const double* direction,
+                   const double* length, double* low, double* high);
+
+/* Host function (no device work): delay[i] = (start_ns[i] - start_ns[first])
+ * - |start[i] - start[first]| / c_m_per_ns, the steps' delays behind the light
+ * front of step `first` in delay_groups (shower/ge2.py:122-147), rounded as
+ * NumPy evaluates that expression; `distance` (may be NULL) receives
+ * |start[i] - start[first]|. */
+int lh_element_delays(int64_t n, const double* start, const double* start_ns, int64_t first,
+                      double c_m_per_ns, double* delay, double* distance);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

@@ -46,3 +46,51 @@ extern "C" int lh_axis_frame_sums(int64_t n, const double* start, const double* 
   }
   return LH_OK;
 }
+
+// Per-coordinate minima and maxima over the element starts and ends
+// start + length * direction (the cell grid of compress, prompt.py:1317-1402,
+// and the route's radial and clock decisions). A NaN coordinate makes that
+// coordinate's bounds NaN, as NumPy's min and max do.
+extern "C" int lh_element_box(int64_t n, const double* start, const double* direction,
+                              const double* length, double* low, double* high) {
+  if (n < 1 || !start || !direction || !length || !low || !high) return LH_EINVAL;
+  for (int j = 0; j < 3; ++j) {
+    double lo = start[j], hi = start[j];
+    bool nan = false;
+    for (int64_t i = 0; i < n; ++i) {
+      const double a = start[3 * i + j];
+      const double product = length[i] * direction[3 * i + j];
+      const double b = a + product;
+      nan = nan || a != a || b != b;
+      lo = a < lo ? a : lo;
+      hi = a > hi ? a : hi;
+      lo = b < lo ? b : lo;
+      hi = b > hi ? b : hi;
+    }
+    low[j] = nan ? __builtin_nan("") : lo;
+    high[j] = nan ? __builtin_nan("") : hi;
+  }
+  return LH_OK;
+}
+
+// delay_groups (shower/ge2.py:122-147): each step's delay behind the light
+// front of step `first`, (t_i - t_first) - |x_i - x_first| / c, with the
+// distance summed x, y, z in that order and every operation rounded to
+// float64 as NumPy evaluates the expression; `distance` (optional) receives
+// |x_i - x_first|.
+extern "C" int lh_element_delays(int64_t n, const double* start, const double* start_ns,
+                                 int64_t first, double c_m_per_ns, double* delay,
+                                 double* distance) {
+  if (n < 1 || first < 0 || first >= n || !start || !start_ns || !delay || !(c_m_per_ns > 0.0))
+    return LH_EINVAL;
+  const double x0 = start[3 * first], y0 = start[3 * first + 1], z0 = start[3 * first + 2];
+  const double t0 = start_ns[first];
+  for (int64_t i = 0; i < n; ++i) {
+    const double dx = start[3 * i] - x0, dy = start[3 * i + 1] - y0, dz = start[3 * i + 2] - z0;
+    const double xx = dx * dx, yy = dy * dy, zz = dz * dz;
+    const double d = __builtin_sqrt((xx + yy) + zz);
+    delay[i] = (start_ns[i] - t0) - d / c_m_per_ns;
+    if (distance) distance[i] = d;
+  }
+  return LH_OK;
+}

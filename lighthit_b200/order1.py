@@ -244,14 +244,17 @@ def _element(source, name):
 def element_box(elements):
     """Per-coordinate minima and maxima of the element starts and ends
     ``start + length * direction`` (``compress``'s cell grid, ``prompt.py:1317-1402``):
-    ``(low, high)``. Column reductions (an axis-0 reduction of an (N, 3) array is
-    several times slower in NumPy); minima and maxima are exact in any order."""
+    ``(low, high)``, in one host pass of the library (minima and maxima are
+    exact in any order)."""
     start = np.ascontiguousarray(_element(elements, "start_m"), float)
     direction = np.ascontiguousarray(_element(elements, "direction"), float)
-    length = np.asarray(_element(elements, "length_m"), float)
-    ends = start + length[:, None] * direction
-    low = np.array([min(start[:, k].min(), ends[:, k].min()) for k in range(3)])
-    high = np.array([max(start[:, k].max(), ends[:, k].max()) for k in range(3)])
+    length = np.ascontiguousarray(_element(elements, "length_m"), float)
+    if len(length) == 0:
+        raise ValueError("element_box of no elements")
+    low, high = np.empty(3), np.empty(3)
+    _lib.check(_lib.load().lh_element_box(len(length), start.ctypes.data, direction.ctypes.data,
+                                          length.ctypes.data, low.ctypes.data, high.ctypes.data),
+               "lh_element_box")
     return low, high
 
 

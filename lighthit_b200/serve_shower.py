@@ -86,6 +86,26 @@ class ShowerServer:
         for t in self.threads:
             t.start()
 
+    def prime(self, sources):
+        """Run ``sources`` once on every worker, before serving (results dropped).
+
+        A worker's route grows its device workspaces and tables (pencil and
+        group tables, source lattices) to the largest shower it has seen, and
+        the allocator keeps freed blocks per stream; a shower larger than any
+        before it therefore allocates device memory in the middle of serving.
+        Priming with the largest showers expected (as many copies as the route
+        has side-stream lanes, so that every lane sees them) sizes all of that
+        up front."""
+        sources = list(sources)
+        if not sources:
+            return
+        with self.lock:
+            if self.in_flight or self.pending:
+                raise RuntimeError("prime() runs before any request is submitted")
+        for route, stream in zip(self.routes, self.streams):
+            for first in range(0, len(sources), self.max_batch):
+                self._run(route, stream, sources[first:first + self.max_batch])
+
     def submit(self, source, *, arrival=None):
         req = ShowerRequest(source, arrival if arrival is not None else time.perf_counter())
         req.footprint = int(self._footprint(source))

@@ -421,10 +421,15 @@ def delay_groups(el, *, prompt_delay_ns, cell_ns, window_end_ns, group_index_max
     ``cell_ns`` cells, each shifted by its smallest delay, unless none of their
     light can arrive before the window ends (``beyond``: charge only).
     Returns ``(prompt_mask, [(mask, shift_ns)], beyond_mask)``."""
-    first = int(np.argmin(el["start_ns"]))
-    d0 = el["start_m"] - el["start_m"][first]
-    distance = np.sqrt(d0[:, 0] * d0[:, 0] + d0[:, 1] * d0[:, 1] + d0[:, 2] * d0[:, 2])
-    delay = el["start_ns"] - el["start_ns"][first] - distance / C_M_PER_NS
+    start_ns = np.ascontiguousarray(el["start_ns"], float)
+    start = np.ascontiguousarray(el["start_m"], float)
+    first = int(np.argmin(start_ns))
+    # (t - t_first) - |x - x_first| / c per step, one host pass of the library
+    delay, distance = np.empty(len(start_ns)), np.empty(len(start_ns))
+    _lib.check(_lib.load().lh_element_delays(len(start_ns), start.ctypes.data,
+                                             start_ns.ctypes.data, first, C_M_PER_NS,
+                                             delay.ctypes.data, distance.ctypes.data),
+               "lh_element_delays")
     prompt = delay <= prompt_delay_ns
     beyond = ~prompt & (delay - (group_index_max - 1.0) * distance / C_M_PER_NS > window_end_ns)
     within = ~prompt & ~beyond

@@ -10,6 +10,7 @@ deposit, time-lattice transform and stencil run in ``liblh_b200.so``.
 from __future__ import annotations
 
 import ctypes as C
+import functools
 from dataclasses import dataclass
 
 import numpy as np
@@ -77,9 +78,31 @@ def axis_frame(start, direction, length, weights):
     helper = np.array([0.0, 0.0, 1.0])
     if abs(float(axis @ helper)) > 0.9:
         helper = np.array([1.0, 0.0, 0.0])
-    first = np.cross(axis, helper)
+    first = _cross(axis, helper)
     first /= np.linalg.norm(first)
-    return centre, axis, first, np.cross(axis, first)
+    return centre, axis, first, _cross(axis, first)
+
+
+@functools.lru_cache(maxsize=8)
+def _gauss_rule(order):
+    x, w = np.polynomial.legendre.leggauss(order)
+    x.flags.writeable = False
+    w.flags.writeable = False
+    return x, w
+
+
+def _gauss_legendre(order):
+    """Gauss-Legendre nodes and weights (``leggauss``, which solves an eigenvalue
+    problem on every call), computed once per order."""
+    return _gauss_rule(int(order))
+
+
+def _cross(a, b):
+    """``np.cross`` of two 3-vectors (the same products and differences, without
+    its axis bookkeeping, which costs more than the arithmetic here)."""
+    a0, a1, a2 = float(a[0]), float(a[1]), float(a[2])
+    b0, b1, b2 = float(b[0]), float(b[1]), float(b[2])
+    return np.array([a1 * b2 - a2 * b1, a2 * b0 - a0 * b2, a0 * b1 - a1 * b0])
 
 
 class SourceCompiler:
@@ -188,7 +211,7 @@ class SourceCompiler:
         centre, axis = np.asarray(frame[0], float), np.asarray(frame[1], float)
         s = self.settings
         order = 1 if float(np.max(length)) <= s.cell_m / 10 else 2
-        x, w = np.polynomial.legendre.leggauss(order)
+        x, w = _gauss_legendre(order)
         fractions, weights = (x + 1) / 2, w / 2
         reference = float(t0.min())
         # axial coordinates as start.axis + f length (direction.axis): matrix-vector

@@ -85,3 +85,46 @@ def test_axis_frame_is_bit_identical_to_the_reference_expressions():
             if float((share * (direction @ axis)).sum()) < 0:
                 axis = -axis
             assert np.array_equal(got[1], axis)
+
+
+def _steps(n, seed):
+    rng = np.random.default_rng(seed)
+    direction = rng.normal(size=(n, 3))
+    direction /= np.linalg.norm(direction, axis=1)[:, None]
+    return (rng.normal(scale=30.0, size=(n, 3)), direction, rng.uniform(0.0, 0.3, n),
+            rng.uniform(0.0, 200.0, n))
+
+
+@pytest.mark.parametrize("n", [1, 7, 5000])
+def test_element_box_is_the_numpy_box(n):
+    from lighthit_b200.order1 import element_box
+    start, direction, length, _ = _steps(n, n)
+    ends = start + length[:, None] * direction
+    low, high = element_box({"start_m": start, "direction": direction, "length_m": length})
+    assert np.array_equal(low, np.minimum(start.min(axis=0), ends.min(axis=0)))
+    assert np.array_equal(high, np.maximum(start.max(axis=0), ends.max(axis=0)))
+    start[n // 2, 1] = np.nan  # NaN bounds for that coordinate only, as NumPy
+    low, high = element_box({"start_m": start, "direction": direction, "length_m": length})
+    assert np.isnan(low[1]) and np.isnan(high[1]) and np.isfinite(low[[0, 2]]).all()
+
+
+def test_delay_groups_match_the_numpy_expressions():
+    from lighthit_b200.shower import C_M_PER_NS, delay_groups
+    start, direction, length, t0 = _steps(4000, 5)
+    el = {"start_m": start, "direction": direction, "length_m": length, "start_ns": t0}
+    first = int(np.argmin(t0))
+    d0 = start - start[first]
+    distance = np.sqrt(d0[:, 0] * d0[:, 0] + d0[:, 1] * d0[:, 1] + d0[:, 2] * d0[:, 2])
+    delay = t0 - t0[first] - distance / C_M_PER_NS
+    kw = dict(prompt_delay_ns=20.0, cell_ns=10.0, window_end_ns=100.0, group_index_max=1.4)
+    prompt, groups, beyond = delay_groups(el, **kw)
+    assert np.array_equal(prompt, delay <= 20.0)
+    far = ~prompt & (delay - 0.4 * distance / C_M_PER_NS > 100.0)
+    assert np.array_equal(beyond, far)
+    within = ~prompt & ~far
+    cells = np.floor(delay / 10.0).astype(np.int64)
+    expected = [(within & (cells == c), float(delay[within & (cells == c)].min()))
+                for c in np.unique(cells[within])]
+    assert len(groups) == len(expected) > 1
+    for (m, shift), (m_ref, shift_ref) in zip(groups, expected):
+        assert np.array_equal(m, m_ref) and shift == shift_ref

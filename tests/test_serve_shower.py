@@ -111,3 +111,27 @@ def test_base_exceptions_are_handed_back_to_the_request():
     done = srv.drain(1, timeout=30)
     assert isinstance(done[0].error, SystemExit)
     srv.close()
+
+
+def test_prime_runs_the_sources_on_every_worker_in_batches():
+    routes = [FakeRoute(delay=0.0) for _ in range(3)]
+    srv = server(routes, max_batch=4, hbm_budget_bytes=1000)
+    srv.prime([{"id": k, "value": k, "bytes": 10} for k in range(6)])
+    for rt in routes:
+        assert rt.batches == [[0, 1, 2, 3], [4, 5]]
+    assert srv.completed == []  # priming hands nothing to drain()
+    reqs = [srv.submit({"id": k, "value": k, "bytes": 10}) for k in range(5)]
+    srv.drain(5, timeout=30)
+    srv.close()
+    assert [r.result for r in reqs] == [2 * k for k in range(5)]
+
+
+def test_prime_refuses_once_requests_are_queued():
+    gate = threading.Event()
+    srv = server([FakeRoute(gate=gate)], max_batch=2, hbm_budget_bytes=1000)
+    srv.submit({"id": 0, "value": 0, "bytes": 10})
+    with pytest.raises(RuntimeError):
+        srv.prime([{"id": 1, "value": 1, "bytes": 10}])
+    gate.set()
+    srv.drain(1, timeout=30)
+    srv.close()
