@@ -581,6 +581,7 @@ class ShowerTransport:
         self.profile = profile
         self.n_lanes = max(1, int(lanes))
         self._lane_list = None
+        self._omega_dev = None
 
     # -- per-event launches on side streams -------------------------------------
     def _lanes(self):
@@ -1066,12 +1067,15 @@ class ShowerTransport:
             origin = np.concatenate([events[k].origins[work] for k, work in row_ev])
             zero = np.concatenate([events[k].charge[work, 2] - events[k].late_charge[work]
                                    for k, work in row_ev])
-            phase = np.exp(-1j * np.outer(origin, omega))
-            phase[:, 0] = 0.0
-            packed = _lib.upload(np.concatenate([phase, zero[:, None].astype(complex)], axis=1),
-                                 torch.complex128, dev)
-            rel = torch.cat(specs) * packed[:, :-1]
-            rel[:, 0] = packed[:, -1]
+            # the phases e^{-i w origin} on the device (one upload of the origins
+            # and zero-frequency charges)
+            packed = _lib.upload(np.concatenate([origin, zero]), torch.float64, dev)
+            rows = len(origin)
+            if getattr(self, "_omega_dev", None) is None:
+                self._omega_dev = torch.tensor(omega, dtype=torch.float64, device=dev)
+            angle = torch.outer(packed[:rows], self._omega_dev).neg_()
+            rel = torch.cat(specs) * torch.polar(torch.ones_like(angle), angle)
+            rel[:, 0] = packed[rows:]
             bins2_d, _ = T.readout.bins(rel.to(torch.complex64), mode=cfg.readout_mode)
         # one read: the >=2 bins and spectra of the active OMs, the order-0 bins
         with_bins0 = [k for k, ev in enumerate(events) if np.any(ev.active)]
