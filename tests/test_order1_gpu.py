@@ -143,3 +143,36 @@ def test_screen_pack_matches_oracle():
     sums = np.bincount(parent[~roots], weights=dev["w0"][~roots], minlength=n)
     assert np.allclose(sums[roots], dev["w0"][roots], rtol=1e-12, atol=0)
     assert np.all(roots[parent[~roots]])
+
+
+@pytest.mark.parametrize("step", [0.01, 0.004])
+def test_long_path_grids_match_the_oracle(step):
+    """Path steps 10 and 25 times finer than the route's (typical grids of
+    ~330 and ~830 nodes against ~33): grids past the 512 nodes that the small
+    batch instance holds in shared memory are handed to the full-size
+    instance. Stage B on the reference's pencils against the oracle's grouped
+    order 1 with the same steps (the finer grids move the charge by ~2e-5, so
+    the comparison sees the grid)."""
+    from dataclasses import replace
+    from lighthit_b200.order1 import Order1Tables, PencilTable, grouped
+    from oracle import order1 as O1
+    g = fixture()
+    base = tables_of(g)
+    s = replace(base.settings, path_step=step, path_step_tail=2.5 * step)
+    tables = Order1Tables({k: g[k] for k in ("mus", "mut", "speed", "s0w", "s2w")},
+                          float(g["g"]), (g["coef"], g["ipow"], g["jpow"], int(g["degree"])),
+                          g["positions_m"], g["looks"], g["areas_m2"], g["edges_ns"], settings=s)
+    pencils = {k: g[f"sub_pencil_{k}"] for k in PENCIL_KEYS}
+    table, n = PencilTable.from_host(pencils, tables.device)
+    work = np.arange(tables.n_om)
+    q, b = grouped(tables, table, work, g["origins_ns"], n_pencils=n)
+    q_ref, b_ref, _, _ = O1.grouped(
+        pencils, g["positions_m"], g["looks"], g["areas_m2"], g["origins_ns"], work,
+        (g["coef"], g["ipow"], g["jpow"], int(g["degree"])), float(g["g"]),
+        {k: g[k] for k in ("mus", "mut", "speed", "s0w", "s2w")}, g["edges_ns"],
+        path_step=step, path_step_tail=2.5 * step, tail_exponent=float(g["tail_exponent"]),
+        direct_bins=int(g["direct_bins"]), max_path_nodes=int(g["max_path_nodes"]),
+        smoothing_factor=float(g["smoothing_factor"]),
+        merge=(float(g["merge_theta_min"]), float(g["merge_theta_ratio"]),
+               float(g["merge_tau_ns"]), float(g["merge_log_r"])))
+    check(q.cpu().numpy(), b.cpu().numpy(), q_ref, b_ref)
