@@ -629,7 +629,10 @@ struct O1GroupShared {
 };
 
 // One thread per (work OM, pencil): _grouped_pencils_order1_block's pencil
-// loop (_prompt_numba.py:1827-1921) with the generic moment layout.
+// loop (_prompt_numba.py:1827-1921) with the generic moment layout. kScreen
+// (kScreen): the coarse screen's instance; the fine instance carries none of
+// the screen's code (a smaller loop for the instruction cache).
+template <bool kScreen>
 __global__ void __launch_bounds__(256, 2)
 o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
                                 int32_t n_pencils_bound, const int32_t* n_pencils_device,
@@ -688,7 +691,7 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
     pen[320] = Pn.var_major[p]; pen[352] = Pn.var_minor[p];
     for (int f = 0; f < 6; ++f) pen[(12 + f) * 32] = Pn.pos_cov[6 * p + f];
     pen[576] = Pn.w0[p]; pen[608] = Pn.w2[p];
-    const int parent = C.screen ? Pn.parent[p] : -1;
+    const int parent = kScreen ? Pn.parent[p] : -1;
     for (int k = 0; k < kO1GroupOms; ++k) {
     const int w = w_first + k;
     if (w >= n_work) break;  // the same for the whole warp
@@ -701,14 +704,14 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
     const double r = sqrt(dx * dx + dy * dy + dz * dz);
     const double hx = dx / r, hy = dy / r, hz = dz / r;
     // the screen's charge batches ignore emission time (_prompt_screen.py:220-229)
-    const double t_emit = C.screen ? 0.0 : pen[96] - origins[d];
-    const double tau = C.screen ? 0.0 : t_emit + r / C.speed_ref;
+    const double t_emit = kScreen ? 0.0 : pen[96] - origins[d];
+    const double tau = kScreen ? 0.0 : t_emit + r / C.speed_ref;
     const double log_r = log(r);
     const long long key0 = (long long)floor(log_r / C.log_r_step) + (1ll << 20);
     const long long key1 =
         min(max((long long)floor(tau / C.tau_step) + (1ll << 20), 0ll), (1ll << 21) - 1);
-    const long long base = C.screen ? key0 * 2 * theta_bins : ((key1 << 21) + key0) * 2 * theta_bins;
-    if (C.screen && live) {  // a parent unless the OM looks into it, else its children
+    const long long base = kScreen ? key0 * 2 * theta_bins : ((key1 << 21) + key0) * 2 * theta_bins;
+    if (kScreen && live) {  // a parent unless the OM looks into it, else its children
       // rows of a table whose stage A overflowed are not written (the caller
       // redoes it): an index outside the table is never followed
       if (parent >= n_pencils || parent < -1) live = false;
@@ -717,7 +720,7 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
     }
     // children stand in for their parent only where the OM looks into it, so
     // most screen warps over children have nothing to add
-    if (C.screen && !__any_sync(0xffffffffu, live)) continue;
+    if (kScreen && !__any_sync(0xffffffffu, live)) continue;
     // _pencil_frame_from_ray_cached_look (_prompt_numba.py:594-606)
     const double sx = pen[128], sy = pen[160], sz = pen[192];
     const double c1 = sx * nx + sy * ny + sz * nz;
@@ -777,7 +780,7 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
         u_ = hx * ax + hy * ay + hz * az;
         v_ = hx * bx + hy * by + hz * bz;
         mode = (!far && extent > 0.0 && theta < sf * extent) ? 2 : 3;
-        if (C.screen) {
+        if (kScreen) {
           // pencil_radial_rule (_prompt_screen.py:143-169): two radial nodes where the
           // OM lies within the pencil's angular smoothing extent
           const double half_tr = 0.5 * (m11 + m22);
@@ -865,7 +868,7 @@ o1_group_kernel(const lh_order1_config C, const lh_order1_pencil_table Pn,
     const int nm = C.n_mono;
     // one group entry per radial node: the screen's two-node rule adds a second
     // (_prompt_screen.py:281-336); every lane of the warp takes both rounds
-    const int nodes = C.screen ? 2 : 1;
+    const int nodes = kScreen ? 2 : 1;
     for (int node = 0; node < nodes; ++node) {
       const bool live_n = live && (node == 0 || weight2 > 0.0);
       const double wn = node == 0 ? weight : weight2;
@@ -1695,7 +1698,8 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
   const size_t group_smem =
       sizeof(double) * 32 * (256 / 32) * (2 * C->n_mono + 6 + lh::kO1PencilFields);
   if (group_smem > 48 * 1024 &&
-      cudaFuncSetAttribute(lh::o1_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(C->screen ? lh::o1_group_kernel<true> : lh::o1_group_kernel<false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)group_smem) != cudaSuccess)
     return LH_ECUDA;
   {
@@ -1704,9 +1708,15 @@ extern "C" int lh_order1_grouped(const lh_order1_config* C, const lh_order1_penc
     // host's pencil count is the table's capacity, far above the pencils a
     // shower makes, so a grid sized from it would mostly launch idle CTAs)
     const int group_grid = std::min(lh::grid_for((int64_t)n_work * n_pencils, 256), 148 * 2);
-    lh::o1_group_kernel<<<group_grid, 256, group_smem, s>>>(
-        *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows, W.gcount,
-        status, lh::kernel_units() ? lh::kernel_units() + LH_KT_O1_GROUP : nullptr);
+    unsigned long long* units = lh::kernel_units() ? lh::kernel_units() + LH_KT_O1_GROUP : nullptr;
+    if (C->screen)
+      lh::o1_group_kernel<true><<<group_grid, 256, group_smem, s>>>(
+          *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows,
+          W.gcount, status, units);
+    else
+      lh::o1_group_kernel<false><<<group_grid, 256, group_smem, s>>>(
+          *C, *P, n_pencils, n_pencils_device, work, n_work, origins, W.gkeys, W.grows,
+          W.gcount, status, units);
   }
   const size_t sort_smem =
       cap <= lh::kO1SmemSort ? sizeof(unsigned long long) * (size_t)cap : 0;
