@@ -20,6 +20,9 @@ def test_served_showers_equal_each_shower_alone():
     server = ShowerServer(lambda: ShowerTransport(ShowerTables.synthetic("c2")), workers=2,
                           max_batch=3)
     try:
+        # workspaces sized by the largest showers first: results are unchanged
+        server.prime(sorted(showers, key=lambda s: len(s["length_m"]))[-2:] * 2)
+        assert server.completed == []
         early = [server.submit(s) for s in showers[:4]]
         time.sleep(0.05)  # the first batches are on the device when the rest arrive
         late = [server.submit(s) for s in showers[4:]]
