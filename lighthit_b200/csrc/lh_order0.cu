@@ -385,6 +385,7 @@ struct O0Shared {
   double cuts[kO0CutPool];
   double warp_charge[kO0Threads / 32];
   double warp_check[kO0Threads / 32];
+  double bin_stage[kO0Threads / 32][32];  // per warp: the lanes' bin values before one add per bin
   int scan[32];
   int chunk;
   int n_pairs;
@@ -797,7 +798,22 @@ order0_kernel(const lh_order0_optics O, const lh_order0_batch B, const O0Work W,
           const double arrival =
               emission + o0_entry(Bq, cosine * along + sine * rho * cos(phi_mid)) / velocity;
           const int slot = o0_search_right(edges, n_edges, arrival) - 1;
-          if (slot >= 0 && slot < nb) atomicAdd(&sbins[slot], value);
+          // the lanes here together that land in one bin (neighbouring s-nodes
+          // of one item, mostly) add their sum once: one shared-memory atomic
+          // per bin and warp instead of one per lane
+          const int key = (slot >= 0 && slot < nb) ? slot : -1;
+          const unsigned here = __activemask();
+          const unsigned peers = __match_any_sync(here, key);
+          const int lane = tid & 31;
+          double* stage = S.bin_stage[tid >> 5];
+          stage[lane] = value;
+          __syncwarp(here);
+          if (key >= 0 && lane == __ffs(peers) - 1) {
+            double sum = 0.0;
+            for (unsigned m = peers; m; m &= m - 1) sum += stage[__ffs(m) - 1];
+            atomicAdd(&sbins[key], sum);
+          }
+          __syncwarp(here);  // the stage is rewritten by the next piece
         }
       }
     }
