@@ -635,6 +635,13 @@ int lh_element_box(int64_t n, const double* start, const double* direction,
 int lh_element_delays(int64_t n, const double* start, const double* start_ns, int64_t first,
                       double c_m_per_ns, double* delay, double* distance);
 
+/* Host function (no device work): the sub-segments of compress
+ * (prompt.py:1317-1402): element i is cut into max(1, ceil(length[i] / a_step))
+ * pieces; offsets[0..n] are the running totals (offsets[0] = 0) and *n_sub the
+ * sum. LH_EINVAL for a negative or non-finite length. */
+int lh_subsegment_offsets(int64_t n, const double* length, double a_step, int64_t* offsets,
+                          int64_t* n_sub);
+
 /* Flash transport that allocates nothing (no counterpart in the reference).
  * For callers that cannot allocate device memory: processes whose device memory
  * is reserved up front by their own framework's allocator (trigger/DAQ farms),

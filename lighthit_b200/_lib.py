@@ -194,6 +194,7 @@ SIGNATURES = {
     "lh_axis_frame_sums": (C.c_int, [C.c_int64, P, P, P, P, P, P]),
     "lh_element_box": (C.c_int, [C.c_int64, P, P, P, P, P]),
     "lh_element_delays": (C.c_int, [C.c_int64, P, P, C.c_int64, C.c_double, P, P]),
+    "lh_subsegment_offsets": (C.c_int, [C.c_int64, P, C.c_double, P, P]),
     "lh_flash_combine": (C.c_int, [C.POINTER(FlashProblem), C.POINTER(FlashNodes),
                                    C.POINTER(FlashBatch), P]),
     "lh_ge2_workspace_bytes": (C.c_size_t, [C.POINTER(Ge2Table), C.POINTER(Ge2Problem)]),

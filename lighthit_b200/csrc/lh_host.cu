@@ -94,3 +94,23 @@ extern "C" int lh_element_delays(int64_t n, const double* start, const double* s
   }
   return LH_OK;
 }
+
+// compress's sub-segment layout (prompt.py:1317-1402): element i is cut into
+// n_a = max(1, ceil(length_i / a_step)) sub-segments; offsets[i] is the first
+// sub-segment of element i (offsets[n] = *n_sub). Lengths must be finite and
+// non-negative.
+extern "C" int lh_subsegment_offsets(int64_t n, const double* length, double a_step,
+                                     int64_t* offsets, int64_t* n_sub) {
+  if (n < 0 || (n && !length) || !offsets || !n_sub || !(a_step > 0.0)) return LH_EINVAL;
+  int64_t total = 0;
+  offsets[0] = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const double x = length[i];
+    if (!(x >= 0.0) || x > 1e300) return LH_EINVAL;
+    const double pieces = __builtin_ceil(x / a_step);
+    total += pieces < 1.0 ? 1 : (int64_t)pieces;
+    offsets[i + 1] = total;
+  }
+  *n_sub = total;
+  return LH_OK;
+}

@@ -179,9 +179,14 @@ class Order1Tables:
         if getattr(self, "_pencil_pool", None) is None or self._pencil_pool.numel() < need:
             self._pencil_pool = torch.empty(max(need, 1 << 22), dtype=torch.float64,
                                             device=self.device)
+        cached = getattr(self, "_pool_table", None)
+        if (cached is not None and cached.capacity == int(capacity)
+                and cached._buffer.data_ptr() == self._pencil_pool.data_ptr()):
+            return cached  # the same views of the same pool: no new table object
         table = PencilTable(capacity, self.device, self._pencil_pool[:need],
                             screen=self.settings.screen)
         table.pooled = True
+        self._pool_table = table
         return table
 
     def workspace(self, n_subseg, n_work):
@@ -274,10 +279,14 @@ def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=Non
     length = np.asarray(_element(elements, "length_m"), float)
     n_el = len(length)
     a_step = 0.5 * s.cell_m
-    n_a = np.maximum(1, np.ceil(length / a_step)).astype(np.int64)
-    offsets = np.zeros(n_el + 1, np.int64)
-    offsets[1:] = np.cumsum(n_a)
-    n_sub = int(offsets[-1])
+    # max(1, ceil(length / a_step)) sub-segments per element, their running totals
+    offsets = np.empty(n_el + 1, np.int64)
+    n_total = np.zeros(1, np.int64)
+    length = np.ascontiguousarray(length, float)
+    if _lib.load().lh_subsegment_offsets(n_el, length.ctypes.data, a_step, offsets.ctypes.data,
+                                         n_total.ctypes.data):
+        raise ValueError("element lengths must be finite and non-negative")
+    n_sub = int(n_total[0])
     if n_el:
         lo_box, hi_box = element_box(elements) if box is None else box
         low = lo_box - s.cell_m
@@ -313,9 +322,13 @@ def pencils(tables: Order1Tables, elements, cone_cos, *, stream=None, status=Non
     # elements share cells. A table that overflows is redone at the full bound.
     if s.screen:  # parents and children
         nodes *= 2
-    capacity = nodes if capacity_full else min(nodes, max(1 << 17, nodes // 4))
+    # pooled tables in powers of two, so that showers of similar size reuse one
+    capacity = (nodes if capacity_full
+                else min(nodes, max(1 << 17, 1 << int(nodes // 4 - 1).bit_length())))
     table = (PencilTable(capacity, dev, screen=s.screen) if capacity_full
              else tables.pencil_table(capacity))
+    if n_sub == 0:
+        table.count.zero_()  # stage A writes no count for no elements (a reused table)
     ws = tables.workspace(n_sub, 0)
     st = status if status is not None else torch.zeros(1, dtype=torch.int32, device=dev)
     sp = _lib.stream_ptr(stream or torch.cuda.current_stream(dev))

@@ -599,6 +599,7 @@ class ShowerTransport:
                     view = copy.copy(getattr(T, name))
                     view._workspace = None
                     view._pencil_pool = None
+                    view._pool_table = None
                     view.__dict__.pop("_bands", None)  # per-band views own workspaces too
                     views[name] = view
                 lanes.append(_Lane(torch.cuda.Stream(T.device), **views))
@@ -732,8 +733,13 @@ class ShowerTransport:
             events.append(ev)
         store = ElementBatch([ev.el for ev in events], dev)  # one upload for every stage
         stage("setup")
+        # the batch's status words, one zeroed allocation: the source compile's,
+        # the prompt stages', then a screen and a fine word per shower
+        words = torch.zeros(2 + 2 * len(events), dtype=torch.int32, device=dev)
+        for k, ev in enumerate(events):
+            ev.words = (words[2 + 2 * k:3 + 2 * k], words[3 + 2 * k:4 + 2 * k])
         # ---- order >=2 sources on the node bands (device, all showers)
-        src_status = torch.zeros(1, dtype=torch.int32, device=dev)
+        src_status = words[0:1]
         compiled = []
         with self._fan_out() as lanes:
             for k, ev in enumerate(events):
@@ -892,11 +898,11 @@ class ShowerTransport:
         prompt_events = [ev for ev in events if len(ev.work)]
         for k, ev in enumerate(events):
             ev.device_el = prompt_store.event(k)
-        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        status = words[1:2]
         cone = float(np.sum(T.prompt["s0w"] * T.phase) / np.sum(T.prompt["s0w"]))
         for ev in prompt_events:
             self._order1_units(ev, cone)
-            ev.status = torch.zeros(1, dtype=torch.int32, device=dev)
+            ev.status = ev.words[0]
         # the coarse order-1 screens run on the lanes while order 0 (one launch for
         # every shower) runs on this stream
         with self._fan_out() as lanes:
@@ -951,7 +957,7 @@ class ShowerTransport:
                                    + cfg.screen_margin * np.maximum(coarse[ev.work], 0.0))
                                   >= threshold]
             if len(ev.fine):
-                ev.status = torch.zeros(1, dtype=torch.int32, device=dev)
+                ev.status = ev.words[1]
                 fine_events.append(ev)
         with self._fan_out() as lanes:
             for k, ev in enumerate(fine_events):

@@ -128,3 +128,20 @@ def test_delay_groups_match_the_numpy_expressions():
     assert len(groups) == len(expected) > 1
     for (m, shift), (m_ref, shift_ref) in zip(groups, expected):
         assert np.array_equal(m, m_ref) and shift == shift_ref
+
+
+def test_subsegment_offsets_are_the_numpy_running_totals():
+    from lighthit_b200 import _lib
+    rng = np.random.default_rng(9)
+    length = np.ascontiguousarray(np.concatenate([rng.uniform(0.0, 3.0, 4000), [0.0, 0.25, 0.5]]))
+    step = 0.25
+    expected = np.zeros(len(length) + 1, np.int64)
+    expected[1:] = np.cumsum(np.maximum(1, np.ceil(length / step)).astype(np.int64))
+    offsets, total = np.empty(len(length) + 1, np.int64), np.zeros(1, np.int64)
+    lib = _lib.load()
+    assert lib.lh_subsegment_offsets(len(length), length.ctypes.data, step, offsets.ctypes.data,
+                                     total.ctypes.data) == 0
+    assert np.array_equal(offsets, expected) and total[0] == expected[-1]
+    bad = np.array([1.0, np.nan])
+    assert lib.lh_subsegment_offsets(2, bad.ctypes.data, step, offsets.ctypes.data,
+                                     total.ctypes.data) != 0
